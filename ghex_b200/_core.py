@@ -1,0 +1,375 @@
+"""Objects shared by the structured and unstructured front ends.
+
+Mirrors the object model of GHEX's Python bindings (bindings/python/src/ghex): a context, a
+pattern container made by make_pattern, field descriptors bound to a pattern with
+``pattern(field)`` (a buffer_info), a communication object whose ``exchange`` returns a handle
+with ``wait()``. Everything below the Python objects is the C ABI of libghex_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from typing import Any, Iterable, Sequence
+
+from . import _capi
+from ._capi import call
+
+
+class Architecture(enum.Enum):
+    """Where a field lives (bindings/python/src/ghex/util.py:22-24). Only GPU is supported."""
+
+    CPU = "cpu"
+    GPU = "gpu"
+
+
+# --------------------------------------------------------------------------------------------
+# device arrays
+# --------------------------------------------------------------------------------------------
+_TYPESTR = {"<f4": _capi.F32, "<f8": _capi.F64, "<i4": _capi.I32, "<i8": _capi.I64,
+            "|u1": _capi.U8, "<u2": _capi.U16}
+
+
+def _torch():
+    try:
+        import torch
+        return torch
+    except ImportError:  # pragma: no cover - torch is part of the environment
+        return None
+
+
+def array_info(field: Any) -> dict:
+    """Pointer, shape, byte strides, dtype code and device of a CUDA array.
+
+    Accepts torch tensors and any object exposing ``__cuda_array_interface__``. Host arrays are
+    rejected: ghex_b200 exchanges device memory only.
+    """
+    torch = _torch()
+    if torch is not None and isinstance(field, torch.Tensor):
+        if not field.is_cuda:
+            raise TypeError("ghex_b200 exchanges device memory only: the tensor is not on a CUDA device")
+        codes = {torch.float32: _capi.F32, torch.float64: _capi.F64, torch.int32: _capi.I32,
+                 torch.int64: _capi.I64, torch.uint8: _capi.U8, torch.uint16: _capi.U16}
+        if field.dtype not in codes:
+            raise TypeError(f"unsupported dtype {field.dtype}")
+        es = field.element_size()
+        return {"ptr": field.data_ptr(), "shape": tuple(field.shape),
+                "strides": tuple(s * es for s in field.stride()), "dtype": codes[field.dtype],
+                "itemsize": es, "device": field.device.index or 0}
+    cai = getattr(field, "__cuda_array_interface__", None)
+    if cai is None:
+        raise TypeError("ghex_b200 exchanges device memory only: expected a CUDA tensor or an object "
+                        "with __cuda_array_interface__")
+    typestr = cai["typestr"]
+    if typestr not in _TYPESTR:
+        raise TypeError(f"unsupported dtype {typestr}")
+    shape = tuple(cai["shape"])
+    itemsize = int(typestr[2:])
+    strides = cai.get("strides")
+    if strides is None:  # C-contiguous
+        strides, s = [], itemsize
+        for n in reversed(shape):
+            strides.insert(0, s)
+            s *= n
+    return {"ptr": int(cai["data"][0]), "shape": shape, "strides": tuple(strides),
+            "dtype": _TYPESTR[typestr], "itemsize": itemsize, "device": None}
+
+
+def stream_of(fields: Iterable[Any]):
+    """The stream an exchange is ordered on: torch's current stream for torch tensors."""
+    torch = _torch()
+    for f in fields:
+        if torch is not None and isinstance(f, torch.Tensor):
+            return C.c_void_p(torch.cuda.current_stream(f.device).cuda_stream)
+    return C.c_void_p(0)
+
+
+# --------------------------------------------------------------------------------------------
+# context
+# --------------------------------------------------------------------------------------------
+class context:
+    """Replaces ghex.context (bindings/python/src/ghex/context.py:20-21).
+
+    One process owns every domain of an exchange, so there is no communicator: rank() is 0 and
+    size() is 1. ``device`` selects the CUDA device the fields live on.
+    """
+
+    def __init__(self, comm: Any = None, thread_safe: bool = False, device: int | None = None):
+        if device is None:
+            torch = _torch()
+            device = torch.cuda.current_device() if torch is not None and torch.cuda.is_available() else 0
+        self.device = int(device)
+        self.thread_safe = bool(thread_safe)
+        h = C.c_void_p()
+        call("ghexb_context_create", self.device, C.byref(h))
+        self._h = h
+
+    def rank(self) -> int:
+        return 0
+
+    def size(self) -> int:
+        return 1
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _capi.lib.ghexb_context_destroy(h)
+            self._h = None
+
+
+def make_context(comm: Any = None, thread_safe: bool = False, device: int | None = None) -> context:
+    """Replaces ghex.context.make_context(comm, thread_safe)."""
+    return context(comm, thread_safe, device)
+
+
+# --------------------------------------------------------------------------------------------
+# patterns and buffer_info
+# --------------------------------------------------------------------------------------------
+class BufferInfo:
+    """A field bound to a pattern (buffer_info.hpp:33-71). Holds references, owns nothing."""
+
+    __slots__ = ("pattern", "field")
+
+    def __init__(self, pattern: "PatternContainer", field: "FieldDescriptorBase"):
+        self.pattern = pattern
+        self.field = field
+
+    def handle(self) -> C.c_void_p:
+        return self.field._bind(self.pattern)
+
+    def arrays(self) -> list:
+        return [self.field.array]
+
+
+class PatternContainer:
+    """The result of make_pattern: one pattern per domain (pattern_container.hpp:32-101)."""
+
+    grid_type = "structured"
+    domain_id_type = "int"
+
+    def __init__(self, ctx: context, handle: C.c_void_p, domain_ids: Sequence[Any]):
+        self.context = ctx
+        self._h = handle
+        self._ids = list(domain_ids)
+
+    def __call__(self, field: "FieldDescriptorBase") -> BufferInfo:
+        if field.domain_key() not in self._ids:
+            raise ValueError("field incompatible with available domains!")
+        return BufferInfo(self, field)
+
+    def __len__(self) -> int:
+        return len(self._ids)
+
+    def size(self) -> int:
+        return len(self._ids)
+
+    def max_tag(self) -> int:
+        v = C.c_int()
+        call("ghexb_pattern_max_tag", self._h, C.byref(v))
+        return v.value
+
+    def domain_index(self, key: Any) -> int:
+        return self._ids.index(key)
+
+    # -- introspection -------------------------------------------------------------------
+    def num_spaces(self, domain_index: int, send: bool = False) -> int:
+        n = C.c_int()
+        call("ghexb_pattern_num_spaces", self._h, domain_index, int(send), C.byref(n))
+        return n.value
+
+    def spaces(self, domain_index: int, send: bool = False) -> list:
+        """Iteration spaces as (neighbour index, local first, local last, global first, global last)."""
+        out = []
+        for k in range(self.num_spaces(domain_index, send)):
+            nb = C.c_int()
+            arrs = [(C.c_int * 4)() for _ in range(4)]
+            call("ghexb_pattern_space", self._h, domain_index, int(send), k, C.byref(nb), *arrs)
+            out.append((nb.value, *(tuple(a) for a in arrs)))
+        return out
+
+    def index_lists(self, domain_index: int, send: bool = False) -> list:
+        """Unstructured entries as (neighbour index, local ids)."""
+        out = []
+        for k in range(self.num_spaces(domain_index, send)):
+            nb, cnt = C.c_int(), C.c_int64()
+            call("ghexb_pattern_space_indices", self._h, domain_index, int(send), k, C.byref(nb), None, 0,
+                 C.byref(cnt))
+            buf = (C.c_int64 * max(1, cnt.value))()
+            call("ghexb_pattern_space_indices", self._h, domain_index, int(send), k, C.byref(nb), buf,
+                 cnt.value, C.byref(cnt))
+            out.append((nb.value, list(buf)[: cnt.value]))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _capi.lib.ghexb_pattern_destroy(h)
+            self._h = None
+
+
+class FieldDescriptorBase:
+    """A wrapped device array; bound lazily to every pattern it is used with."""
+
+    def __init__(self, array: Any):
+        self.array = array
+        self._handles: dict[int, C.c_void_p] = {}
+
+    def domain_key(self) -> Any:  # pragma: no cover - abstract
+        raise NotImplementedError
+
+    def _wrap(self, pattern: PatternContainer) -> C.c_void_p:  # pragma: no cover - abstract
+        raise NotImplementedError
+
+    def _bind(self, pattern: PatternContainer) -> C.c_void_p:
+        key = id(pattern)
+        h = self._handles.get(key)
+        if h is None:
+            h = self._wrap(pattern)
+            self._handles[key] = h
+            self._patterns = getattr(self, "_patterns", []) + [pattern]  # keep patterns alive
+        return h
+
+    def __del__(self):
+        for h in getattr(self, "_handles", {}).values():
+            _capi.lib.ghexb_field_destroy(h)
+        self._handles = {}
+
+
+def _flatten(args: tuple) -> list[BufferInfo]:
+    if len(args) == 1 and isinstance(args[0], (list, tuple)):
+        args = tuple(args[0])
+    out = []
+    for a in args:
+        if isinstance(a, (list, tuple)):
+            out.extend(a)
+        else:
+            out.append(a)
+    for a in out:
+        if not isinstance(a, BufferInfo):
+            raise TypeError("exchange expects buffer_info objects made by pattern(field)")
+    return out
+
+
+# --------------------------------------------------------------------------------------------
+# communication object
+# --------------------------------------------------------------------------------------------
+class Handle:
+    """communication_handle (communication_object.hpp:67-105)."""
+
+    def __init__(self, co: "CommunicationObject", h: C.c_void_p, keep: list):
+        self._co = co
+        self._h = h
+        self._keep = keep
+
+    def wait(self) -> None:
+        call("ghexb_handle_wait", self._h)
+        self._keep = []
+
+    def is_ready(self) -> bool:
+        r = C.c_int()
+        call("ghexb_handle_is_ready", self._h, C.byref(r))
+        if r.value:
+            self._keep = []
+        return bool(r.value)
+
+    def progress(self) -> None:
+        self.is_ready()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _capi.lib.ghexb_handle_destroy(h)
+            self._h = None
+
+
+class CommunicationObject:
+    """communication_object (communication_object.hpp:111-625).
+
+    ``exchange`` accepts a list of buffer_info objects or buffer_infos as positional arguments
+    (_pyghex/structured/regular/communication_object.cpp:60-78). The exchange is ordered on the
+    current torch stream of the fields; ``wait()`` blocks the host until it has finished. Calling
+    exchange again before wait() raises "earlier exchange operation was not finished".
+    """
+
+    def __init__(self, ctx: context):
+        self.context = ctx
+        h = C.c_void_p()
+        call("ghexb_co_create", ctx._h, C.byref(h))
+        self._h = h
+
+    def exchange(self, *buffer_infos) -> Handle:
+        bis = _flatten(buffer_infos)
+        handles = (C.c_void_p * len(bis))(*[bi.handle() for bi in bis])
+        arrays = [a for bi in bis for a in bi.arrays()]
+        h = C.c_void_p()
+        call("ghexb_co_exchange", self._h, handles, len(bis), stream_of(arrays), C.byref(h))
+        return Handle(self, h, [bis, arrays])
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _capi.lib.ghexb_co_destroy(h)
+            self._h = None
+
+
+def make_communication_object(ctx: context) -> CommunicationObject:
+    return CommunicationObject(ctx)
+
+
+# --------------------------------------------------------------------------------------------
+# explicit plans (no reference counterpart): batched / per-field / per-box forms, graph,
+# adjoint, autotuning
+# --------------------------------------------------------------------------------------------
+class ExchangePlan:
+    """The work-descriptor table of one set of buffer_infos, built once."""
+
+    BATCHED = _capi.FORM_BATCHED
+    PER_FIELD = _capi.FORM_PER_FIELD
+    PER_BOX = _capi.FORM_PER_BOX
+
+    def __init__(self, ctx: context, buffer_infos: Sequence[BufferInfo]):
+        self.context = ctx
+        self._bis = _flatten(tuple(buffer_infos))
+        self._arrays = [a for bi in self._bis for a in bi.arrays()]
+        handles = (C.c_void_p * len(self._bis))(*[bi.handle() for bi in self._bis])
+        h = C.c_void_p()
+        call("ghexb_plan_create", ctx._h, handles, len(self._bis), C.byref(h))
+        self._h = h
+
+    def info(self) -> dict:
+        i = _capi.PlanInfo()
+        call("ghexb_plan_get_info", self._h, C.byref(i))
+        return i.as_dict()
+
+    def set_tuning(self, tile_elems: int = 0, block: int = 0, ctas_per_sm: int = 0) -> None:
+        call("ghexb_plan_set_tuning", self._h, tile_elems, block, ctas_per_sm)
+
+    def _stream(self, stream):
+        if stream is None:
+            return stream_of(self._arrays)
+        if isinstance(stream, int):
+            return C.c_void_p(stream)
+        return C.c_void_p(getattr(stream, "cuda_stream", stream))
+
+    def launch(self, form: int = _capi.FORM_BATCHED, stream=None) -> None:
+        call("ghexb_plan_launch", self._h, form, self._stream(stream))
+
+    def graph_launch(self, stream=None) -> None:
+        call("ghexb_plan_graph_launch", self._h, self._stream(stream))
+
+    def adjoint(self, stream=None) -> None:
+        call("ghexb_plan_adjoint_launch", self._h, self._stream(stream))
+
+    def autotune(self, repeats: int = 10, stream=None) -> dict:
+        i = _capi.PlanInfo()
+        call("ghexb_plan_autotune", self._h, self._stream(stream), repeats, C.byref(i))
+        return i.as_dict()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _capi.lib.ghexb_plan_destroy(h)
+            self._h = None
+
+
+def make_exchange_plan(ctx: context, buffer_infos: Sequence[BufferInfo]) -> ExchangePlan:
+    return ExchangePlan(ctx, buffer_infos)

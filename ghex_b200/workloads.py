@@ -1,0 +1,156 @@
+"""Seeded synthetic workloads of the benchmark configurations.
+
+No public dataset is involved: every input is generated here from a seed.
+  * values: splitmix64 (Steele, Lea & Flood, "Fast splittable pseudorandom number generators",
+    OOPSLA 2014; the finaliser constants of Vigna's public-domain splitmix64) of the seed and a
+    global linear index, mapped to [-1, 1); halos start as NaN;
+  * regular grids: a global box split into a tensor product of (optionally uneven, seeded)
+    intervals, one domain per cell of the product, fields padded by their halo widths and stored
+    x fastest.
+
+Arrays are numpy arrays indexed by coordinate (x, y, z[, c]) with x the fastest dimension in
+memory (Fortran order), index 0 being the first cell of the padded memory.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+_GAMMA = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def splitmix64(seed: int, index: np.ndarray) -> np.ndarray:
+    """The splitmix64 output for state seed + (index + 1) * golden gamma (uint64 arithmetic)."""
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed & 0xFFFFFFFFFFFFFFFF) + (np.asarray(index, dtype=np.uint64) + np.uint64(1)) * _GAMMA
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        return z ^ (z >> np.uint64(31))
+
+
+def unit_values(seed: int, index: np.ndarray) -> np.ndarray:
+    """splitmix64 mapped to [-1, 1): the top 53 bits as a fraction, times 2, minus 1."""
+    z = splitmix64(seed, index)
+    return (z >> np.uint64(11)).astype(np.float64) * (2.0 / 9007199254740992.0) - 1.0
+
+
+def uneven_splits(n: int, parts: int, rng: np.random.Generator, lo: float = 0.5, hi: float = 1.5) -> list[tuple[int, int]]:
+    """Split [0, n) into `parts` intervals whose lengths lie within [lo, hi] x the mean."""
+    mean = n / parts
+    for _ in range(10000):
+        w = rng.uniform(lo, hi, size=parts)
+        lengths = np.floor(w / w.sum() * n).astype(int)
+        lengths[-1] = n - lengths[:-1].sum()
+        if np.all(lengths >= int(np.ceil(lo * mean))) and np.all(lengths <= int(np.floor(hi * mean))):
+            break
+    else:  # pragma: no cover - the bounds above always admit a solution for parts >= 1
+        raise RuntimeError("could not draw an uneven split")
+    out, s = [], 0
+    for L in lengths:
+        out.append((s, s + int(L) - 1))
+        s += int(L)
+    return out
+
+
+def even_splits(n: int, parts: int) -> list[tuple[int, int]]:
+    base, rem = divmod(n, parts)
+    out, s = [], 0
+    for p in range(parts):
+        L = base + (1 if p < rem else 0)
+        out.append((s, s + L - 1))
+        s += L
+    return out
+
+
+@dataclass
+class FieldSpec:
+    name: str
+    dtype: type
+    halos: tuple          # (x-, x+, y-, y+, z-, z+)
+    seed: int
+
+
+@dataclass
+class RegularWorkload:
+    name: str
+    shape: tuple                       # global cells per dimension
+    periodic: tuple
+    domains: list                      # (id, first, last) with inclusive global coordinates
+    fields: list = field(default_factory=list)
+
+    @property
+    def dim(self) -> int:
+        return len(self.shape)
+
+    def halo_groups(self) -> dict:
+        """Fields grouped by halo widths (one pattern per group)."""
+        groups: dict = {}
+        for f in self.fields:
+            groups.setdefault(f.halos, []).append(f)
+        return groups
+
+    def extents(self, dom, spec: FieldSpec) -> tuple:
+        _, first, last = dom
+        return tuple(last[k] - first[k] + 1 + spec.halos[2 * k] + spec.halos[2 * k + 1] for k in range(self.dim))
+
+    def offsets(self, spec: FieldSpec) -> tuple:
+        return tuple(spec.halos[2 * k] for k in range(self.dim))
+
+    def domain_array(self, dom, spec: FieldSpec) -> np.ndarray:
+        """Interior = splitmix64(seed, global linear index) in [-1, 1), halo = NaN; x fastest."""
+        _, first, last = dom
+        ext = self.extents(dom, spec)
+        off = self.offsets(spec)
+        a = np.full(ext, np.nan, dtype=spec.dtype, order="F")
+        grids = np.meshgrid(*[np.arange(first[k], last[k] + 1, dtype=np.int64) for k in range(self.dim)], indexing="ij")
+        lin = np.zeros(grids[0].shape, dtype=np.int64)
+        stride = 1
+        for k in range(self.dim):
+            lin += grids[k] * stride
+            stride *= self.shape[k]
+        vals = unit_values(spec.seed, lin).astype(spec.dtype)
+        a[tuple(slice(off[k], off[k] + last[k] - first[k] + 1) for k in range(self.dim))] = vals
+        return a
+
+
+def regular_decomposition(shape: Sequence[int], parts: Sequence[int], seed: int | None = None) -> list:
+    """Domains of a tensor-product split, ids in x-fastest order."""
+    rng = np.random.default_rng(seed) if seed is not None else None
+    splits = [uneven_splits(n, p, rng) if rng is not None else even_splits(n, p) for n, p in zip(shape, parts)]
+    doms = []
+    for idx, combo in enumerate(np.ndindex(*reversed(parts))):
+        c = tuple(reversed(combo))
+        first = tuple(splits[k][c[k]][0] for k in range(len(shape)))
+        last = tuple(splits[k][c[k]][1] for k in range(len(shape)))
+        doms.append((idx, first, last))
+    return doms
+
+
+def config0(seed: int = 42) -> RegularWorkload:
+    """64^3 float64 split 2x2x2, halo 1 on all sides, periodic in x, y and z."""
+    w = RegularWorkload("cfg0: 64^3 f64, 2x2x2, halo 1, periodic xyz", (64, 64, 64), (True, True, True),
+                        regular_decomposition((64, 64, 64), (2, 2, 2)))
+    w.fields = [FieldSpec("f64", np.float64, (1, 1, 1, 1, 1, 1), seed)]
+    return w
+
+
+def config1(seed: int = 42, shape=(400, 300, 96)) -> RegularWorkload:
+    """400x300x96 split 3x3x3 at seeded uneven points; 3 float64 fields with halo (3,3,3,3,0,0)
+    and 2 float32 fields with halo (2,2,2,2,1,1); periodic in y only."""
+    w = RegularWorkload(f"cfg1: {shape[0]}x{shape[1]}x{shape[2]} uneven 3x3x3, 3 f64 (3,3,3,3,0,0) + 2 f32 (2,2,2,2,1,1), periodic y",
+                        tuple(shape), (False, True, False), regular_decomposition(shape, (3, 3, 3), seed))
+    w.fields = [FieldSpec(f"f64_{i}", np.float64, (3, 3, 3, 3, 0, 0), seed + 1 + i) for i in range(3)] + \
+               [FieldSpec(f"f32_{i}", np.float32, (2, 2, 2, 2, 1, 1), seed + 11 + i) for i in range(2)]
+    return w
+
+
+def config4(seed: int = 42, dtype=np.float64, shape=(256, 256, 128)) -> RegularWorkload:
+    """256x256x128 split 2x2x2, halo 1, periodic (the differentiable stencil program)."""
+    w = RegularWorkload(f"cfg4: {shape[0]}x{shape[1]}x{shape[2]} 2x2x2 halo 1 periodic", tuple(shape), (True, True, True),
+                        regular_decomposition(shape, (2, 2, 2)))
+    w.fields = [FieldSpec("x", dtype, (1, 1, 1, 1, 1, 1), seed)]
+    return w

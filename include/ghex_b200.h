@@ -1,0 +1,194 @@
+/*
+ * ghex_b200 C ABI — B200-native halo exchange for many sub-domains resident on one GPU.
+ *
+ * Every entry point returns an int status (GHEXB_OK == 0). On failure the message is
+ * kept per thread and read with ghexb_last_error(). All handles are opaque; all
+ * sizes and coordinates are plain ints; data pointers are device pointers of the
+ * current CUDA device; streams are cudaStream_t passed as void*.
+ *
+ * Each group below names the GHEX interface it replaces (paths relative to the
+ * GHEX source tree, version 0.4.0).
+ */
+#ifndef GHEX_B200_H
+#define GHEX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------- */
+#define GHEXB_OK 0
+#define GHEXB_ERR_INVALID 1      /* bad argument (null pointer, negative size, bad dtype ...) */
+#define GHEXB_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define GHEXB_ERR_BUSY 3         /* "earlier exchange operation was not finished"
+                                    (communication_object.hpp:360,401) */
+#define GHEXB_ERR_INCOMPATIBLE 4 /* "field incompatible with available domains!"
+                                    (pattern_container.hpp:94), dtype/component mismatch */
+#define GHEXB_ERR_RANGE 5        /* a halo box or index falls outside the wrapped memory */
+#define GHEXB_ERR_ALLOC 6        /* device or host allocation failed */
+#define GHEXB_ERR_INTERNAL 7
+
+/* ---- element types (bitwise copies; negation/addition only for float types) ---------- */
+#define GHEXB_F32 0
+#define GHEXB_F64 1
+#define GHEXB_I32 2
+#define GHEXB_I64 3
+#define GHEXB_U8 4
+#define GHEXB_U16 5
+
+/* ---- exchange forms for ghexb_plan_launch -------------------------------------------- */
+#define GHEXB_FORM_BATCHED 0   /* one kernel walks the whole descriptor table */
+#define GHEXB_FORM_PER_FIELD 1 /* one kernel launch per field */
+#define GHEXB_FORM_PER_BOX 2   /* one kernel launch per field per iteration space, the launch
+                                  granularity of serialization<gpu>::pack/unpack
+                                  (structured/pack_kernels.hpp:196-215) */
+
+typedef struct ghexb_context_s* ghexb_context;
+typedef struct ghexb_pattern_s* ghexb_pattern;
+typedef struct ghexb_field_s* ghexb_field; /* a field bound to a pattern: GHEX's buffer_info */
+typedef struct ghexb_co_s* ghexb_co;
+typedef struct ghexb_handle_s* ghexb_handle;
+typedef struct ghexb_plan_s* ghexb_plan;
+
+typedef struct ghexb_plan_info_t
+{
+    int64_t num_fields;        /* fields given to the plan */
+    int64_t num_descriptors;   /* box or index-list work descriptors */
+    int64_t num_tiles;         /* tiles of the batched kernel */
+    int64_t halo_elements;     /* halo elements written per exchange */
+    int64_t algorithmic_bytes; /* sum over halo elements of sizeof(T) * (1 read + 1 write) */
+    int64_t index_bytes;       /* bytes of index lists read per exchange (unstructured) */
+    int64_t adjoint_phases;    /* conflict-free phases of the adjoint */
+    int32_t tile_elems;        /* current tuning: elements per tile */
+    int32_t block;             /* current tuning: threads per CTA */
+    int32_t ctas_per_sm;       /* current tuning: resident CTAs per SM for the persistent grid */
+    int32_t grid;              /* CTAs of the batched launch */
+} ghexb_plan_info_t;
+
+/* ---- errors / version ----------------------------------------------------------------- */
+int ghexb_last_error(char* buf, size_t len);
+int ghexb_version(int* major, int* minor, int* patch);
+
+/* ---- context: replaces ghex::context(MPI_Comm, bool) (context.hpp:20-35, src/context.cpp:14-19).
+ * One process owns all domains of the exchange, so no communicator is taken; `device`
+ * selects the CUDA device whose memory the fields live in. */
+int ghexb_context_create(int device, ghexb_context* out);
+int ghexb_context_destroy(ghexb_context ctx);
+
+/* ---- patterns: replace ghex::make_pattern<Grid>(ctx, halo_gen, domains)
+ * (pattern_container.hpp:112-146) ------------------------------------------------------ */
+
+/* Regular structured grid: structured::regular::halo_generator(g_first, g_last, halos, periodic)
+ * (structured/regular/halo_generator.hpp:68-78) and domain_descriptor(id, first, last)
+ * (structured/regular/domain_descriptor.hpp:248-254). dim in 1..3; halos holds 2*dim values
+ * (dim0-, dim0+, dim1-, ...); domain_first/last hold n_domains*dim inclusive global coords. */
+int ghexb_pattern_create_regular(ghexb_context ctx, int dim, const int* g_first, const int* g_last,
+    const int* halos, const int* periodic, int n_domains, const int64_t* domain_ids,
+    const int* domain_first, const int* domain_last, ghexb_pattern* out);
+
+/* Cubed sphere: cubed_sphere::halo_generator(halos) (structured/cubed_sphere/halo_generator.hpp:59-71)
+ * and domain_descriptor(cube{edge_size, levels}, tile, x_first, x_last, y_first, y_last)
+ * (structured/cubed_sphere/domain_descriptor.hpp:92-104). halos holds 4 values in the order of
+ * the reference's m_halo array: [0] -x, [1] +x, [2] -y, [3] +y. Domain ids are (tile, x_first,
+ * y_first); ghexb_field_wrap addresses a cubed-sphere domain by its index in this list. */
+int ghexb_pattern_create_cubed_sphere(ghexb_context ctx, int edge_size, int levels,
+    const int* halos, int n_domains, const int* tiles, const int* x_first, const int* x_last,
+    const int* y_first, const int* y_last, ghexb_pattern* out);
+
+/* Unstructured: unstructured::domain_descriptor(id, gids, outer_lids)
+ * (unstructured/user_concepts.hpp:145-174) and halo_generator() / halo_generator(gids)
+ * (user_concepts.hpp:232-255), pattern set-up of unstructured/pattern.hpp:187-370.
+ * Domain k owns gids[gid_offsets[k] .. gid_offsets[k+1]) in storage order and its outer
+ * (halo) local ids outer_lids[outer_offsets[k] .. outer_offsets[k+1]). If halo_gid_offsets is
+ * NULL every outer gid is a halo (halo_generator()); otherwise domain k's halo is the gid list
+ * halo_gids[halo_gid_offsets[k] .. halo_gid_offsets[k+1]) (halo_generator(gids)). */
+int ghexb_pattern_create_unstructured(ghexb_context ctx, int n_domains, const int64_t* domain_ids,
+    const int64_t* gid_offsets, const int64_t* gids, const int64_t* outer_offsets,
+    const int64_t* outer_lids, const int64_t* halo_gid_offsets, const int64_t* halo_gids,
+    ghexb_pattern* out);
+
+int ghexb_pattern_destroy(ghexb_pattern p);
+
+/* Introspection, mirroring pattern::recv_halos()/send_halos() (structured/pattern.hpp:184-187). */
+int ghexb_pattern_num_domains(ghexb_pattern p, int* n);
+int ghexb_pattern_domain_id(ghexb_pattern p, int domain_index, int64_t* id);
+int ghexb_pattern_max_tag(ghexb_pattern p, int* max_tag);
+/* Number of (neighbour, iteration space) entries received (send==0) or sent (send==1) by a domain. */
+int ghexb_pattern_num_spaces(ghexb_pattern p, int domain_index, int send, int* n);
+/* Structured entry k: neighbour domain index, local first/last and global first/last, 4 ints each
+ * (regular: x,y,z padded with 0; cubed sphere: tile,x,y,z as in the reference). */
+int ghexb_pattern_space(ghexb_pattern p, int domain_index, int send, int k, int* neighbor_index,
+    int* local_first, int* local_last, int* global_first, int* global_last);
+/* Unstructured entry k: neighbour domain index and its local-index list (receiver's halo order). */
+int ghexb_pattern_space_indices(ghexb_pattern p, int domain_index, int send, int k,
+    int* neighbor_index, int64_t* lids, int64_t capacity, int64_t* count);
+
+/* ---- fields bound to a pattern: replace wrap_field<Arch, Layout>(dom, data, offsets, extents
+ * [, strides], device) (structured/regular/field_descriptor.hpp:167-194),
+ * cubed_sphere::field_descriptor(dom, data, offsets, extents, ncomp, is_vector)
+ * (structured/cubed_sphere/field_descriptor.hpp:113-121) and pattern(field) -> buffer_info
+ * (pattern_container.hpp:88-95).
+ * ndim: domain dimension, plus one trailing component dimension when num_components > 1
+ * (regular) — cubed-sphere fields are always (x, y, z, c).
+ * layout_map: ndim ints, gridtools convention (the largest value has stride 1); NULL means
+ * x fastest, i.e. {ndim-1, ..., 0}.
+ * byte_strides: NULL to derive strides from layout_map and extents (field_utils.hpp:92-111).
+ * domain: the domain id (regular) or the domain's index (cubed sphere). */
+int ghexb_field_wrap(ghexb_pattern p, int64_t domain, int dtype, void* data, int ndim,
+    const int* offsets, const int* extents, const int* layout_map, const int64_t* byte_strides,
+    int num_components, int is_vector, ghexb_field* out);
+
+/* Replaces unstructured::data_descriptor<gpu,...>(dom, field, levels, levels_first, outer_stride)
+ * (unstructured/user_concepts.hpp:524-535). outer_stride 0 means no padding. */
+int ghexb_field_wrap_unstructured(ghexb_pattern p, int64_t domain_id, int dtype, void* data,
+    int64_t levels, int levels_first, int64_t outer_stride, ghexb_field* out);
+
+int ghexb_field_destroy(ghexb_field f);
+
+/* ---- communication object: replaces make_communication_object<Pattern>(ctx)
+ * (communication_object.hpp:653-660), exchange(buffer_info...) (:233-240) and
+ * communication_handle::wait/is_ready (:627-640). The exchange of the given fields is ordered on
+ * `stream` (NULL = legacy default stream); wait() blocks the host until it has completed,
+ * like the reference's wait() (:503-512). A second exchange before wait() fails with
+ * GHEXB_ERR_BUSY. Fields of the same pattern are matched across domains by their order in
+ * `fields`: the k-th field given for domain a pairs with the k-th field given for domain b. */
+int ghexb_co_create(ghexb_context ctx, ghexb_co* out);
+int ghexb_co_destroy(ghexb_co co);
+int ghexb_co_exchange(
+    ghexb_co co, const ghexb_field* fields, int n, void* stream, ghexb_handle* out);
+int ghexb_handle_wait(ghexb_handle h);
+int ghexb_handle_is_ready(ghexb_handle h, int* ready);
+int ghexb_handle_destroy(ghexb_handle h);
+
+/* ---- explicit plans: the work-descriptor table of one field set, built once and reused.
+ * No reference counterpart: GHEX rebuilds its message layout on every exchange
+ * (communication_object.hpp:536-624). */
+int ghexb_plan_create(ghexb_context ctx, const ghexb_field* fields, int n, ghexb_plan* out);
+int ghexb_plan_destroy(ghexb_plan plan);
+/* Host-only validation, no device needed: builds the plan's tables and replays the address
+ * computation of every element the forward and adjoint kernels touch, failing with
+ * GHEXB_ERR_RANGE if one falls outside its field's memory span. */
+int ghexb_plan_check(ghexb_context ctx, const ghexb_field* fields, int n, int64_t* elements_checked);
+int ghexb_plan_get_info(ghexb_plan plan, ghexb_plan_info_t* info);
+/* tile_elems/block/ctas_per_sm <= 0 keep the current value. Invalidates the captured graph. */
+int ghexb_plan_set_tuning(ghexb_plan plan, int tile_elems, int block, int ctas_per_sm);
+/* One forward exchange in the given form, stream-ordered. */
+int ghexb_plan_launch(ghexb_plan plan, int form, void* stream);
+/* The batched form captured once into a CUDA graph and replayed on `stream`. */
+int ghexb_plan_graph_launch(ghexb_plan plan, void* stream);
+/* Adjoint of the exchange: every halo value is added into the interior value it was copied
+ * from (negated where the forward negated it), in a fixed order, then the halo is zeroed.
+ * Float fields only. */
+int ghexb_plan_adjoint_launch(ghexb_plan plan, void* stream);
+/* Times the candidate tilings on `stream` with CUDA events and keeps the fastest one; the
+ * chosen tuning is returned through `info` when it is not NULL. Runs real exchanges. */
+int ghexb_plan_autotune(ghexb_plan plan, void* stream, int repeats, ghexb_plan_info_t* info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GHEX_B200_H */

@@ -1,0 +1,103 @@
+"""Known-answer cases of the reference's regular-grid tests, shared by the oracle tests (CPU) and the
+GPU parity tests.
+
+* simple_2d: test/structured/regular/test_simple_regular_domain.cpp:38-140 — 2-D, 8 domains of
+  DIM x DIM/2 cells (DIM = 8) laid out as in make_domain (:162-168) for a 2x2 process grid with
+  two domains per process, halo HALO = 3, element = the global (x, y) pair of the cell; after the
+  exchange every halo cell holds the coordinate of its periodic owner, or (-1, -1) outside a
+  non-periodic boundary (expected/compare/check, :97-140).
+* owner check (cfg0-style): every halo cell equals the value of the cell it wraps to, NaN beyond a
+  non-periodic boundary.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+DIM, HALO = 8, 3
+
+
+def simple_2d_domains():
+    """(id, first, last) of the 8 domains: ranks on a 2x2 grid, 2 domains each (:162-168)."""
+    doms = []
+    dims = (2, 2)
+    for rank in range(4):
+        cx, cy = divmod(rank, dims[1])  # MPI cartesian coordinates: the last one varies fastest
+        for i in range(2):
+            x = cx * DIM
+            y = (cy * 2 + i) * (DIM // 2)
+            doms.append((rank * 2 + i, (x, y), (x + DIM - 1, y + DIM // 2 - 1)))
+    return doms
+
+
+def simple_2d_fields(doms):
+    """Fields of (x, y) int32 pairs, -1 outside the interior; shape (DIM+2H, DIM/2+2H, 2)."""
+    out = []
+    for _, first, _ in doms:
+        a = np.full((DIM + 2 * HALO, DIM // 2 + 2 * HALO, 2), -1, dtype=np.int32)
+        xs = np.arange(DIM) + first[0]
+        ys = np.arange(DIM // 2) + first[1]
+        a[HALO:HALO + DIM, HALO:HALO + DIM // 2, 0] = xs[:, None]
+        a[HALO:HALO + DIM, HALO:HALO + DIM // 2, 1] = ys[None, :]
+        out.append(a)
+    return out
+
+
+def _expected(coord, dim, first, last, periodic):
+    """expected() of the reference test (:97-105)."""
+    ext = last + 1 - first
+    res = first + coord
+    if first == 0 and coord < 0:
+        res = dim * DIM + coord if periodic else -1
+    if last == dim * DIM - 1 and coord >= ext:
+        res = coord - ext if periodic else -1
+    return res
+
+
+def simple_2d_check(a, first, last, periodic, dims=(2, 2)):
+    """check() of the reference test (:118-134): returns the list of mismatching cells."""
+    bad = []
+    for j in range(-HALO, DIM // 2 + HALO):
+        y = _expected(j, dims[1], first[1], last[1], periodic[1])
+        for i in range(-HALO, DIM + HALO):
+            x = _expected(i, dims[0], first[0], last[0], periodic[0])
+            ex, ey = (-1, -1) if (x == -1 or y == -1) else (x, y)
+            v = a[i + HALO, j + HALO]
+            if (int(v[0]), int(v[1])) != (ex, ey):
+                bad.append(((i, j), (int(v[0]), int(v[1])), (ex, ey)))
+    return bad
+
+
+def owner_check(w, arrays, spec):
+    """Every halo cell of every domain equals the value at its (periodically wrapped) owner
+    coordinate, or NaN where no owner exists. Returns the number of mismatching cells."""
+    dim = w.dim
+    glob = {}
+    off = w.offsets(spec)
+    for (i, first, last), a in zip(w.domains, arrays):
+        glob[i] = (first, last, a)
+    bad = 0
+    for (i, first, last), a in zip(w.domains, arrays):
+        ext = a.shape[:dim]
+        grids = np.meshgrid(*[np.arange(ext[k]) - off[k] + first[k] for k in range(dim)], indexing="ij")
+        owner_vals = np.full(ext, np.nan, dtype=a.dtype)
+        valid = np.ones(ext, dtype=bool)
+        g = []
+        for k in range(dim):
+            c = grids[k]
+            if w.periodic[k]:
+                c = np.mod(c, w.shape[k])
+            else:
+                valid &= (c >= 0) & (c < w.shape[k])
+            g.append(c)
+        for j, (f2, l2, b) in glob.items():
+            inside = valid.copy()
+            for k in range(dim):
+                inside &= (g[k] >= f2[k]) & (g[k] <= l2[k])
+            if not inside.any():
+                continue
+            idx = tuple(g[k][inside] - f2[k] + off[k] for k in range(dim))
+            owner_vals[inside] = b[idx]
+        # compare bit patterns (NaN-aware)
+        u = np.dtype(f"u{a.itemsize}")
+        bad += int(np.count_nonzero(owner_vals.view(u) != np.ascontiguousarray(a).view(u)))
+    return bad

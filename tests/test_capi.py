@@ -1,0 +1,84 @@
+"""The C ABI library loads, exports every symbol include/ghex_b200.h declares, and reports errors
+through status codes (no GPU needed)."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+from ghex_b200 import _capi
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "ghex_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^int (ghexb_\w+)\(", text, flags=re.M)))
+
+
+def test_header_declares_functions():
+    names = declared_functions()
+    assert len(names) >= 30
+    assert "ghexb_co_exchange" in names and "ghexb_handle_wait" in names
+
+
+@pytest.mark.parametrize("name", declared_functions())
+def test_symbol_exported(name):
+    assert hasattr(_capi.lib, name), f"{name} is declared but not exported"
+    assert name in _capi.SIGNATURES, f"{name} has no ctypes signature"
+
+
+def test_version_and_errors():
+    a, b, c = C.c_int(), C.c_int(), C.c_int()
+    _capi.call("ghexb_version", C.byref(a), C.byref(b), C.byref(c))
+    assert (a.value, b.value) == (0, 1)
+    rc = _capi.lib.ghexb_version(None, None, None)
+    assert rc == _capi.ERR_INVALID
+    assert "null" in _capi.last_error()
+
+
+def test_context_without_device_and_bad_pattern():
+    h = C.c_void_p()
+    _capi.call("ghexb_context_create", 0, C.byref(h))
+    try:
+        p = C.c_void_p()
+        # empty domain
+        rc = _capi.lib.ghexb_pattern_create_regular(
+            h, 1, _capi.int_array([0]), _capi.int_array([9]), _capi.int_array([1, 1]), _capi.int_array([1]), 1,
+            _capi.int64_array([0]), _capi.int_array([5]), _capi.int_array([4]), C.byref(p))
+        assert rc == _capi.ERR_INVALID
+        assert "empty" in _capi.last_error()
+        # repeated ids
+        rc = _capi.lib.ghexb_pattern_create_regular(
+            h, 1, _capi.int_array([0]), _capi.int_array([9]), _capi.int_array([1, 1]), _capi.int_array([1]), 2,
+            _capi.int64_array([3, 3]), _capi.int_array([0, 5]), _capi.int_array([4, 9]), C.byref(p))
+        assert rc == _capi.ERR_INVALID
+        assert "repeated" in _capi.last_error()
+    finally:
+        _capi.lib.ghexb_context_destroy(h)
+
+
+def test_field_wrap_checks():
+    from ghex_b200.structured import regular as R
+    ctx = R.make_context(device=0)
+    hg = R.HaloGenerator(((0,), (9,)), (1,), (True,))
+    p = R.make_pattern(ctx, hg, [R.DomainDescriptor(0, ((0,), (4,))), R.DomainDescriptor(1, ((5,), (9,)))])
+    f = C.c_void_p()
+    # unknown domain id
+    rc = _capi.lib.ghexb_field_wrap(p._h, 7, _capi.F64, C.c_void_p(4096), 1, _capi.int_array([1]),
+                                    _capi.int_array([7]), None, None, 1, 0, C.byref(f))
+    assert rc == _capi.ERR_INCOMPATIBLE
+    assert "incompatible" in _capi.last_error()
+    # misaligned pointer
+    rc = _capi.lib.ghexb_field_wrap(p._h, 0, _capi.F64, C.c_void_p(4100), 1, _capi.int_array([1]),
+                                    _capi.int_array([7]), None, None, 1, 0, C.byref(f))
+    assert rc == _capi.ERR_INVALID
+    # components on a field without a component dimension
+    rc = _capi.lib.ghexb_field_wrap(p._h, 0, _capi.F64, C.c_void_p(4096), 1, _capi.int_array([1]),
+                                    _capi.int_array([7]), None, None, 3, 0, C.byref(f))
+    assert rc == _capi.ERR_INVALID
+    assert "components" in _capi.last_error()
+    # a valid wrap needs no device
+    _capi.call("ghexb_field_wrap", p._h, 0, _capi.F64, C.c_void_p(4096), 1, _capi.int_array([1]),
+               _capi.int_array([7]), None, None, 1, 0, C.byref(f))
+    _capi.lib.ghexb_field_destroy(f)

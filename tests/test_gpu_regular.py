@@ -1,0 +1,123 @@
+"""GPU parity of the regular structured exchange: bit-exact against the oracle, through the C ABI."""
+import numpy as np
+import pytest
+import torch
+
+from ghex_b200 import _capi
+from ghex_b200 import workloads as W
+from ghex_b200.structured import regular as R
+from gpu_helpers import RegularRun, bits_equal, to_device
+from regular_cases import DIM, HALO, simple_2d_check, simple_2d_domains, simple_2d_fields
+
+pytestmark = pytest.mark.gpu
+
+
+def test_cfg0_exchange_bitexact(cuda):
+    run = RegularRun(W.config0(), cuda)
+    expected = run.oracle()
+    co = R.make_communication_object(run.ctx)
+    co.exchange(run.bis).wait()
+    assert run.mismatches(expected) == {}
+
+
+@pytest.mark.parametrize("form", ["batched", "per_field", "per_box", "graph"])
+def test_cfg1_small_all_forms_bitexact(cuda, form):
+    run = RegularRun(W.config1(shape=(60, 45, 15)), cuda)
+    expected = run.oracle()
+    plan = R.make_exchange_plan(run.ctx, run.bis)
+    if form == "graph":
+        plan.graph_launch()
+    else:
+        plan.launch({"batched": plan.BATCHED, "per_field": plan.PER_FIELD, "per_box": plan.PER_BOX}[form])
+    assert run.mismatches(expected) == {}
+    info = plan.info()
+    assert info["num_fields"] == 5 * 27
+
+
+def test_cfg1_full_size_bitexact(cuda):
+    w = W.config1()
+    run = RegularRun(w, cuda)
+    expected = run.oracle()
+    co = R.make_communication_object(run.ctx)
+    for _ in range(2):  # second exchange reuses the cached plan and graph
+        co.exchange(run.bis).wait()
+    assert run.mismatches(expected) == {}
+    plan = R.make_exchange_plan(run.ctx, run.bis)
+    info = plan.info()
+    # algorithmic bytes = sum over written halo cells of sizeof(T) * 2
+    n64 = sum(int(np.count_nonzero(~np.isnan(e) & np.isnan(h))) for e, h in zip(expected["f64_0"], run.host["f64_0"]))
+    n32 = sum(int(np.count_nonzero(~np.isnan(e) & np.isnan(h))) for e, h in zip(expected["f32_0"], run.host["f32_0"]))
+    assert info["algorithmic_bytes"] == 3 * n64 * 16 + 2 * n32 * 8
+
+
+@pytest.mark.parametrize("tile,block,cps", [(64, 32, 1), (1000, 128, 3), (1 << 20, 512, 2)])
+def test_tunings_bitexact(cuda, tile, block, cps):
+    run = RegularRun(W.config1(shape=(50, 40, 12)), cuda)
+    expected = run.oracle()
+    plan = R.make_exchange_plan(run.ctx, run.bis)
+    plan.set_tuning(tile, block, cps)
+    plan.launch()
+    assert run.mismatches(expected) == {}
+
+
+def test_autotune_then_bitexact(cuda):
+    run = RegularRun(W.config1(shape=(80, 60, 24)), cuda)
+    expected = run.oracle()
+    plan = R.make_exchange_plan(run.ctx, run.bis)
+    info = plan.autotune(repeats=2)
+    assert info["tile_elems"] > 0 and info["block"] in (128, 256, 512)
+    run.reset()
+    plan.graph_launch()
+    assert run.mismatches(expected) == {}
+
+
+@pytest.mark.parametrize("periodic", [(True, True), (False, True)])
+def test_simple_2d_known_answer(cuda, periodic):
+    """test_simple_regular_domain.cpp's check on the device: (x, y) int32 pairs, x fastest."""
+    doms = simple_2d_domains()
+    host = simple_2d_fields(doms)
+    ctx = R.make_context()
+    hg = R.HaloGenerator(((0, 0), (2 * DIM - 1, 4 * (DIM // 2) - 1)), (HALO, HALO), periodic)
+    dds = [R.DomainDescriptor(i, (f, l)) for i, f, l in doms]
+    pat = R.make_pattern(ctx, hg, dds)
+    tens, bis = [], []
+    for dd, a in zip(dds, host):
+        # memory order [y][x][pair] as the reference's layout_map<1,0> field of array<int,2>
+        buf = np.ascontiguousarray(a.transpose(1, 0, 2)).transpose(1, 0, 2)
+        t = to_device(buf, cuda)
+        tens.append(t)
+        fd = R.make_field_descriptor(dd, t, (HALO, HALO), (DIM + 2 * HALO, DIM // 2 + 2 * HALO))
+        bis.append(pat(fd))
+    co = R.make_communication_object(ctx)
+    co.exchange(bis).wait()
+    for (i, f, l), t in zip(doms, tens):
+        assert simple_2d_check(t.cpu().numpy(), f, l, periodic) == [], f"domain {i}"
+
+
+def test_busy_guard_and_errors(cuda):
+    run = RegularRun(W.config0(), cuda)
+    co = R.make_communication_object(run.ctx)
+    h = co.exchange(run.bis)
+    with pytest.raises(_capi.GhexError) as e:
+        co.exchange(run.bis)
+    assert e.value.code == _capi.ERR_BUSY and "not finished" in str(e.value)
+    h.wait()
+    co.exchange(run.bis).wait()
+    # a neighbour without a field in the exchange
+    with pytest.raises(_capi.GhexError) as e:
+        co.exchange(run.bis[:3]).wait()
+    assert e.value.code == _capi.ERR_INCOMPATIBLE
+
+
+def test_out_of_range_box_is_rejected(cuda):
+    w = W.config0()
+    ctx = R.make_context()
+    hg = R.HaloGenerator(((0, 0, 0), (63, 63, 63)), (2, 2, 2), (True, True, True))
+    doms = [R.DomainDescriptor(i, (f, l)) for i, f, l in w.domains]
+    pat = R.make_pattern(ctx, hg, doms)
+    # memory padded for halo 1 only: the halo-2 boxes do not fit
+    tens = [torch.zeros((34, 34, 34), dtype=torch.float64, device=cuda) for _ in doms]
+    bis = [pat(R.make_field_descriptor(d, t, (1, 1, 1), (34, 34, 34))) for d, t in zip(doms, tens)]
+    with pytest.raises(_capi.GhexError) as e:
+        R.make_exchange_plan(ctx, bis)
+    assert e.value.code == _capi.ERR_RANGE
