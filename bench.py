@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--baseline-seconds", type=float, default=10.0)
+    ap.add_argument("--profile", choices=["batched", "per_field", "adjoint"], default=None,
+                    help="only run `--steps` launches of one form after `--warmup` (for ncu captures)")
     return ap.parse_args()
 
 
@@ -231,6 +233,15 @@ def main():
             bis += [pat(R.make_field_descriptor(dm, t, w.offsets(s), w.extents(d, s)))
                     for dm, d, t in zip(doms, w.domains, tens[s.name])]
     plan = R.make_exchange_plan(ctx, bis)
+    if args.profile:
+        launch = {"batched": lambda: plan.launch(plan.BATCHED), "per_field": lambda: plan.launch(plan.PER_FIELD),
+                  "adjoint": lambda: plan.adjoint()}[args.profile]
+        for _ in range(args.warmup + args.steps):
+            launch()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": args.profile, "config": w.name, "launches": args.warmup + args.steps,
+                          "plan": plan.info()}), flush=True)
+        return
     tuning = plan.info() if args.no_autotune else plan.autotune(repeats=5)
     info = plan.info()
     alg = info["algorithmic_bytes"]

@@ -507,15 +507,15 @@ int ghexb_plan_get_info(ghexb_plan plan, ghexb_plan_info_t* info)
         require(plan && info, "null argument");
         info->num_fields = (int64_t)plan->fields.size();
         info->num_descriptors = (int64_t)(plan->boxes.size() + plan->lists.size());
-        info->num_tiles = (int64_t)plan->tiles.size();
+        info->num_tiles = plan->num_tiles();
         info->halo_elements = plan->halo_elements;
         info->algorithmic_bytes = plan->algorithmic_bytes;
         info->index_bytes = plan->index_bytes;
-        info->adjoint_phases = (int64_t)plan->phase_range.size();
+        info->adjoint_phases = (int64_t)plan->adj_bphase_range.size();
         info->tile_elems = plan->tile_elems;
         info->block = plan->block;
         info->ctas_per_sm = plan->ctas_per_sm;
-        info->grid = plan->grid((int)plan->tiles.size());
+        info->grid = plan->grid((int)plan->ftiles[0].size());
     });
 }
 

@@ -49,28 +49,49 @@ struct fast_div
     }
 };
 
-// Strided box copy: for every (i0,i1,i2,i3) < (n0,n1,n2,n3)
-//   dst[i0*d0 + i1*d1 + i2*d2 + i3*d3] = src[i0*s0 + i1*s1 + i2*s2 + i3*s3] ^ xor_mask
-// in units of `esize` bytes. i0 runs fastest and is the destination's contiguous dimension.
-// All offsets fit int32 (checked when the table is built).
+// How the lanes of a warp cover rows of n elements: W = 2^wlog lanes share a row (W is the next
+// power of two of n, at most 32), each taking j = ceil(n / W) elements, and a thread takes p rows
+// per pipeline chunk, so that p * j <= 8 elements per thread and chunk.
+struct row_map
+{
+    uint8_t wlog;
+    uint8_t j;
+    uint8_t p;
+    uint8_t pad;
+
+    static row_map make(int n)
+    {
+        row_map m{0, 1, 8, 0};
+        while ((1 << m.wlog) < n && m.wlog < 5) ++m.wlog;
+        m.j = (uint8_t)((n + (1 << m.wlog) - 1) >> m.wlog);
+        m.p = (uint8_t)(m.j > 8 ? 1 : 8 / m.j);
+        return m;
+    }
+};
+
+// Strided box copy, organised in rows: for every row r < n1 * n2 with (i1, i2) = (r mod n1, r / n1)
+// and every i0 < n0
+//   dst[i0*d0 + i1*d1 + i2*d2] = src[i0*s0 + i1*s1 + i2*s2] ^ xor_mask
+// in units of `esize` bytes. Dimension 0 is the destination's contiguous dimension and n0 <= 256
+// (longer rows are split into several descriptors). All offsets fit int32.
 struct alignas(16) box_desc
 {
     const char* src;
     char* dst;
-    int32_t n0, n1, n2, n3;
-    int32_t s0, s1, s2, s3;
-    int32_t d0, d1, d2, d3;
+    int32_t n0, n1, n2;
+    int32_t s0, s1, s2;
+    int32_t d0, d1, d2;
     uint32_t esize;     // bytes per element: 1, 2, 4 or 8
     uint32_t field;     // logical field the descriptor belongs to
+    row_map map;
     uint64_t xor_mask;  // sign-bit mask for negated vector components, else 0
-    fast_div div0, div1, div2;
-    uint32_t pad;
+    fast_div div1;      // divides a row index by n1
 };
 
-// Index-list copy of column data: for k < count, l < levels
+// Index-list copy of column data, organised in rows (columns): for k < count, l < levels
 //   dst[didx[k]*d_is + l*d_ls] = src[sidx[k]*s_is + l*s_ls]
-// in units of `unit` bytes (16 when every column is 16-byte aligned, else the element size).
-// If level_fastest, consecutive threads walk l, else k.
+// in units of `unit` bytes (16 when every column is 16-byte aligned, else the element size);
+// levels <= 256 units per descriptor.
 struct alignas(16) list_desc
 {
     const char* src;
@@ -81,12 +102,11 @@ struct alignas(16) list_desc
     int32_t levels; // in units
     int32_t s_is, s_ls, d_is, d_ls; // in units
     uint32_t unit;
-    uint32_t level_fastest;
     uint32_t field;
-    fast_div divq; // divides by levels (level_fastest) or by count
+    row_map map;
 };
 
-// A contiguous range [start, start+count) of one descriptor's flattened index space.
+// A contiguous range [start, start+count) of one descriptor's rows.
 struct alignas(16) tile
 {
     int32_t desc;

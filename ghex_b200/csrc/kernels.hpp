@@ -7,14 +7,22 @@
 
 namespace ghexb
 {
-// Forward exchange over tiles[0, ntiles): box and list descriptors, any element type.
-cudaError_t launch_exchange(const box_desc* boxes, const list_desc* lists, const tile* tiles,
-    int ntiles, int grid, int block, cudaStream_t stream);
+// Forward exchange over tiles[0, ntiles) of box descriptors (3-D boxes; `large`: elements of 8 and 4
+// bytes mixed freely, else of 2 and 1 bytes) and of list descriptors (`large`: units of 16 and 8
+// bytes, else of 4, 2 and 1 bytes). The large classes claim tiles dynamically through
+// counters[0..1] (zero before the launch, zero again after it); launches sharing counters must be
+// ordered on one stream.
+cudaError_t launch_box_exchange(const box_desc* boxes, const tile* tiles, int ntiles, bool large, unsigned* counters,
+    int grid, int block, cudaStream_t stream);
+cudaError_t launch_list_exchange(const list_desc* lists, const tile* tiles, int ntiles, bool large, unsigned* counters,
+    int grid, int block, cudaStream_t stream);
 
 // Adjoint over tiles[0, ntiles) whose owner elements are pairwise distinct:
 // owner += halo (owner -= halo for negated components); halo = 0. Float and double only.
-cudaError_t launch_adjoint(const box_desc* boxes, const list_desc* lists, const tile* tiles,
-    int ntiles, int grid, int block, cudaStream_t stream);
+cudaError_t launch_box_adjoint(const box_desc* boxes, const tile* tiles, int ntiles, unsigned* counters, int grid,
+    int block, cudaStream_t stream);
+cudaError_t launch_list_adjoint(const list_desc* lists, const tile* tiles, int ntiles, unsigned* counters, int grid,
+    int block, cudaStream_t stream);
 
 // Reads n16 16-byte words of `buf` so that the L2 holds clean lines of an unrelated buffer;
 // `sink` receives a value only when the data sum to a sentinel that a zero-filled buffer never

@@ -71,15 +71,15 @@ struct builder
         return f.byte_strides[a] / f.esize;
     }
 
-    // Emits a box descriptor from a list of axes (any order) and the element offsets of the
-    // box origin in source and destination.
+    // Emits box descriptors from a list of axes (any order) and the element offsets of the box
+    // origin in source and destination. Rows longer than 256 elements are split.
     void emit_box(const ghexb_field_s& src, int src_slot, const ghexb_field_s& dst, int dst_slot,
         std::vector<axis> ax, int64_t src_origin, int64_t dst_origin, uint64_t xor_mask,
         int logical, const owner_region& reg)
     {
         std::stable_sort(ax.begin(), ax.end(), [](const axis& a, const axis& b) { return a.order > b.order; });
-        while (ax.size() < 4) ax.push_back(axis{1, 0, 0, -1});
-        if (ax.size() > 4) throw error(GHEXB_ERR_INTERNAL, "box with more than 4 axes");
+        while (ax.size() < 3) ax.push_back(axis{1, 0, 0, -1});
+        if (ax.size() > 3) throw error(GHEXB_ERR_INTERNAL, "box descriptors are 3-dimensional");
         int64_t nelem = 1, sspan = 0, dspan = 0;
         for (const auto& a : ax)
         {
@@ -90,24 +90,27 @@ struct builder
         }
         if (nelem > k_i32max || sspan > k_i32max || dspan > k_i32max)
             throw error(GHEXB_ERR_RANGE, "a halo box spans more than 2^31 elements");
-        box_desc b{};
-        b.src = src.data + src_origin * src.esize;
-        b.dst = dst.data + dst_origin * dst.esize;
-        b.n0 = ax[0].n, b.n1 = ax[1].n, b.n2 = ax[2].n, b.n3 = ax[3].n;
-        b.s0 = (int32_t)ax[0].ss, b.s1 = (int32_t)ax[1].ss, b.s2 = (int32_t)ax[2].ss, b.s3 = (int32_t)ax[3].ss;
-        b.d0 = (int32_t)ax[0].ds, b.d1 = (int32_t)ax[1].ds, b.d2 = (int32_t)ax[2].ds, b.d3 = (int32_t)ax[3].ds;
-        b.esize = (uint32_t)dst.esize;
-        b.field = (uint32_t)logical;
-        b.xor_mask = xor_mask;
-        b.div0 = fast_div::make((uint32_t)b.n0);
-        b.div1 = fast_div::make((uint32_t)b.n1);
-        b.div2 = fast_div::make((uint32_t)b.n2);
-        plan.boxes.push_back(b);
-        plan.box_src_slot.push_back(src_slot);
-        plan.box_dst_slot.push_back(dst_slot);
-        owner_region r = reg;
-        r.field = src_slot;
-        box_owner.push_back(r);
+        constexpr int k_max_row = 256;
+        for (int x0 = 0; x0 < ax[0].n; x0 += k_max_row)
+        {
+            box_desc b{};
+            b.n0 = std::min(k_max_row, ax[0].n - x0);
+            b.src = src.data + (src_origin + x0 * ax[0].ss) * src.esize;
+            b.dst = dst.data + (dst_origin + x0 * ax[0].ds) * dst.esize;
+            b.n1 = ax[1].n, b.n2 = ax[2].n;
+            b.s0 = (int32_t)ax[0].ss, b.s1 = (int32_t)ax[1].ss, b.s2 = (int32_t)ax[2].ss;
+            b.d0 = (int32_t)ax[0].ds, b.d1 = (int32_t)ax[1].ds, b.d2 = (int32_t)ax[2].ds;
+            b.esize = (uint32_t)dst.esize;
+            b.field = (uint32_t)logical;
+            b.map = row_map::make(b.n0);
+            b.xor_mask = xor_mask;
+            b.div1 = fast_div::make((uint32_t)b.n1);
+            plan.boxes.push_back(b);
+            plan.box_src_slot.push_back(src_slot);
+            plan.box_dst_slot.push_back(dst_slot);
+            box_owner.push_back(reg);
+            box_owner.back().field = src_slot;
+        }
         plan.halo_elements += nelem;
         plan.algorithmic_bytes += nelem * dst.esize * 2;
     }
@@ -143,8 +146,15 @@ struct builder
         }
         if (dst.ndim == D + 1)
         {
-            ax.push_back(axis{dst.num_components, estride(src, D), estride(dst, D), dst.layout[D]});
-            reg.lo[D] = 0, reg.hi[D] = dst.num_components - 1;
+            // one descriptor per component: the kernels walk 3-D boxes
+            for (int c = 0; c < dst.num_components; ++c)
+            {
+                owner_region rc = reg;
+                rc.lo[D] = rc.hi[D] = c;
+                emit_box(src, src_slot, dst, dst_slot, ax, so + c * estride(src, D), dof + c * estride(dst, D), 0,
+                    logical, rc);
+            }
+            return;
         }
         emit_box(src, src_slot, dst, dst_slot, ax, so, dof, 0, logical, reg);
     }
@@ -208,14 +218,6 @@ struct builder
         const uint64_t sign = dst.esize == 8 ? (1ull << 63) : (1ull << 31);
         const bool neg0 = dst.is_vector && r[2] == -1;
         const bool neg1 = dst.is_vector && r[1] == -1;
-        if (!neg0 && !neg1)
-        {
-            auto ax2 = ax;
-            ax2.push_back(axis{nc, sC, estride(dst, 3), dst.layout[3]});
-            reg.hi[3] = nc - 1;
-            emit_box(src, src_slot, dst, dst_slot, ax2, src_origin, dst_origin, 0, logical, reg);
-            return;
-        }
         for (int comp = 0; comp < nc; ++comp)
         {
             const uint64_t xm = (comp == 0 && neg0) || (comp == 1 && neg1) ? sign : 0;
@@ -245,7 +247,8 @@ struct builder
         for (auto v : S) plan.idx.push_back((int32_t)v);
         for (auto v : R) plan.idx.push_back((int32_t)v);
 
-        // forward descriptor: 16-byte columns when every column is 16-byte aligned
+        // forward descriptors: 16-byte columns when every column is 16-byte aligned; columns of
+        // more than 256 units are split into level segments
         const bool cols = dst.level_stride == 1 && src.level_stride == 1;
         const bool vec16 = cols && (L * es) % 16 == 0 && (dst.index_stride * es) % 16 == 0 &&
                            (src.index_stride * es) % 16 == 0 &&
@@ -253,27 +256,31 @@ struct builder
                            reinterpret_cast<uintptr_t>(src.data) % 16 == 0;
         const int unit = vec16 ? 16 : es;
         const int64_t k = unit / es;
-        list_desc l{};
-        l.src = src.data;
-        l.dst = dst.data;
-        l.count = (int32_t)cnt;
-        l.levels = (int32_t)(L / k);
-        l.s_is = (int32_t)(src.index_stride / k);
-        l.s_ls = (int32_t)(vec16 ? 1 : src.level_stride);
-        l.d_is = (int32_t)(dst.index_stride / k);
-        l.d_ls = (int32_t)(vec16 ? 1 : dst.level_stride);
-        l.unit = (uint32_t)unit;
-        l.level_fastest = dst.level_stride == 1 ? 1u : 0u;
-        l.field = (uint32_t)logical;
-        l.divq = fast_div::make((uint32_t)(l.level_fastest ? l.levels : l.count));
-        const int64_t span_s = smax * (int64_t)l.s_is + (int64_t)(l.levels - 1) * l.s_ls;
-        const int64_t span_d = dmax * (int64_t)l.d_is + (int64_t)(l.levels - 1) * l.d_ls;
-        if (cnt * l.levels > k_i32max || span_s > k_i32max || span_d > k_i32max)
+        const int64_t levels_u = L / k;
+        const int64_t s_is = src.index_stride / k, d_is = dst.index_stride / k;
+        const int64_t s_ls = vec16 ? 1 : src.level_stride, d_ls = vec16 ? 1 : dst.level_stride;
+        const int64_t span_s = smax * s_is + (levels_u - 1) * s_ls;
+        const int64_t span_d = dmax * d_is + (levels_u - 1) * d_ls;
+        if (span_s > k_i32max || span_d > k_i32max)
             throw error(GHEXB_ERR_RANGE, "an index-list descriptor spans more than 2^31 elements");
-        plan.lists.push_back(l);
-        plan.list_idx_off.push_back(idx0);
-        plan.list_src_slot.push_back(src_slot);
-        plan.list_dst_slot.push_back(dst_slot);
+        constexpr int64_t k_max_row = 256;
+        for (int64_t l0 = 0; l0 < levels_u; l0 += k_max_row)
+        {
+            list_desc l{};
+            l.src = src.data + l0 * s_ls * unit;
+            l.dst = dst.data + l0 * d_ls * unit;
+            l.count = (int32_t)cnt;
+            l.levels = (int32_t)std::min(k_max_row, levels_u - l0);
+            l.s_is = (int32_t)s_is, l.s_ls = (int32_t)s_ls;
+            l.d_is = (int32_t)d_is, l.d_ls = (int32_t)d_ls;
+            l.unit = (uint32_t)unit;
+            l.field = (uint32_t)logical;
+            l.map = row_map::make(l.levels);
+            plan.lists.push_back(l);
+            plan.list_idx_off.push_back(idx0);
+            plan.list_src_slot.push_back(src_slot);
+            plan.list_dst_slot.push_back(dst_slot);
+        }
         plan.halo_elements += cnt * L;
         plan.algorithmic_bytes += cnt * L * es * 2;
         plan.index_bytes += cnt * 8;
@@ -286,49 +293,32 @@ struct builder
             std::unordered_map<int64_t, int> seen;
             int64_t e = b;
             while (e < cnt && seen.emplace(S[e], 1).second) ++e;
-            list_desc a{};
-            a.src = src.data;
-            a.dst = dst.data;
-            a.count = (int32_t)(e - b);
-            a.levels = (int32_t)L;
-            a.s_is = (int32_t)src.index_stride;
-            a.s_ls = (int32_t)src.level_stride;
-            a.d_is = (int32_t)dst.index_stride;
-            a.d_ls = (int32_t)dst.level_stride;
-            a.unit = (uint32_t)es;
-            a.level_fastest = dst.level_stride == 1 ? 1u : 0u;
-            a.field = (uint32_t)logical;
-            a.divq = fast_div::make((uint32_t)(a.level_fastest ? a.levels : a.count));
-            plan.adj_lists.push_back(a);
-            plan.adj_idx_off.push_back(idx0 + b);
-            plan.adj_didx_off.push_back(idx0 + cnt + b);
-            plan.adj_src_slot.push_back(src_slot);
-            plan.adj_dst_slot.push_back(dst_slot);
-            list_src_field.push_back(src_slot);
+            for (int64_t l0 = 0; l0 < L; l0 += k_max_row)
+            {
+                list_desc a{};
+                a.src = src.data + l0 * src.level_stride * es;
+                a.dst = dst.data + l0 * dst.level_stride * es;
+                a.count = (int32_t)(e - b);
+                a.levels = (int32_t)std::min(k_max_row, L - l0);
+                a.s_is = (int32_t)src.index_stride;
+                a.s_ls = (int32_t)src.level_stride;
+                a.d_is = (int32_t)dst.index_stride;
+                a.d_ls = (int32_t)dst.level_stride;
+                a.unit = (uint32_t)es;
+                a.field = (uint32_t)logical;
+                a.map = row_map::make(a.levels);
+                plan.adj_lists.push_back(a);
+                plan.adj_idx_off.push_back(idx0 + b);
+                plan.adj_didx_off.push_back(idx0 + cnt + b);
+                plan.adj_src_slot.push_back(src_slot);
+                plan.adj_dst_slot.push_back(dst_slot);
+                list_src_field.push_back(src_slot);
+            }
             b = e;
         }
     }
 };
 
-void make_tiles(const std::vector<box_desc>& boxes, const std::vector<list_desc>& lists,
-    const std::vector<int>& box_order, const std::vector<int>& list_order, int tile_elems,
-    std::vector<tile>& out)
-{
-    auto emit = [&](int desc, int kind, int64_t n) {
-        for (int64_t s = 0; s < n; s += tile_elems)
-            out.push_back(tile{desc, kind, (uint32_t)s, (uint32_t)std::min<int64_t>(tile_elems, n - s)});
-    };
-    for (int i : box_order)
-    {
-        const auto& b = boxes[i];
-        emit(i, 0, (int64_t)b.n0 * b.n1 * b.n2 * b.n3);
-    }
-    for (int i : list_order)
-    {
-        const auto& l = lists[i];
-        emit(i, 1, (int64_t)l.count * l.levels);
-    }
-}
 } // namespace
 
 void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* fields, int n)
@@ -490,6 +480,8 @@ void upload_plan(ghexb_plan_s& plan)
     }
     upload(plan.d_boxes, plan.boxes);
     upload(plan.d_lists, plan.lists);
+    // two scheduler counters per forward tile class and per adjoint kernel
+    upload(plan.d_counters, std::vector<unsigned>(2 * (ghexb_plan_s::k_classes + 2), 0u));
     upload(plan.d_adj_lists, plan.adj_lists);
     check_cuda(cudaStreamCreateWithFlags(&plan.cap_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     retile(plan);
@@ -534,44 +526,39 @@ int64_t check_tables(const ghexb_plan_s& plan)
         const auto& sf = plan.fields[plan.box_src_slot[i]];
         const auto& df = plan.fields[plan.box_dst_slot[i]];
         const int64_t ss = field_span(sf), ds = field_span(df);
-        const uint32_t n = (uint32_t)((int64_t)b.n0 * b.n1 * b.n2 * b.n3);
-        for (uint32_t f = 0; f < n; ++f)
+        if (b.n0 < 1 || b.n0 > 256 || b.map.j * (1 << b.map.wlog) < b.n0 || b.map.p * b.map.j > 8)
+            throw error(GHEXB_ERR_INTERNAL, "invalid row mapping");
+        const uint32_t rows = (uint32_t)((int64_t)b.n1 * b.n2);
+        for (uint32_t r = 0; r < rows; ++r)
         {
-            // the decomposition of box_tile / box_adjoint_tile in kernels.cu
-            const uint32_t q0 = b.div0.div(f);
-            const int32_t i0 = (int32_t)(f - q0 * (uint32_t)b.n0);
-            const uint32_t q1 = b.div1.div(q0);
-            const int32_t i1 = (int32_t)(q0 - q1 * (uint32_t)b.n1);
-            const uint32_t q2 = b.div2.div(q1);
-            const int32_t i2 = (int32_t)(q1 - q2 * (uint32_t)b.n2);
-            const int32_t i3 = (int32_t)q2;
-            if (i3 >= b.n3) throw error(GHEXB_ERR_INTERNAL, "box decomposition out of range");
-            check_offset(sf, b.src, (int64_t)i0 * b.s0 + (int64_t)i1 * b.s1 + (int64_t)i2 * b.s2 + (int64_t)i3 * b.s3, ss, "source");
-            check_offset(df, b.dst, (int64_t)i0 * b.d0 + (int64_t)i1 * b.d1 + (int64_t)i2 * b.d2 + (int64_t)i3 * b.d3, ds, "destination");
+            // the row decomposition of box_issue / box_drain / box_adjoint_rows in kernels.cu
+            const uint32_t q = b.div1.div(r);
+            const int64_t i1 = (int64_t)(r - q * (uint32_t)b.n1), i2 = q;
+            if (i1 >= b.n1 || i2 >= b.n2) throw error(GHEXB_ERR_INTERNAL, "box decomposition out of range");
+            for (int i0 = 0; i0 < b.n0; ++i0)
+            {
+                check_offset(sf, b.src, i0 * (int64_t)b.s0 + i1 * b.s1 + i2 * b.s2, ss, "source");
+                check_offset(df, b.dst, i0 * (int64_t)b.d0 + i1 * b.d1 + i2 * b.d2, ds, "destination");
+            }
         }
-        checked += n;
+        checked += (int64_t)rows * b.n0;
     }
     auto check_list = [&](const list_desc& l, int64_t s_off, int64_t d_off, const ghexb_field_s& sf,
                           const ghexb_field_s& df) {
         const int64_t k = l.unit / sf.esize; // elements per unit
         const int64_t ss = field_span(sf), ds = field_span(df);
-        const uint32_t n = (uint32_t)((int64_t)l.count * l.levels);
-        for (uint32_t f = 0; f < n; ++f)
-        {
-            const uint32_t q = l.divq.div(f);
-            int32_t col, lev;
-            if (l.level_fastest) col = (int32_t)q, lev = (int32_t)(f - q * (uint32_t)l.levels);
-            else
-                lev = (int32_t)q, col = (int32_t)(f - q * (uint32_t)l.count);
-            if (col >= l.count || lev >= l.levels) throw error(GHEXB_ERR_INTERNAL, "list decomposition out of range");
-            const int64_t so = ((int64_t)plan.idx[s_off + col] * l.s_is + (int64_t)lev * l.s_ls) * k;
-            const int64_t dof = ((int64_t)plan.idx[d_off + col] * l.d_is + (int64_t)lev * l.d_ls) * k;
-            check_offset(sf, l.src, so, ss, "source");
-            check_offset(sf, l.src, so + k - 1, ss, "source");
-            check_offset(df, l.dst, dof, ds, "destination");
-            check_offset(df, l.dst, dof + k - 1, ds, "destination");
-        }
-        return (int64_t)n;
+        if (l.levels < 1 || l.levels > 256) throw error(GHEXB_ERR_INTERNAL, "invalid list descriptor");
+        for (int32_t col = 0; col < l.count; ++col)
+            for (int32_t lev = 0; lev < l.levels; ++lev)
+            {
+                const int64_t so = ((int64_t)plan.idx[s_off + col] * l.s_is + (int64_t)lev * l.s_ls) * k;
+                const int64_t dof = ((int64_t)plan.idx[d_off + col] * l.d_is + (int64_t)lev * l.d_ls) * k;
+                check_offset(sf, l.src, so, ss, "source");
+                check_offset(sf, l.src, so + k - 1, ss, "source");
+                check_offset(df, l.dst, dof, ds, "destination");
+                check_offset(df, l.dst, dof + k - 1, ds, "destination");
+            }
+        return (int64_t)l.count * l.levels;
     };
     for (size_t i = 0; i < plan.lists.size(); ++i)
         checked += check_list(plan.lists[i], plan.list_idx_off[i], plan.list_idx_off[i] + plan.lists[i].count,
@@ -585,48 +572,94 @@ int64_t check_tables(const ghexb_plan_s& plan)
 void retile(ghexb_plan_s& plan)
 {
     release_graph(plan);
-    // forward: grouped by logical field
-    plan.tiles.clear();
-    plan.logical_range.assign(plan.n_logical, {0, 0});
-    plan.desc_range.assign(plan.boxes.size() + plan.lists.size(), {0, 0});
-    for (int lg = 0; lg < plan.n_logical; ++lg)
+    // Tiles are row ranges. A tile holds about tile_elems elements, fewer for short rows: a row of
+    // n0 elements touches at least one 32-byte sector, so the cost per element grows as rows
+    // shrink below 256 bytes.
+    auto box_rows = [&](int i) { return (int64_t)plan.boxes[i].n1 * plan.boxes[i].n2; };
+    auto box_len = [&](int i) {
+        const auto& b = plan.boxes[i];
+        const int64_t rb = std::min<int64_t>(std::max<int64_t>((int64_t)b.n0 * b.esize, 32), 256);
+        const int64_t elems = std::max<int64_t>(256, plan.tile_elems * rb / 256);
+        return std::max<int64_t>(1, elems / b.n0);
+    };
+    auto list_len = [&](const list_desc& l) { return std::max<int64_t>(1, plan.tile_elems / l.levels); };
+    auto box_class = [&](int i) { return plan.boxes[i].esize >= 4 ? 0 : 1; };
+    auto list_class = [&](int i) { return plan.lists[i].unit >= 8 ? 2 : 3; };
+    auto split = [&](int desc, int kind, int64_t rows, int64_t len, std::vector<tile>& out) {
+        for (int64_t st = 0; st < rows; st += len)
+            out.push_back(tile{desc, kind, (uint32_t)st, (uint32_t)std::min<int64_t>(len, rows - st)});
+    };
+    // the batched table hands out the most expensive descriptors (shortest rows) first
+    std::vector<int> box_order(plan.boxes.size());
+    for (size_t i = 0; i < box_order.size(); ++i) box_order[i] = (int)i;
+    std::stable_sort(box_order.begin(), box_order.end(), [&](int a, int b) {
+        return (int64_t)plan.boxes[a].n0 * plan.boxes[a].esize < (int64_t)plan.boxes[b].n0 * plan.boxes[b].esize;
+    });
+    plan.box_range.assign(plan.boxes.size(), {0, 0});
+    plan.list_range.assign(plan.lists.size(), {0, 0});
+    for (int c = 0; c < ghexb_plan_s::k_classes; ++c)
     {
-        const int begin = (int)plan.tiles.size();
-        for (int i = 0; i < (int)plan.boxes.size(); ++i)
+        auto& F = plan.ftiles[c];
+        auto& P = plan.ptiles[c];
+        F.clear();
+        P.clear();
+        plan.logical_range[c].assign(plan.n_logical, {0, 0});
+        if (c < 2)
         {
-            if ((int)plan.boxes[i].field != lg) continue;
-            const int b0 = (int)plan.tiles.size();
-            make_tiles(plan.boxes, plan.lists, {i}, {}, plan.tile_elems, plan.tiles);
-            plan.desc_range[i] = {b0, (int)plan.tiles.size() - b0};
+            for (int i : box_order)
+                if (box_class(i) == c) split(i, 0, box_rows(i), box_len(i), F);
         }
-        for (int i = 0; i < (int)plan.lists.size(); ++i)
+        else
+            for (int i = 0; i < (int)plan.lists.size(); ++i)
+                if (list_class(i) == c) split(i, 1, plan.lists[i].count, list_len(plan.lists[i]), F);
+        for (int lg = 0; lg < plan.n_logical; ++lg)
         {
-            if ((int)plan.lists[i].field != lg) continue;
-            const int b0 = (int)plan.tiles.size();
-            make_tiles(plan.boxes, plan.lists, {}, {i}, plan.tile_elems, plan.tiles);
-            plan.desc_range[plan.boxes.size() + i] = {b0, (int)plan.tiles.size() - b0};
+            const int begin = (int)P.size();
+            if (c < 2)
+                for (int i : box_order)
+                {
+                    if ((int)plan.boxes[i].field != lg || box_class(i) != c) continue;
+                    const int b0 = (int)P.size();
+                    split(i, 0, box_rows(i), box_len(i), P);
+                    plan.box_range[i] = {b0, (int)P.size() - b0};
+                }
+            else
+                for (int i = 0; i < (int)plan.lists.size(); ++i)
+                {
+                    if ((int)plan.lists[i].field != lg || list_class(i) != c) continue;
+                    const int b0 = (int)P.size();
+                    split(i, 1, plan.lists[i].count, list_len(plan.lists[i]), P);
+                    plan.list_range[i] = {b0, (int)P.size() - b0};
+                }
+            plan.logical_range[c][lg] = {begin, (int)P.size() - begin};
         }
-        plan.logical_range[lg] = {begin, (int)plan.tiles.size() - begin};
     }
     // adjoint: grouped by phase
-    plan.adj_tiles.clear();
-    plan.phase_range.clear();
+    plan.adj_btiles.clear();
+    plan.adj_ltiles.clear();
+    plan.adj_bphase_range.clear();
+    plan.adj_lphase_range.clear();
     int nph = 0;
     for (int p : plan.box_phase) nph = std::max(nph, p + 1);
     for (int p : plan.list_phase) nph = std::max(nph, p + 1);
     for (int ph = 0; ph < nph; ++ph)
     {
-        const int begin = (int)plan.adj_tiles.size();
-        std::vector<int> bo, lo;
-        for (int i = 0; i < (int)plan.boxes.size(); ++i)
-            if (plan.box_phase[i] == ph) bo.push_back(i);
+        int begin = (int)plan.adj_btiles.size();
+        for (int i : box_order)
+            if (plan.box_phase[i] == ph) split(i, 0, box_rows(i), box_len(i), plan.adj_btiles);
+        plan.adj_bphase_range.push_back({begin, (int)plan.adj_btiles.size() - begin});
+        begin = (int)plan.adj_ltiles.size();
         for (int i = 0; i < (int)plan.adj_lists.size(); ++i)
-            if (plan.list_phase[i] == ph) lo.push_back(i);
-        make_tiles(plan.boxes, plan.adj_lists, bo, lo, plan.tile_elems, plan.adj_tiles);
-        plan.phase_range.push_back({begin, (int)plan.adj_tiles.size() - begin});
+            if (plan.list_phase[i] == ph) split(i, 1, plan.adj_lists[i].count, list_len(plan.adj_lists[i]), plan.adj_ltiles);
+        plan.adj_lphase_range.push_back({begin, (int)plan.adj_ltiles.size() - begin});
     }
-    upload(plan.d_tiles, plan.tiles);
-    upload(plan.d_adj_tiles, plan.adj_tiles);
+    for (int c = 0; c < ghexb_plan_s::k_classes; ++c)
+    {
+        upload(plan.d_ftiles[c], plan.ftiles[c]);
+        upload(plan.d_ptiles[c], plan.ptiles[c]);
+    }
+    upload(plan.d_adj_btiles, plan.adj_btiles);
+    upload(plan.d_adj_ltiles, plan.adj_ltiles);
 }
 
 void release_graph(ghexb_plan_s& plan)
@@ -637,20 +670,30 @@ void release_graph(ghexb_plan_s& plan)
 
 void launch_plan(ghexb_plan_s& plan, int form, cudaStream_t stream)
 {
-    auto run = [&](int begin, int count) {
+    auto run = [&](int c, int begin, int count) {
         if (count <= 0) return;
-        check_cuda(launch_exchange(plan.d_boxes, plan.d_lists, plan.d_tiles + begin, count,
-                       plan.grid(count), plan.block, stream),
-            "exchange kernel launch");
+        const tile* t = (form == GHEXB_FORM_BATCHED ? plan.d_ftiles[c] : plan.d_ptiles[c]) + begin;
+        unsigned* ctr = plan.d_counters + 2 * c;
+        const cudaError_t e = c < 2
+            ? launch_box_exchange(plan.d_boxes, t, count, c == 0, ctr, plan.grid(count), plan.block, stream)
+            : launch_list_exchange(plan.d_lists, t, count, c == 2, ctr, plan.grid(count), plan.block, stream);
+        check_cuda(e, "exchange kernel launch");
     };
     switch (form)
     {
-        case GHEXB_FORM_BATCHED: run(0, (int)plan.tiles.size()); break;
+        case GHEXB_FORM_BATCHED:
+            for (int c = 0; c < ghexb_plan_s::k_classes; ++c) run(c, 0, (int)plan.ftiles[c].size());
+            break;
         case GHEXB_FORM_PER_FIELD:
-            for (const auto& r : plan.logical_range) run(r.first, r.second);
+            for (int lg = 0; lg < plan.n_logical; ++lg)
+                for (int c = 0; c < ghexb_plan_s::k_classes; ++c)
+                    run(c, plan.logical_range[c][lg].first, plan.logical_range[c][lg].second);
             break;
         case GHEXB_FORM_PER_BOX:
-            for (const auto& r : plan.desc_range) run(r.first, r.second);
+            for (size_t i = 0; i < plan.boxes.size(); ++i)
+                run(plan.boxes[i].esize >= 4 ? 0 : 1, plan.box_range[i].first, plan.box_range[i].second);
+            for (size_t i = 0; i < plan.lists.size(); ++i)
+                run(plan.lists[i].unit >= 8 ? 2 : 3, plan.list_range[i].first, plan.list_range[i].second);
             break;
         default: throw error(GHEXB_ERR_INVALID, "unknown exchange form " + std::to_string(form));
     }
@@ -661,11 +704,22 @@ void graph_launch_plan(ghexb_plan_s& plan, cudaStream_t stream)
     if (!plan.exec)
     {
         check_cuda(cudaStreamBeginCapture(plan.cap_stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
-        cudaError_t le = launch_exchange(plan.d_boxes, plan.d_lists, plan.d_tiles, (int)plan.tiles.size(),
-            plan.grid((int)plan.tiles.size()), plan.block, plan.cap_stream);
+        std::string err;
+        try
+        {
+            launch_plan(plan, GHEXB_FORM_BATCHED, plan.cap_stream);
+        }
+        catch (const error& e)
+        {
+            err = e.what();
+        }
         cudaGraph_t g = nullptr;
         cudaError_t ce = cudaStreamEndCapture(plan.cap_stream, &g);
-        check_cuda(le, "exchange kernel capture");
+        if (!err.empty())
+        {
+            if (g) cudaGraphDestroy(g);
+            throw error(GHEXB_ERR_CUDA, err);
+        }
         check_cuda(ce, "cudaStreamEndCapture");
         plan.graph = g;
         check_cuda(cudaGraphInstantiate(&plan.exec, plan.graph, 0), "cudaGraphInstantiate");
@@ -676,12 +730,18 @@ void graph_launch_plan(ghexb_plan_s& plan, cudaStream_t stream)
 void adjoint_plan(ghexb_plan_s& plan, cudaStream_t stream)
 {
     if (!plan.adjoint_ok) throw error(GHEXB_ERR_INVALID, plan.adjoint_reason);
-    for (const auto& r : plan.phase_range)
+    for (size_t ph = 0; ph < plan.adj_bphase_range.size(); ++ph)
     {
-        if (r.second <= 0) continue;
-        check_cuda(launch_adjoint(plan.d_boxes, plan.d_adj_lists, plan.d_adj_tiles + r.first, r.second,
-                       plan.grid(r.second), plan.block, stream),
-            "adjoint kernel launch");
+        const auto rb = plan.adj_bphase_range[ph];
+        const auto rl = plan.adj_lphase_range[ph];
+        if (rb.second > 0)
+            check_cuda(launch_box_adjoint(plan.d_boxes, plan.d_adj_btiles + rb.first, rb.second,
+                           plan.d_counters + 2 * ghexb_plan_s::k_classes, plan.grid(rb.second), plan.block, stream),
+                "adjoint kernel launch");
+        if (rl.second > 0)
+            check_cuda(launch_list_adjoint(plan.d_adj_lists, plan.d_adj_ltiles + rl.first, rl.second,
+                           plan.d_counters + 2 * ghexb_plan_s::k_classes + 2, plan.grid(rl.second), plan.block, stream),
+                "adjoint kernel launch");
     }
 }
 
@@ -756,7 +816,9 @@ ghexb_plan_s::~ghexb_plan_s()
 {
     ghexb::release_graph(*this);
     if (cap_stream) cudaStreamDestroy(cap_stream);
-    for (void* p : {(void*)d_boxes, (void*)d_lists, (void*)d_adj_lists, (void*)d_idx, (void*)d_tiles, (void*)d_adj_tiles})
+    for (void* p : {(void*)d_boxes, (void*)d_lists, (void*)d_adj_lists, (void*)d_idx, (void*)d_ftiles[0],
+             (void*)d_ftiles[1], (void*)d_ftiles[2], (void*)d_ftiles[3], (void*)d_ptiles[0], (void*)d_ptiles[1],
+             (void*)d_ptiles[2], (void*)d_ptiles[3], (void*)d_adj_btiles, (void*)d_adj_ltiles, (void*)d_counters})
         if (p) cudaFree(p);
 }
 

@@ -28,12 +28,20 @@ struct ghexb_plan_s
     std::vector<int> adj_src_slot, adj_dst_slot;   // field slots of each adjoint list descriptor
     int n_logical = 0;
 
-    // tiles: forward tiles are grouped by logical field, then by descriptor
-    std::vector<ghexb::tile> tiles;
-    std::vector<std::pair<int, int>> logical_range; // [begin, count) in tiles
-    std::vector<std::pair<int, int>> desc_range;    // per box desc, then per list desc
-    std::vector<ghexb::tile> adj_tiles;
-    std::vector<std::pair<int, int>> phase_range;
+    // Forward tiles in four classes, each with its own kernel instance: box descriptors of 8/4-byte
+    // and of 2/1-byte elements, list descriptors of 16/8-byte and of 4/2/1-byte units. Within a
+    // class, tiles are grouped by logical field, then by descriptor.
+    // ftiles: the batched form's table, most expensive tiles first (dynamic scheduling then fills
+    // the tail with cheap ones); ptiles: the same tiles grouped by logical field for the per-field
+    // and per-box forms.
+    static constexpr int k_classes = 4;
+    std::vector<ghexb::tile> ftiles[k_classes];
+    std::vector<ghexb::tile> ptiles[k_classes];
+    std::vector<std::pair<int, int>> logical_range[k_classes]; // [begin, count) in ptiles per logical field
+    std::vector<std::pair<int, int>> box_range, list_range;    // [begin, count) in ptiles per descriptor
+    // adjoint tiles (box, list) grouped by phase
+    std::vector<ghexb::tile> adj_btiles, adj_ltiles;
+    std::vector<std::pair<int, int>> adj_bphase_range, adj_lphase_range;
     std::vector<int> box_phase, list_phase;
 
     // device copies
@@ -41,8 +49,18 @@ struct ghexb_plan_s
     ghexb::list_desc* d_lists = nullptr;
     ghexb::list_desc* d_adj_lists = nullptr;
     int32_t* d_idx = nullptr;
-    ghexb::tile* d_tiles = nullptr;
-    ghexb::tile* d_adj_tiles = nullptr;
+    ghexb::tile* d_ftiles[k_classes] = {nullptr, nullptr, nullptr, nullptr};
+    ghexb::tile* d_ptiles[k_classes] = {nullptr, nullptr, nullptr, nullptr};
+    ghexb::tile* d_adj_btiles = nullptr;
+    ghexb::tile* d_adj_ltiles = nullptr;
+    unsigned* d_counters = nullptr; // tile scheduler counters, two per tile class
+
+    int64_t num_tiles() const
+    {
+        int64_t n = 0;
+        for (const auto& t : ftiles) n += (int64_t)t.size();
+        return n;
+    }
 
     // statistics
     int64_t halo_elements = 0;
