@@ -90,6 +90,7 @@ SIGNATURES = {
     "ghexb_plan_graph_launch": [_vp, _vp],
     "ghexb_plan_adjoint_launch": [_vp, _vp],
     "ghexb_plan_autotune": [_vp, _vp, _i, C.POINTER(PlanInfo)],
+    "ghexb_exchange_noalloc": [_vp, C.POINTER(_vp), _i, _vp],
 }
 
 for _name, _args in SIGNATURES.items():

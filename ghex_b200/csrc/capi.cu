@@ -71,6 +71,12 @@ std::vector<int64_t> signature(const ghexb_field* fields, int n)
 }
 } // namespace
 
+namespace ghexb
+{
+// Records a failure for ghexb_last_error() from entry points defined in other files.
+int set_last_error(int code, const std::string& msg) { return set_error(code, msg); }
+} // namespace ghexb
+
 struct ghexb_co_s
 {
     ghexb_context_s* ctx = nullptr;

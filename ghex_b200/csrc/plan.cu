@@ -572,6 +572,18 @@ int64_t check_tables(const ghexb_plan_s& plan)
 void retile(ghexb_plan_s& plan)
 {
     release_graph(plan);
+    build_tiles(plan);
+    for (int c = 0; c < ghexb_plan_s::k_classes; ++c)
+    {
+        upload(plan.d_ftiles[c], plan.ftiles[c]);
+        upload(plan.d_ptiles[c], plan.ptiles[c]);
+    }
+    upload(plan.d_adj_btiles, plan.adj_btiles);
+    upload(plan.d_adj_ltiles, plan.adj_ltiles);
+}
+
+void build_tiles(ghexb_plan_s& plan)
+{
     // Tiles are row ranges. A tile holds about tile_elems elements, fewer for short rows: a row of
     // n0 elements touches at least one 32-byte sector, so the cost per element grows as rows
     // shrink below 256 bytes.
@@ -653,13 +665,6 @@ void retile(ghexb_plan_s& plan)
             if (plan.list_phase[i] == ph) split(i, 1, plan.adj_lists[i].count, list_len(plan.adj_lists[i]), plan.adj_ltiles);
         plan.adj_lphase_range.push_back({begin, (int)plan.adj_ltiles.size() - begin});
     }
-    for (int c = 0; c < ghexb_plan_s::k_classes; ++c)
-    {
-        upload(plan.d_ftiles[c], plan.ftiles[c]);
-        upload(plan.d_ptiles[c], plan.ptiles[c]);
-    }
-    upload(plan.d_adj_btiles, plan.adj_btiles);
-    upload(plan.d_adj_ltiles, plan.adj_ltiles);
 }
 
 void release_graph(ghexb_plan_s& plan)

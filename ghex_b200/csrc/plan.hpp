@@ -94,6 +94,9 @@ void build_plan(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* fie
 // Replays on the host the address computation of every element the forward and adjoint kernels
 // touch and checks it against the memory span of its field; returns the number of elements.
 int64_t check_tables(const ghexb_plan_s& plan);
+// Host-only: tile tables of the current tuning (no device memory touched).
+void build_tiles(ghexb_plan_s& plan);
+// build_tiles + upload of the tile tables.
 void retile(ghexb_plan_s& plan);
 void release_graph(ghexb_plan_s& plan);
 void launch_plan(ghexb_plan_s& plan, int form, cudaStream_t stream);
@@ -101,4 +104,6 @@ void graph_launch_plan(ghexb_plan_s& plan, cudaStream_t stream);
 void adjoint_plan(ghexb_plan_s& plan, cudaStream_t stream);
 void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats);
 void check_cuda(cudaError_t e, const char* what);
+// Records a failure for ghexb_last_error() (capi.cu).
+int set_last_error(int code, const std::string& msg);
 } // namespace ghexb

@@ -187,6 +187,19 @@ int ghexb_plan_adjoint_launch(ghexb_plan plan, void* stream);
  * chosen tuning is returned through `info` when it is not NULL. Runs real exchanges. */
 int ghexb_plan_autotune(ghexb_plan plan, void* stream, int repeats, ghexb_plan_info_t* info);
 
+/* ---- batched exchange without device allocation. This entry point has no counterpart in GHEX.
+ * For callers that cannot allocate device memory when they exchange: an application whose memory
+ * manager owns the device memory (a pool that reserved HBM at start-up and treats any other
+ * cudaMalloc as a failure), or code that must not call cudaMalloc/cudaFree because they may
+ * synchronize the device. The work tables go into one fixed device array of 4 MiB that every GPU
+ * holds while the library is loaded; exchanges whose tables are larger fail with
+ * GHEXB_ERR_RANGE. Each call copies the tables (scheduler counters zeroed) and launches the
+ * batched kernels on `stream`; no cudaMalloc or cudaFree is called. The first call on a device
+ * looks up the array's device address and must be made with that device current and before any
+ * stream capture. All calls share the array and it keeps the last call's tables: calls that
+ * overlap on the GPU race on it. */
+int ghexb_exchange_noalloc(ghexb_context ctx, const ghexb_field* fields, int n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
