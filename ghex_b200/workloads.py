@@ -154,3 +154,68 @@ def config4(seed: int = 42, dtype=np.float64, shape=(256, 256, 128)) -> RegularW
                         regular_decomposition(shape, (2, 2, 2)))
     w.fields = [FieldSpec("x", dtype, (1, 1, 1, 1, 1, 1), seed)]
     return w
+
+
+# ---------------------------------------------------------------------------------------------
+# cubed sphere
+# ---------------------------------------------------------------------------------------------
+# Face orientation of the cube: the outward normal and the directions of increasing x and y of
+# each tile, chosen so that neighbouring tiles share edges as in the tile table of the
+# cubed-sphere transforms. Only the smoothness of the synthetic values depends on it.
+_FACES = (((1, 0, 0), (0, 1, 0), (0, 0, 1)), ((0, 1, 0), (-1, 0, 0), (0, 0, 1)), ((0, 0, 1), (0, 1, 0), (-1, 0, 0)),
+          ((-1, 0, 0), (0, 0, 1), (0, 1, 0)), ((0, -1, 0), (0, 0, 1), (1, 0, 0)), ((0, 0, -1), (1, 0, 0), (0, 1, 0)))
+
+
+@dataclass
+class CubedSphereWorkload:
+    name: str
+    edge: int
+    levels: int
+    halo: int
+    domains: list      # (tile, x_first, x_last, y_first, y_last)
+    seed: int
+
+    def extents(self, dom) -> tuple:
+        _, x0, x1, y0, y1 = dom
+        return (x1 - x0 + 1 + 2 * self.halo, y1 - y0 + 1 + 2 * self.halo, self.levels)
+
+    def offsets(self) -> tuple:
+        return (self.halo, self.halo, 0)
+
+    def cell_centres(self, dom):
+        """Unit-sphere points of the domain's cell centres, shape (nx, ny, 3)."""
+        t, x0, x1, y0, y1 = dom
+        n, ex, ey = (np.array(v, dtype=np.float64) for v in _FACES[t])
+        a = -1.0 + (np.arange(x0, x1 + 1) + 0.5) * 2.0 / self.edge
+        b = -1.0 + (np.arange(y0, y1 + 1) + 0.5) * 2.0 / self.edge
+        A, B = np.meshgrid(a, b, indexing="ij")
+        p = n[None, None, :] + A[..., None] * ex[None, None, :] + B[..., None] * ey[None, None, :]
+        return p / np.linalg.norm(p, axis=-1, keepdims=True)
+
+    def domain_array(self, dom, ncomp: int, field_seed: int) -> np.ndarray:
+        """(x, y, z, c) memory, x fastest: interior = low-order spherical harmonics of the cell
+        centres (different per component and level) + 1e-3 seeded uniform noise; halos NaN."""
+        t, x0, x1, y0, y1 = dom
+        nx, ny = x1 - x0 + 1, y1 - y0 + 1
+        h = self.halo
+        a = np.full(self.extents(dom) + (ncomp,), np.nan, dtype=np.float64, order="F")
+        p = self.cell_centres(dom)
+        X, Y, Z = p[..., 0], p[..., 1], p[..., 2]
+        rng = np.random.default_rng([self.seed, field_seed, t, x0, y0])
+        lev = np.arange(self.levels, dtype=np.float64)[None, None, :]
+        for c in range(ncomp):
+            base = [1.0 + 0.5 * Z + 0.3 * X * Y + 0.2 * (3 * Z * Z - 1),   # s / u
+                    0.4 * X - 0.6 * Y + 0.25 * X * Z,                       # v
+                    0.7 * Y * Z - 0.1 * (X * X - Y * Y)][c % 3]
+            vals = base[..., None] * (1.0 + 0.01 * lev) + 1e-3 * rng.uniform(-1.0, 1.0, size=(nx, ny, self.levels))
+            a[h:h + nx, h:h + ny, :, c] = vals
+        return a
+
+
+def config3(seed: int = 42, edge: int = 384, levels: int = 90, split: int = 2, halo: int = 3) -> CubedSphereWorkload:
+    """6 tiles of edge x edge cells, `levels` levels, every tile split split x split, halo 3."""
+    step = edge // split
+    doms = [(t, i * step, (i + 1) * step - 1, j * step, (j + 1) * step - 1)
+            for t in range(6) for j in range(split) for i in range(split)]
+    return CubedSphereWorkload(f"cfg3: cubed sphere 6x{edge}^2x{levels}, {split}x{split} per tile, halo {halo}, "
+                               f"f64 scalar + f64 vector (u,v)", edge, levels, halo, doms, seed)

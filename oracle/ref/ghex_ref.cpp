@@ -1,0 +1,297 @@
+// C entry points that run GHEX 0.4.0's own CPU exchange — test infrastructure, built into
+// oracle/_ref/libghex_ref.so by oracle/ref/build.py from the reference's headers and
+// src/context.cpp, with the stand-ins of oracle/ref/shim for its absent dependencies (MPI, oomph,
+// gridtools, hwmalloc). One process holds every domain; messages go through the loopback
+// transport (one copy per message, as an MPI self-send).
+//
+// Used as the oracle for golden outputs and as the timed CPU baseline of the reference.
+#include <ghex/config.hpp>
+#include <ghex/context.hpp>
+#include <ghex/communication_object.hpp>
+#include <ghex/structured/cubed_sphere/field_descriptor.hpp>
+#include <ghex/structured/cubed_sphere/halo_generator.hpp>
+#include <ghex/structured/pattern.hpp>
+#include <ghex/structured/regular/domain_descriptor.hpp>
+#include <ghex/structured/regular/field_descriptor.hpp>
+#include <ghex/structured/regular/halo_generator.hpp>
+#include <ghex/unstructured/pattern.hpp>
+#include <ghex/unstructured/user_concepts.hpp>
+
+#include <chrono>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+namespace
+{
+thread_local std::string g_err;
+
+int fail(const std::string& m)
+{
+    g_err = m;
+    return 1;
+}
+
+enum dtype_code
+{
+    F32 = 0,
+    F64 = 1,
+    I32 = 2,
+    I64 = 3
+};
+
+// runs `exchange` once untimed and then `iters` times timed; returns seconds per exchange
+template<typename F>
+double timed(int iters, F&& exchange)
+{
+    exchange();
+    if (iters <= 0) return 0.0;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int i = 0; i < iters; ++i) exchange();
+    const auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(t1 - t0).count() / iters;
+}
+
+// Exchanges all buffer_info vectors of a tuple of vectors in one call of the communication object.
+template<typename CO, typename V0>
+void exchange_all(CO& co, V0& v0)
+{
+    if (!v0.empty()) co.exchange(v0.begin(), v0.end()).wait();
+}
+template<typename CO, typename V0, typename V1>
+void exchange_all(CO& co, V0& v0, V1& v1)
+{
+    if (v0.empty()) return exchange_all(co, v1);
+    if (v1.empty()) return exchange_all(co, v0);
+    co.exchange(v0.begin(), v0.end(), v1.begin(), v1.end()).wait();
+}
+
+// ---- regular -------------------------------------------------------------------------------
+template<int D>
+int regular(const int* g_first, const int* g_last, int n_dom, const int* ids, const int* firsts, const int* lasts,
+    int n_groups, const int* halos, const int* periodic, int n_fields, const int* field_group, const int* dtype,
+    void** data, const int* offsets, const int* extents, int iters, double* seconds)
+{
+    using dom_t = ghex::structured::regular::domain_descriptor<int, std::integral_constant<int, D>>;
+    using hg_t = ghex::structured::regular::halo_generator<int, std::integral_constant<int, D>>;
+    using layout = std::conditional_t<D == 3, gridtools::layout_map<2, 1, 0>,
+        std::conditional_t<D == 2, gridtools::layout_map<1, 0>, gridtools::layout_map<0>>>;
+    using arr = std::array<int, D>;
+    ghex::context ctxt(MPI_COMM_WORLD, true);
+    std::vector<dom_t> doms;
+    for (int i = 0; i < n_dom; ++i)
+    {
+        arr f, l;
+        for (int k = 0; k < D; ++k) f[k] = firsts[i * D + k], l[k] = lasts[i * D + k];
+        doms.emplace_back(ids[i], f, l);
+    }
+    arr gf, gl;
+    for (int k = 0; k < D; ++k) gf[k] = g_first[k], gl[k] = g_last[k];
+    using pattern_t = decltype(ghex::make_pattern<ghex::structured::grid>(
+        ctxt, std::declval<hg_t&>(), doms));
+    std::vector<pattern_t> pats;
+    pats.reserve(n_groups);
+    for (int g = 0; g < n_groups; ++g)
+    {
+        std::array<int, 2 * D> h;
+        std::array<bool, D> p;
+        for (int k = 0; k < 2 * D; ++k) h[k] = halos[g * 2 * D + k];
+        for (int k = 0; k < D; ++k) p[k] = periodic[g * D + k] != 0;
+        hg_t hg(gf, gl, h, p);
+        pats.push_back(ghex::make_pattern<ghex::structured::grid>(ctxt, hg, doms));
+    }
+    using fd_d = ghex::structured::regular::field_descriptor<double, ghex::cpu, dom_t, layout>;
+    using fd_f = ghex::structured::regular::field_descriptor<float, ghex::cpu, dom_t, layout>;
+    using fd_i = ghex::structured::regular::field_descriptor<int32_t, ghex::cpu, dom_t, layout>;
+    using fd_l = ghex::structured::regular::field_descriptor<int64_t, ghex::cpu, dom_t, layout>;
+    std::vector<fd_d> fdd;
+    std::vector<fd_f> fdf;
+    std::vector<fd_i> fdi;
+    std::vector<fd_l> fdl;
+    fdd.reserve(n_fields * n_dom), fdf.reserve(n_fields * n_dom), fdi.reserve(n_fields * n_dom), fdl.reserve(n_fields * n_dom);
+    std::vector<decltype(pats[0](std::declval<fd_d&>()))> bd;
+    std::vector<decltype(pats[0](std::declval<fd_f&>()))> bf;
+    std::vector<decltype(pats[0](std::declval<fd_i&>()))> bi;
+    std::vector<decltype(pats[0](std::declval<fd_l&>()))> bl;
+    for (int fi = 0; fi < n_fields; ++fi)
+        for (int d = 0; d < n_dom; ++d)
+        {
+            arr off, ext;
+            for (int k = 0; k < D; ++k) off[k] = offsets[fi * D + k], ext[k] = extents[(fi * n_dom + d) * D + k];
+            void* p = data[fi * n_dom + d];
+            auto& pat = pats[field_group[fi]];
+            switch (dtype[fi])
+            {
+                case F64:
+                    fdd.push_back(ghex::wrap_field<ghex::cpu, layout>(doms[d], (double*)p, off, ext));
+                    bd.push_back(pat(fdd.back()));
+                    break;
+                case F32:
+                    fdf.push_back(ghex::wrap_field<ghex::cpu, layout>(doms[d], (float*)p, off, ext));
+                    bf.push_back(pat(fdf.back()));
+                    break;
+                case I32:
+                    fdi.push_back(ghex::wrap_field<ghex::cpu, layout>(doms[d], (int32_t*)p, off, ext));
+                    bi.push_back(pat(fdi.back()));
+                    break;
+                default:
+                    fdl.push_back(ghex::wrap_field<ghex::cpu, layout>(doms[d], (int64_t*)p, off, ext));
+                    bl.push_back(pat(fdl.back()));
+                    break;
+            }
+        }
+    if (!bi.empty() || !bl.empty())
+    {
+        if (!bd.empty() || !bf.empty()) return fail("integer fields cannot be mixed with float fields here");
+        auto co = ghex::make_communication_object<pattern_t>(ctxt);
+        *seconds = timed(iters, [&] { exchange_all(co, bi, bl); });
+        return 0;
+    }
+    auto co = ghex::make_communication_object<pattern_t>(ctxt);
+    *seconds = timed(iters, [&] { exchange_all(co, bd, bf); });
+    return 0;
+}
+
+// ---- cubed sphere -------------------------------------------------------------------------
+template<typename T>
+int cubed(int edge, int levels, const int* halos, int n_dom, const int* tiles, const int* xf, const int* xl,
+    const int* yf, const int* yl, int n_fields, const int* ncomp, const int* is_vector, void** data,
+    const int* offsets, const int* extents, int iters, double* seconds)
+{
+    using namespace ghex::structured::cubed_sphere;
+    ghex::context ctxt(MPI_COMM_WORLD, true);
+    cube c{edge, levels};
+    std::vector<domain_descriptor> doms;
+    for (int i = 0; i < n_dom; ++i) doms.emplace_back(c, tiles[i], xf[i], xl[i], yf[i], yl[i]);
+    halo_generator hg(std::array<int, 4>{halos[0], halos[1], halos[2], halos[3]});
+    auto pat = ghex::make_pattern<ghex::structured::grid>(ctxt, hg, doms);
+    using fd_t = field_descriptor<T, ghex::cpu>;
+    std::vector<fd_t> fds;
+    fds.reserve(n_fields * n_dom);
+    std::vector<decltype(pat(std::declval<fd_t&>()))> bis;
+    for (int fi = 0; fi < n_fields; ++fi)
+        for (int d = 0; d < n_dom; ++d)
+        {
+            std::array<int, 3> off{offsets[fi * 3], offsets[fi * 3 + 1], offsets[fi * 3 + 2]};
+            const int* e = extents + (fi * n_dom + d) * 3;
+            std::array<int, 3> ext{e[0], e[1], e[2]};
+            fds.emplace_back(doms[d], (T*)data[fi * n_dom + d], off, ext, (unsigned)ncomp[fi], is_vector[fi] != 0);
+            bis.push_back(pat(fds.back()));
+        }
+    auto co = ghex::make_communication_object<decltype(pat)>(ctxt);
+    *seconds = timed(iters, [&] { co.exchange(bis.begin(), bis.end()).wait(); });
+    return 0;
+}
+
+// ---- unstructured --------------------------------------------------------------------------
+int unstructured(int n_dom, const int* ids, const int64_t* gid_off, const int* gids, const int64_t* outer_off,
+    const int64_t* outer_lids, int n_fields, const int* dtype, const int* levels, const int* levels_first,
+    void** data, int iters, double* seconds)
+{
+    using dom_t = ghex::unstructured::domain_descriptor<int, int>;
+    using hg_t = ghex::unstructured::halo_generator<int, int>;
+    ghex::context ctxt(MPI_COMM_WORLD, true);
+    std::vector<dom_t> doms;
+    for (int i = 0; i < n_dom; ++i)
+    {
+        std::vector<int> g(gids + gid_off[i], gids + gid_off[i + 1]);
+        std::vector<std::size_t> o(outer_lids + outer_off[i], outer_lids + outer_off[i + 1]);
+        doms.emplace_back(ids[i], g.begin(), g.end(), o.begin(), o.end());
+    }
+    hg_t hg;
+    auto pat = ghex::make_pattern<ghex::unstructured::grid>(ctxt, hg, doms);
+    using dd_d = ghex::unstructured::data_descriptor<ghex::cpu, int, int, double>;
+    using dd_f = ghex::unstructured::data_descriptor<ghex::cpu, int, int, float>;
+    std::vector<dd_d> fdd;
+    std::vector<dd_f> fdf;
+    fdd.reserve(n_fields * n_dom), fdf.reserve(n_fields * n_dom);
+    std::vector<decltype(pat(std::declval<dd_d&>()))> bd;
+    std::vector<decltype(pat(std::declval<dd_f&>()))> bf;
+    for (int fi = 0; fi < n_fields; ++fi)
+        for (int d = 0; d < n_dom; ++d)
+        {
+            void* p = data[fi * n_dom + d];
+            if (dtype[fi] == F64)
+            {
+                fdd.emplace_back(doms[d], (double*)p, (std::size_t)levels[fi], levels_first[fi] != 0);
+                bd.push_back(pat(fdd.back()));
+            }
+            else
+            {
+                fdf.emplace_back(doms[d], (float*)p, (std::size_t)levels[fi], levels_first[fi] != 0);
+                bf.push_back(pat(fdf.back()));
+            }
+        }
+    auto co = ghex::make_communication_object<decltype(pat)>(ctxt);
+    *seconds = timed(iters, [&] { exchange_all(co, bd, bf); });
+    return 0;
+}
+} // namespace
+
+extern "C" {
+
+int ghexref_last_error(char* buf, size_t len)
+{
+    std::snprintf(buf, len, "%s", g_err.c_str());
+    return 0;
+}
+
+int ghexref_regular_exchange(int dim, const int* g_first, const int* g_last, int n_dom, const int* ids,
+    const int* firsts, const int* lasts, int n_groups, const int* halos, const int* periodic, int n_fields,
+    const int* field_group, const int* dtype, void** data, const int* offsets, const int* extents, int iters,
+    double* seconds)
+{
+    try
+    {
+        switch (dim)
+        {
+            case 2:
+                return regular<2>(g_first, g_last, n_dom, ids, firsts, lasts, n_groups, halos, periodic, n_fields,
+                    field_group, dtype, data, offsets, extents, iters, seconds);
+            case 3:
+                return regular<3>(g_first, g_last, n_dom, ids, firsts, lasts, n_groups, halos, periodic, n_fields,
+                    field_group, dtype, data, offsets, extents, iters, seconds);
+            default: return fail("dim must be 2 or 3");
+        }
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+int ghexref_cubed_exchange(int dtype, int edge, int levels, const int* halos, int n_dom, const int* tiles,
+    const int* xf, const int* xl, const int* yf, const int* yl, int n_fields, const int* ncomp, const int* is_vector,
+    void** data, const int* offsets, const int* extents, int iters, double* seconds)
+{
+    try
+    {
+        if (dtype == F64)
+            return cubed<double>(edge, levels, halos, n_dom, tiles, xf, xl, yf, yl, n_fields, ncomp, is_vector, data,
+                offsets, extents, iters, seconds);
+        return cubed<float>(edge, levels, halos, n_dom, tiles, xf, xl, yf, yl, n_fields, ncomp, is_vector, data,
+            offsets, extents, iters, seconds);
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+int ghexref_unstructured_exchange(int n_dom, const int* ids, const int64_t* gid_off, const int* gids,
+    const int64_t* outer_off, const int64_t* outer_lids, int n_fields, const int* dtype, const int* levels,
+    const int* levels_first, void** data, int iters, double* seconds)
+{
+    try
+    {
+        return unstructured(n_dom, ids, gid_off, gids, outer_off, outer_lids, n_fields, dtype, levels, levels_first,
+            data, iters, seconds);
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+} // extern "C"

@@ -76,3 +76,43 @@ def test_check_rejects_too_small_memory():
     n = C.c_int64()
     rc = _capi.lib.ghexb_plan_check(ctx._h, arr, len(handles), C.byref(n))
     assert rc == _capi.ERR_RANGE
+
+
+def cubed_handles(w_edge, w_levels, halo, boxes, ncomps, vectors, mem_halo=None, dtype_size=8):
+    from ghex_b200.structured import cubed_sphere as CS
+    mem_halo = halo if mem_halo is None else mem_halo
+    ctx = CS.make_context(device=0)
+    cube = CS.cube(w_edge, w_levels)
+    doms = [CS.DomainDescriptor(cube, *b) for b in boxes]
+    pat = CS.make_pattern(ctx, CS.HaloGenerator(halo), doms)
+    keep, handles, base = [ctx, pat], [], 1 << 40
+    code = _capi.F64 if dtype_size == 8 else _capi.F32
+    for nc, isv in zip(ncomps, vectors):
+        for d, b in zip(doms, boxes):
+            nx, ny = b[2] - b[1] + 1 + 2 * mem_halo, b[4] - b[3] + 1 + 2 * mem_halo
+            ext = (nx, ny, w_levels, nc)
+            strides = (dtype_size, dtype_size * nx, dtype_size * nx * ny, dtype_size * nx * ny * w_levels)
+            f = CS.FieldDescriptor.__new__(CS.FieldDescriptor)
+            f.array, f._handles, f.domain = None, {}, d
+            f.info = {"ptr": base, "shape": ext, "strides": strides, "dtype": code, "itemsize": dtype_size, "device": 0}
+            f.offsets, f.extents = (mem_halo, mem_halo, 0, 0), ext
+            f.num_components, f.is_vector, f.layout = nc, isv, R._layout_order(strides)
+            base += ((nx * ny * w_levels * nc * dtype_size + 255) // 256) * 256
+            keep.append(f)
+            handles.append(pat(f).handle())
+    return ctx, keep, handles
+
+
+@pytest.mark.parametrize("case", ["cfg3", "reference-test"])
+def test_cubed_plan_accesses_in_bounds(case):
+    from ghex_b200 import workloads as W
+    if case == "cfg3":
+        w = W.config3()
+        ctx, keep, handles = cubed_handles(w.edge, w.levels, w.halo, w.domains, [1, 2], [False, True])
+    else:
+        boxes = [(t, x0, x0 + 4, y0, y0 + 4) for t in range(6) for (x0, y0) in ((0, 0), (5, 0), (0, 5), (5, 5))]
+        ctx, keep, handles = cubed_handles(10, 6, 2, boxes, [8, 8], [False, True], mem_halo=3, dtype_size=4)
+    arr = (C.c_void_p * len(handles))(*handles)
+    n = C.c_int64()
+    _capi.call("ghexb_plan_check", ctx._h, arr, len(handles), C.byref(n))
+    assert n.value > 0
