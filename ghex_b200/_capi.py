@@ -127,6 +127,25 @@ def int_array(values) -> C.Array:
     return (C.c_int * max(1, len(values)))(*values)
 
 
-def int64_array(values) -> C.Array:
+def int64_array(values):
+    """An int64 buffer for a C call: numpy arrays are passed without copying element by element
+    (the returned object keeps the memory alive for the duration of the call)."""
+    try:
+        import numpy as np
+        if isinstance(values, np.ndarray) or (isinstance(values, (list, tuple)) and len(values) > 4096):
+            arr = np.ascontiguousarray(np.asarray(values, dtype=np.int64))
+            if arr.size == 0:
+                arr = np.zeros(1, dtype=np.int64)
+            return _NumpyArg(arr, C.c_int64)
+    except ImportError:  # pragma: no cover
+        pass
     values = [int(v) for v in values]
     return (C.c_int64 * max(1, len(values)))(*values)
+
+
+class _NumpyArg:
+    """Wraps a numpy array as a ctypes pointer argument (ctypes calls `_as_parameter_`)."""
+
+    def __init__(self, arr, ctype):
+        self._arr = arr
+        self._as_parameter_ = arr.ctypes.data_as(C.POINTER(ctype))

@@ -26,22 +26,25 @@ class DomainDescriptor:
     (halo) elements."""
 
     def __init__(self, index: int, indices: Sequence[int], halo_indices: Sequence[int]):
+        import numpy as np
         self._id = int(index)
-        self.gids = [int(g) for g in indices]
-        self.outer_lids = [int(l) for l in halo_indices]
-        if len(set(self.outer_lids)) != len(self.outer_lids):
+        self.gids = np.asarray(indices, dtype=np.int64).ravel()
+        self.outer_lids = np.asarray(halo_indices, dtype=np.int64).ravel()
+        if np.unique(self.outer_lids).size != self.outer_lids.size:
             raise ValueError("repeated outer (local) index")
-        outer = set(self.outer_lids)
-        inner = [g for l, g in enumerate(self.gids) if l not in outer]
-        if len(set(inner)) != len(inner):
+        if self.outer_lids.size and (self.outer_lids.min() < 0 or self.outer_lids.max() >= self.gids.size):
+            raise ValueError("outer local index out of range")
+        inner = np.ones(self.gids.size, dtype=bool)
+        inner[self.outer_lids] = False
+        if np.unique(self.gids[inner]).size != int(inner.sum()):
             raise ValueError("repeated inner (global) index")
-        self._inner = len(inner)
+        self._inner = int(inner.sum())
 
     def domain_id(self) -> int:
         return self._id
 
     def size(self) -> int:
-        return len(self.gids)
+        return int(self.gids.size)
 
     def inner_size(self) -> int:
         return self._inner
@@ -76,23 +79,17 @@ def make_pattern(context: context, halo_gen: Union[HaloGenerator, Sequence[HaloG
     gens = list(halo_gen) if isinstance(halo_gen, (list, tuple)) else [halo_gen] * len(domains)
     if len(gens) != len(domains):
         raise ValueError("one halo generator per domain is needed")
-    gid_off, outer_off = [0], [0]
-    gids, outer = [], []
-    for d in domains:
-        gids += d.gids
-        gid_off.append(len(gids))
-        outer += d.outer_lids
-        outer_off.append(len(outer))
+    import numpy as np
+    gid_off = np.cumsum([0] + [d.gids.size for d in domains])
+    outer_off = np.cumsum([0] + [d.outer_lids.size for d in domains])
+    gids = np.concatenate([d.gids for d in domains])
+    outer = np.concatenate([d.outer_lids for d in domains])
     halo_off_arr = halo_arr = None
     if any(g.gids is not None for g in gens):
-        halo_off, halo = [0], []
-        for d, g in zip(domains, gens):
-            if g.gids is None:
-                halo += [d.gids[l] for l in sorted(d.outer_lids)]
-            else:
-                halo += g.gids
-            halo_off.append(len(halo))
-        halo_off_arr, halo_arr = int64_array(halo_off), int64_array(halo)
+        halo_lists = [d.gids[np.sort(d.outer_lids)] if g.gids is None else np.asarray(g.gids, dtype=np.int64)
+                      for d, g in zip(domains, gens)]
+        halo_off_arr = int64_array(np.cumsum([0] + [h.size for h in halo_lists]))
+        halo_arr = int64_array(np.concatenate(halo_lists) if halo_lists else np.zeros(0, dtype=np.int64))
     h = C.c_void_p()
     call("ghexb_pattern_create_unstructured", context._h, len(domains), int64_array([d.domain_id() for d in domains]),
          int64_array(gid_off), int64_array(gids), int64_array(outer_off), int64_array(outer), halo_off_arr, halo_arr,

@@ -219,3 +219,85 @@ def config3(seed: int = 42, edge: int = 384, levels: int = 90, split: int = 2, h
             for t in range(6) for j in range(split) for i in range(split)]
     return CubedSphereWorkload(f"cfg3: cubed sphere 6x{edge}^2x{levels}, {split}x{split} per tile, halo {halo}, "
                                f"f64 scalar + f64 vector (u,v)", edge, levels, halo, doms, seed)
+
+
+# ---------------------------------------------------------------------------------------------
+# unstructured: periodic triangulated lattice partitioned by recursive coordinate bisection
+# ---------------------------------------------------------------------------------------------
+# the six neighbours of a vertex of a triangulated lattice (each quad split along (i,j)-(i+1,j+1))
+LATTICE_NEIGHBOURS = ((1, 0), (-1, 0), (0, 1), (0, -1), (1, 1), (-1, -1))
+
+
+def rcb(x: np.ndarray, y: np.ndarray, parts: int) -> np.ndarray:
+    """Recursive coordinate bisection: the part of every point; each level halves every part at
+    the median of its longer coordinate extent (parts must be a power of two)."""
+    part = np.zeros(x.size, dtype=np.int32)
+    groups = [np.arange(x.size)]
+    while len(groups) < parts:
+        nxt = []
+        for g in groups:
+            gx, gy = x[g], y[g]
+            c = gx if (gx.max() - gx.min()) >= (gy.max() - gy.min()) else gy
+            order = np.argsort(c, kind="stable")
+            half = g.size // 2
+            nxt += [g[order[:half]], g[order[half:]]]
+        groups = nxt
+    for p, g in enumerate(groups):
+        part[g] = p
+    return part
+
+
+@dataclass
+class UnstructuredWorkload:
+    name: str
+    levels: int
+    domains: list  # (id, gids (int64), outer_lids (int64))
+    seed: int
+
+    def domain_array(self, dom, dtype, field_seed: int, levels_first: bool = True) -> np.ndarray:
+        """(n, levels): inner vertex rows = splitmix64(seed, gid*levels + level) in [-1, 1), halo
+        rows NaN; levels contiguous (C order) when levels_first, else vertices contiguous."""
+        _, gids, outer = dom
+        n = gids.size
+        a = np.full((n, self.levels), np.nan, dtype=dtype, order="C" if levels_first else "F")
+        inner = np.ones(n, dtype=bool)
+        inner[outer] = False
+        idx = gids[inner][:, None].astype(np.int64) * self.levels + np.arange(self.levels)[None, :]
+        a[inner] = unit_values(self.seed * 1000003 + field_seed, idx).astype(dtype)
+        return a
+
+
+def config2(seed: int = 42, ni: int = 1024, nj: int = 2048, parts: int = 16, levels: int = 64) -> UnstructuredWorkload:
+    """A periodic ni x nj triangulated lattice, vertex ids permuted by the seed, coordinates
+    jittered by uniform +-0.3 cell, partitioned into `parts` domains by recursive coordinate
+    bisection; every domain stores its inner vertices (ascending lattice index) followed by its
+    1-ring halo (ascending gid)."""
+    rng = np.random.default_rng(seed)
+    n = ni * nj
+    perm = rng.permutation(n).astype(np.int64)
+    i = np.repeat(np.arange(ni), nj)
+    j = np.tile(np.arange(nj), ni)
+    x = i + rng.uniform(-0.3, 0.3, size=n)
+    y = j + rng.uniform(-0.3, 0.3, size=n)
+    part = rcb(x, y, parts)
+    halo_of = [[] for _ in range(parts)]
+    for di, dj in LATTICE_NEIGHBOURS:
+        nb = ((i + di) % ni) * nj + (j + dj) % nj
+        cut = part[nb] != part
+        src_part, nbv = part[cut], nb[cut]
+        order = np.argsort(src_part, kind="stable")
+        src_part, nbv = src_part[order], nbv[order]
+        bounds = np.searchsorted(src_part, np.arange(parts + 1))
+        for p in range(parts):
+            halo_of[p].append(nbv[bounds[p]:bounds[p + 1]])
+    doms = []
+    for p in range(parts):
+        inner = np.nonzero(part == p)[0]
+        halo = np.unique(np.concatenate(halo_of[p]))
+        hg = perm[halo]
+        hg = np.sort(hg)
+        gids = np.concatenate([perm[inner], hg])
+        outer = np.arange(inner.size, gids.size, dtype=np.int64)
+        doms.append((p, gids, outer))
+    return UnstructuredWorkload(f"cfg2: periodic triangulated lattice {ni}x{nj} ({n} vertices), RCB into {parts} "
+                                f"domains, 1-ring halos, {levels} levels", levels, doms, seed)

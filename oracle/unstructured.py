@@ -1,0 +1,118 @@
+"""Oracle for unstructured grids (test infrastructure only).
+
+Restates, in plain Python and numpy:
+  * unstructured::domain_descriptor (unstructured/user_concepts.hpp:37-175) and make_outer_lids
+    (:88-113): repeated halo gids take their local ids in ascending order (the reference uses
+    std::unordered_multimap's equal_range order; every local id of one gid receives the value of
+    the same owner, so the exchanged values do not depend on it);
+  * halo_generator (:180-256), all outer gids or an explicit list;
+  * make_pattern_impl<unstructured grid>::apply without domain hints (unstructured/pattern.hpp:
+    187-370): the send list of owner i towards domain o is the subsequence of o's halo gids that are
+    inner to i (in o's halo order), the receive list its local ids in o; tags
+    (i << num_bits(#domains)) | id(o), maps ordered by tag;
+  * the exchange (data_descriptor get/set, user_concepts.hpp:383-452, with the message buffer
+    removed) and its adjoint in receive-map order, column by column.
+
+Fields are numpy arrays of shape (n,) or (n, levels) — either memory order.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+class Domain:
+    def __init__(self, id_: int, gids, outer_lids):
+        self.id = int(id_)
+        self.gids = [int(g) for g in gids]
+        self.outer_lids = [int(x) for x in outer_lids]
+        outer = set(self.outer_lids)
+        if len(outer) != len(self.outer_lids):
+            raise ValueError("repeated outer (local) index")
+        self.inner: dict[int, int] = {}
+        self.outer: dict[int, list[int]] = {}
+        self.outer_gids: list[int] = []
+        for lid, g in enumerate(self.gids):
+            if lid in outer:
+                self.outer.setdefault(g, []).append(lid)
+                self.outer_gids.append(g)
+            else:
+                if g in self.inner:
+                    raise ValueError("repeated inner (global) index")
+                self.inner[g] = lid
+
+    def make_outer_lids(self, gids):
+        lids, used = [], {}
+        for g in gids:
+            if g not in self.outer:
+                continue
+            k = used.get(g, 0)
+            if k >= len(self.outer[g]):
+                raise ValueError("halo gid does not have an associated lid in the domain")
+            lids.append(self.outer[g][k])
+            used[g] = k + 1
+        for g, k in used.items():
+            if k != len(self.outer[g]):
+                raise ValueError("halo gid occurs not often enough")
+        return lids
+
+
+@dataclass
+class Entry:
+    neighbor: int
+    tag: int
+    lids: list = field(default_factory=list)
+
+
+def _num_bits(n: int) -> int:
+    return 1 if n == 0 else 1 + _num_bits(n >> 1)
+
+
+def make_pattern(domains: list[Domain], halo_gids=None):
+    """Receive and send entries per domain. halo_gids: None (all outer gids) or one gid list per
+    domain."""
+    n = len(domains)
+    halos = []
+    for i, d in enumerate(domains):
+        lids = d.make_outer_lids(d.outer_gids if halo_gids is None else halo_gids[i])
+        halos.append([d.gids[l] for l in lids])
+    shift = _num_bits(n)
+    recv = [dict() for _ in range(n)]
+    send = [dict() for _ in range(n)]
+    for o in range(n):
+        for i in range(n):
+            tag = (i << shift) | domains[o].id
+            s = [domains[i].inner[g] for g in halos[o] if g in domains[i].inner]
+            if not s:
+                continue
+            g_list = [g for g in halos[o] if g in domains[i].inner]
+            send[i][tag] = Entry(o, tag, s)
+            recv[o][tag] = Entry(i, tag, domains[o].make_outer_lids(g_list))
+    max_tag = (n << shift) | max(d.id for d in domains)
+    return ([[recv[d][t] for t in sorted(recv[d])] for d in range(n)],
+            [[send[d][t] for t in sorted(send[d])] for d in range(n)], max_tag)
+
+
+def _pairs(recv, send):
+    """(receiver, sender, receive lids, send lids) in receive-map order."""
+    for d, entries in enumerate(recv):
+        for en in entries:
+            s = next(x for x in send[en.neighbor] if x.neighbor == d and x.tag == en.tag)
+            yield d, en.neighbor, np.asarray(en.lids), np.asarray(s.lids)
+
+
+def exchange(recv, send, fields) -> None:
+    for d, e, R, S in _pairs(recv, send):
+        fields[d][R] = fields[e][S]
+
+
+def adjoint(recv, send, grads) -> None:
+    """owner += halo in receive-map order, then halo = 0 (np.add.at adds repeated owners in order)."""
+    for d, e, R, S in _pairs(recv, send):
+        h = grads[d][R].copy()
+        if grads[e].ndim == 1:
+            np.add.at(grads[e], S, h)
+        else:
+            np.add.at(grads[e], (S, slice(None)), h)
+        grads[d][R] = 0

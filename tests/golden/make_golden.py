@@ -1,0 +1,112 @@
+"""Generates the golden fixtures of tests/golden/ from the reference.
+
+    python tests/golden/make_golden.py [--reference /root/reference]
+
+* unstructured_4domain.json — the hand-built 4-domain unstructured test case of GHEX's Python
+  test (test/bindings/python/test_unstructured_domain_descriptor.py: the `domains` literal, read
+  as text with ast, never imported);
+* unstructured_4domain.npz — its fields (2 levels, value rank*1000 + 10*gid + level on inner
+  vertices, -1 elsewhere, both storage orders) exchanged by GHEX's own code (oracle/_ref);
+* cubed_sphere_test.npz — the cubed-sphere test configuration of
+  test/structured/cubed_sphere/test_cubed_sphere_exchange.cpp, scalar and vector, exchanged by
+  GHEX's own code;
+* regular_small.npz — small regular cases (periodic 2x2x2 halo 1; uneven 3x3x3 with the five
+  fields of the benchmark's batched case) exchanged by GHEX's own code.
+
+Every input is seeded or analytic; the script needs the reference tree and oracle/_ref.
+"""
+from __future__ import annotations
+
+import argparse
+import ast
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+
+
+def read_domains_literal(reference: Path) -> dict:
+    src = (reference / "test" / "bindings" / "python" / "test_unstructured_domain_descriptor.py").read_text()
+    for node in ast.parse(src).body:
+        if isinstance(node, ast.Assign) and any(getattr(t, "id", None) == "domains" for t in node.targets):
+            return ast.literal_eval(node.value)
+    raise RuntimeError("no `domains` literal found")
+
+
+def unstructured_fields(dom: dict, rank: int, levels: int, order: str) -> np.ndarray:
+    inner = set(dom["inner"])
+    a = np.full((len(dom["all"]), levels), -1.0, dtype=np.float64, order=order)
+    for x, gid in enumerate(dom["all"]):
+        if gid in inner:
+            for l in range(levels):
+                a[x, l] = rank * 1000 + 10 * gid + l
+    return a
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    a = ap.parse_args()
+    reference = Path(a.reference)
+    from oracle import reflib
+    from oracle.ref import build as refbuild
+    refbuild.build(str(reference))
+    if not reflib.available():
+        raise SystemExit("oracle/_ref is not built")
+
+    # ---- unstructured 4-domain case
+    doms = read_domains_literal(reference)
+    (HERE / "unstructured_4domain.json").write_text(json.dumps({str(k): v for k, v in doms.items()}, indent=1))
+    out = {}
+    rdoms = [(r, doms[r]["all"], doms[r]["outer_lids"]) for r in sorted(doms)]
+    for order, first in (("C", True), ("F", False)):
+        fields = [unstructured_fields(doms[r], r, 2, order) for r in sorted(doms)]
+        for r, f in zip(sorted(doms), fields):
+            out[f"in_{order}_{r}"] = f.copy()
+        reflib.unstructured_exchange(rdoms, [(2, first, fields)])
+        for r, f in zip(sorted(doms), fields):
+            out[f"out_{order}_{r}"] = f
+    np.savez_compressed(HERE / "unstructured_4domain.npz", **out)
+
+    # ---- cubed sphere test configuration
+    import cs_cases as cs
+    out = {}
+    for vec in (False, True):
+        arrs = cs.fields()
+        reflib.cubed_exchange(cs.EDGE, cs.LEVELS, (cs.HALO,) * 4, cs.domains(),
+                              [(cs.NCOMP, vec, (cs.MEM_HALO, cs.MEM_HALO, 0), arrs)])
+        for i, x in enumerate(arrs):
+            out[f"{'vector' if vec else 'scalar'}_{i}"] = x
+    np.savez_compressed(HERE / "cubed_sphere_test.npz", **out)
+
+    # ---- small regular cases
+    from ghex_b200 import workloads as W
+    out = {}
+    for name, w in (("periodic", W.RegularWorkload("16^3 2x2x2 halo 1 periodic", (16, 16, 16), (True, True, True),
+                                                      W.regular_decomposition((16, 16, 16), (2, 2, 2)),
+                                                      [W.FieldSpec("f64", np.float64, (1,) * 6, 7)])),
+                    ("batched", W.config1(shape=(40, 30, 12)))):
+        groups = list(w.halo_groups().items())
+        fields = []
+        for gi, (halos, specs) in enumerate(groups):
+            for s in specs:
+                arrs = [w.domain_array(d, s) for d in w.domains]
+                fields.append((gi, w.offsets(s), arrs, s.name))
+        reflib.regular_exchange(w.shape, [(h, w.periodic) for h, _ in groups], w.domains,
+                                [(g, off, arrs) for g, off, arrs, _ in fields])
+        for g, off, arrs, fname in fields:
+            for i, x in enumerate(arrs):
+                out[f"{name}_{fname}_{i}"] = x
+    np.savez_compressed(HERE / "regular_small.npz", **out)
+    for p in sorted(HERE.glob("*.np*")) + sorted(HERE.glob("*.json")):
+        print(p.name, p.stat().st_size)
+
+
+if __name__ == "__main__":
+    main()

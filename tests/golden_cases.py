@@ -1,0 +1,45 @@
+"""Loaders of the golden fixtures in tests/golden/ (made by tests/golden/make_golden.py from GHEX's
+own code)."""
+from __future__ import annotations
+
+import json
+from pathlib import Path
+
+import numpy as np
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def unstructured_domains() -> dict:
+    d = json.loads((GOLDEN / "unstructured_4domain.json").read_text())
+    return {int(k): v for k, v in d.items()}
+
+
+def unstructured_arrays() -> dict:
+    with np.load(GOLDEN / "unstructured_4domain.npz") as z:
+        return {k: z[k] for k in z.files}
+
+
+def cubed_arrays() -> dict:
+    with np.load(GOLDEN / "cubed_sphere_test.npz") as z:
+        return {k: z[k] for k in z.files}
+
+
+def regular_arrays() -> dict:
+    with np.load(GOLDEN / "regular_small.npz") as z:
+        return {k: z[k] for k in z.files}
+
+
+def unstructured_check(data: np.ndarray, dom: dict, rank: int, levels: int) -> int:
+    """check_field of test_unstructured_domain_descriptor.py: inner values keep
+    rank*1000 + 10*gid + l, halo values equal 10*gid + l modulo 1000. Returns the mismatches."""
+    inner = set(dom["inner"])
+    bad = 0
+    for x, gid in enumerate(dom["all"]):
+        for l in range(levels):
+            v = data[x, l]
+            if gid in inner:
+                bad += v != rank * 1000 + 10 * gid + l
+            else:
+                bad += (v - 1000 * int(v / 1000)) != 10 * gid + l
+    return int(bad)

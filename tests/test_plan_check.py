@@ -116,3 +116,39 @@ def test_cubed_plan_accesses_in_bounds(case):
     n = C.c_int64()
     _capi.call("ghexb_plan_check", ctx._h, arr, len(handles), C.byref(n))
     assert n.value > 0
+
+
+def unstructured_handles(doms_spec, levels, levels_first, dtype_size=8):
+    from ghex_b200 import unstructured as U
+    ctx = U.make_context(device=0)
+    doms = [U.DomainDescriptor(*d) for d in doms_spec]
+    pat = U.make_pattern(ctx, U.HaloGenerator(), doms)
+    keep, handles, base = [ctx, pat], [], 1 << 40
+    code = _capi.F64 if dtype_size == 8 else _capi.F32
+    for d in doms:
+        n = d.size()
+        f = U.FieldDescriptor.__new__(U.FieldDescriptor)
+        f.array, f._handles, f.domain_desc = None, {}, d
+        f.info = {"ptr": base, "shape": (n, levels), "dtype": code, "itemsize": dtype_size, "device": 0}
+        f.levels, f.levels_first, f.outer_stride = levels, levels_first, 0
+        base += ((n * levels * dtype_size + 255) // 256) * 256
+        keep.append(f)
+        handles.append(pat(f).handle())
+    return ctx, keep, handles
+
+
+@pytest.mark.parametrize("case", ["cfg2-f64", "cfg2-f32", "fixture-levels-last"])
+def test_unstructured_plan_accesses_in_bounds(case):
+    import golden_cases as G
+    from ghex_b200 import workloads as W
+    if case.startswith("cfg2"):
+        doms = W.config2().domains
+        ctx, keep, handles = unstructured_handles(doms, 64, True, 8 if case.endswith("64") else 4)
+    else:
+        g = G.unstructured_domains()
+        doms = [(r, g[r]["all"], g[r]["outer_lids"]) for r in sorted(g)]
+        ctx, keep, handles = unstructured_handles(doms, 2, False)
+    arr = (C.c_void_p * len(handles))(*handles)
+    n = C.c_int64()
+    _capi.call("ghexb_plan_check", ctx._h, arr, len(handles), C.byref(n))
+    assert n.value > 0
