@@ -333,7 +333,7 @@ def main():
         "config": {"workload": w.name, "form": "batched persistent kernel, CUDA graph", "domains": len(w.domains),
                    "fields": len(w.fields), "algorithmic_bytes_per_exchange": alg,
                    "l2": "cold: a 2 x L2 read of an unrelated buffer before every timed exchange, outside its events",
-                   "parallelism": f"replicas x{world}", "tuning": {k: tuning[k] for k in ("tile_elems", "block", "ctas_per_sm", "grid")}},
+                   "parallelism": f"replicas x{world}", "tuning": {k: tuning[k] for k in ("elems_per_thread", "block", "grid")}},
         "exchanges_per_s": world * 1e3 / ms_batched,
         "per_field": {"ms_per_step": ms_field, "GB/s": world * alg / (ms_field * 1e-3) / 1e9,
                       "exchanges_per_s": world * 1e3 / ms_field, "launches_per_exchange": len(w.fields)},

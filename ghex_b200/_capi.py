@@ -44,11 +44,12 @@ class PlanInfo(C.Structure):
         ("halo_elements", C.c_int64),
         ("algorithmic_bytes", C.c_int64),
         ("index_bytes", C.c_int64),
-        ("adjoint_phases", C.c_int64),
-        ("tile_elems", C.c_int32),
+        ("adjoint_launches", C.c_int64),
+        ("adjoint_cells", C.c_int64),
+        ("elems_per_thread", C.c_int32),
         ("block", C.c_int32),
-        ("ctas_per_sm", C.c_int32),
         ("grid", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -85,12 +86,15 @@ SIGNATURES = {
     "ghexb_plan_destroy": [_vp],
     "ghexb_plan_check": [_vp, C.POINTER(_vp), _i, _pi64],
     "ghexb_plan_get_info": [_vp, C.POINTER(PlanInfo)],
-    "ghexb_plan_set_tuning": [_vp, _i, _i, _i],
+    "ghexb_plan_set_tuning": [_vp, _i, _i],
     "ghexb_plan_launch": [_vp, _i, _vp],
     "ghexb_plan_graph_launch": [_vp, _vp],
     "ghexb_plan_adjoint_launch": [_vp, _vp],
     "ghexb_plan_autotune": [_vp, _vp, _i, C.POINTER(PlanInfo)],
     "ghexb_exchange_noalloc": [_vp, C.POINTER(_vp), _i, _vp],
+    "ghexb_plan_rebind": [_vp, C.POINTER(_vp), _i, _vp],
+    "ghexb_stencil7": [_i, _i, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_int64), C.POINTER(C.c_int64), _i,
+                       C.c_double, _i, _vp],
 }
 
 for _name, _args in SIGNATURES.items():

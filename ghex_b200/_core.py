@@ -74,6 +74,11 @@ def array_info(field: Any) -> dict:
             "dtype": _TYPESTR[typestr], "itemsize": itemsize, "device": None}
 
 
+def _layout_of(a: Any) -> tuple:
+    i = array_info(a)
+    return (i["shape"], i["strides"], i["dtype"], i["device"])
+
+
 def stream_of(fields: Iterable[Any]):
     """The stream an exchange is ordered on: torch's current stream for torch tensors."""
     torch = _torch()
@@ -330,6 +335,8 @@ class ExchangePlan:
         self.context = ctx
         self._bis = _flatten(tuple(buffer_infos))
         self._arrays = [a for bi in self._bis for a in bi.arrays()]
+        self._layout = [_layout_of(a) for a in self._arrays]
+        self._bound = tuple(array_info(a)["ptr"] for a in self._arrays)
         handles = (C.c_void_p * len(self._bis))(*[bi.handle() for bi in self._bis])
         h = C.c_void_p()
         call("ghexb_plan_create", ctx._h, handles, len(self._bis), C.byref(h))
@@ -340,12 +347,15 @@ class ExchangePlan:
         call("ghexb_plan_get_info", self._h, C.byref(i))
         return i.as_dict()
 
-    def set_tuning(self, tile_elems: int = 0, block: int = 0, ctas_per_sm: int = 0) -> None:
-        call("ghexb_plan_set_tuning", self._h, tile_elems, block, ctas_per_sm)
+    def set_tuning(self, elems_per_thread: int = 0, block: int = 0) -> None:
+        """Elements per thread (4, 8 or 16) and threads per CTA of the forward kernel; 0 keeps."""
+        call("ghexb_plan_set_tuning", self._h, elems_per_thread, block)
 
     def _stream(self, stream):
         if stream is None:
             return stream_of(self._arrays)
+        if isinstance(stream, C.c_void_p):
+            return stream
         if isinstance(stream, int):
             return C.c_void_p(stream)
         return C.c_void_p(getattr(stream, "cuda_stream", stream))
@@ -358,6 +368,28 @@ class ExchangePlan:
 
     def adjoint(self, stream=None) -> None:
         call("ghexb_plan_adjoint_launch", self._h, self._stream(stream))
+
+    def bound_pointers(self) -> tuple:
+        """Data pointers the plan's tables currently address, one per field."""
+        return self._bound
+
+    def rebind(self, arrays: Sequence[Any], stream=None, keep: bool = True) -> None:
+        """Points the plan at new memory: arrays[i] takes the place of the i-th field's array and
+        must have its shape, strides, dtype and device (checked here). Stream-ordered. With
+        keep=False the plan holds no reference to the arrays: the caller keeps them alive while
+        the plan's launches run and rebinds before launching on other memory."""
+        if len(arrays) != len(self._layout):
+            raise ValueError(f"rebind needs {len(self._layout)} arrays")
+        ptrs = []
+        for new, lay in zip(arrays, self._layout):
+            if _layout_of(new) != lay:
+                raise TypeError("rebind: array layout differs from the plan's field")
+            ptrs.append(array_info(new)["ptr"])
+        if stream is None:
+            stream = stream_of(arrays)
+        call("ghexb_plan_rebind", self._h, (C.c_void_p * len(ptrs))(*ptrs), len(ptrs), self._stream(stream))
+        self._bound = tuple(ptrs)
+        self._arrays = list(arrays) if keep else []
 
     def autotune(self, repeats: int = 10, stream=None) -> dict:
         i = _capi.PlanInfo()

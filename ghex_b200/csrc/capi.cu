@@ -8,8 +8,10 @@
 #include <new>
 #include <string>
 
+#include "exchange.hpp"
 #include "kernels.hpp"
 #include "plan.hpp"
+#include "stencil.hpp"
 
 namespace
 {
@@ -517,26 +519,32 @@ int ghexb_plan_get_info(ghexb_plan plan, ghexb_plan_info_t* info)
         info->halo_elements = plan->halo_elements;
         info->algorithmic_bytes = plan->algorithmic_bytes;
         info->index_bytes = plan->index_bytes;
-        info->adjoint_phases = (int64_t)plan->adj_bphase_range.size();
-        info->tile_elems = plan->tile_elems;
+        info->adjoint_launches = plan->adjoint_launches();
+        info->adjoint_cells = plan->gather_ok ? (int64_t)plan->cells.size() : 0;
+        info->elems_per_thread = plan->per_thread;
         info->block = plan->block;
-        info->ctas_per_sm = plan->ctas_per_sm;
-        info->grid = plan->grid((int)plan->ftiles[0].size());
+        info->grid = (int32_t)plan->xf.size();
+        info->reserved = 0;
     });
 }
 
-int ghexb_plan_set_tuning(ghexb_plan plan, int tile_elems, int block, int ctas_per_sm)
+int ghexb_plan_set_tuning(ghexb_plan plan, int elems_per_thread, int block)
 {
     return guarded([&] {
         require(plan != nullptr, "null plan");
-        if (tile_elems > 0) plan->tile_elems = tile_elems;
+        if (elems_per_thread > 0)
+        {
+            require(elems_per_thread == 4 || elems_per_thread == 8 || elems_per_thread == 16,
+                "elements per thread must be 4, 8 or 16");
+            plan->per_thread = elems_per_thread;
+        }
         if (block > 0)
         {
             require(block % 32 == 0 && block <= ghexb::k_max_block, "block must be a multiple of 32 and at most 512");
             plan->block = block;
         }
-        if (ctas_per_sm > 0) plan->ctas_per_sm = ctas_per_sm;
         ghexb::retile(*plan);
+        ghexb::check_cuda(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
     });
 }
 
@@ -564,6 +572,14 @@ int ghexb_plan_adjoint_launch(ghexb_plan plan, void* stream)
     });
 }
 
+int ghexb_plan_rebind(ghexb_plan plan, void* const* data, int n, void* stream)
+{
+    return guarded([&] {
+        require(plan && data, "null argument");
+        ghexb::rebind_plan(*plan, data, n, static_cast<cudaStream_t>(stream));
+    });
+}
+
 int ghexb_plan_autotune(ghexb_plan plan, void* stream, int repeats, ghexb_plan_info_t* info)
 {
     return guarded([&] {
@@ -574,6 +590,42 @@ int ghexb_plan_autotune(ghexb_plan plan, void* stream, int repeats, ghexb_plan_i
             const int rc = ghexb_plan_get_info(plan, info);
             if (rc != GHEXB_OK) throw ghexb::error(rc, g_last_error);
         }
+    });
+}
+
+int ghexb_stencil7(int dtype, int n, const void* const* in, void* const* out, const int64_t* extents,
+                   const int64_t* strides, int halo, double alpha, int adjoint, void* stream)
+{
+    return guarded([&] {
+        require(in && out && extents && strides, "null argument");
+        require(dtype == GHEXB_F32 || dtype == GHEXB_F64, "the stencil computes in float32 or float64");
+        require(n >= 0, "negative domain count");
+        require(halo >= 1, "the 7-point stencil needs a halo of width >= 1");
+        const int64_t es = dtype == GHEXB_F64 ? 8 : 4;
+        std::vector<ghexb::stencil_domain> doms(n);
+        for (int i = 0; i < n; ++i)
+        {
+            require(in[i] && out[i], "null data pointer");
+            require(reinterpret_cast<uintptr_t>(in[i]) % es == 0 && reinterpret_cast<uintptr_t>(out[i]) % es == 0,
+                "data pointer not aligned to its element size");
+            int64_t span = 1;
+            for (int a = 0; a < 3; ++a)
+            {
+                require(extents[3 * i + a] > 2 * halo && extents[3 * i + a] < (int64_t(1) << 30),
+                    "every extent must exceed twice the halo width");
+                require(strides[3 * i + a] > 0, "strides must be positive");
+                span += (extents[3 * i + a] - 1) * strides[3 * i + a];
+            }
+            const char* a0 = static_cast<const char*>(in[i]);
+            const char* b0 = static_cast<const char*>(out[i]);
+            require(a0 + span * es <= b0 || b0 + span * es <= a0, "input and output overlap");
+            doms[i] = ghexb::stencil_domain{in[i], out[i], (int32_t)extents[3 * i], (int32_t)extents[3 * i + 1],
+                (int32_t)extents[3 * i + 2], halo, strides[3 * i], strides[3 * i + 1], strides[3 * i + 2]};
+        }
+        if (n == 0) return;
+        ghexb::check_cuda(ghexb::launch_stencil7(dtype == GHEXB_F64, doms.data(), n, alpha, adjoint != 0,
+                              static_cast<cudaStream_t>(stream)),
+            "stencil launch");
     });
 }
 

@@ -106,6 +106,79 @@ struct alignas(16) list_desc
     row_map map;
 };
 
+// A forward work item: the elements [e0, e0 + count) of one box or list descriptor, with all
+// the kernel needs to address them, so that a CTA reads one 96-byte record and nothing else
+// before its data loads.
+//  * box:  element e -> i0 = e mod n0, r = e / n0, i1 = r mod n1, i2 = r / n1;
+//          dst[i0*d0 + i1*d1 + i2*d2] = src[i0*s0 + i1*s1 + i2*s2]  (sign bit flipped if neg)
+//  * list: element e -> k = e / n0 (column), l = e mod n0 (level);
+//          dst[didx[k]*d0 + l*d1] = src[sidx[k]*s0 + l*s1]
+// Offsets are in units of `unit` bytes (the element size; 16 for aligned list columns).
+struct alignas(16) xtile
+{
+    const char* src;
+    char* dst;
+    const int32_t* sidx;
+    const int32_t* didx;
+    uint32_t e0, count;
+    int32_t s0, s1, s2;
+    int32_t d0, d1, d2;
+    uint32_t n0, m0;  // first extent and its fast-division magic
+    uint32_t n1, m1;  // second extent (boxes)
+    uint8_t l0, l1;   // fast-division shifts
+    uint8_t unit;     // bytes per element: 1, 2, 4, 8 or 16
+    uint8_t kind;     // 0 box, 1 list
+    uint8_t neg;      // 1: flip the sign bit (negated cubed-sphere vector components)
+    uint8_t pad[11];
+};
+static_assert(sizeof(xtile) == 96, "xtile is six 16-byte words");
+
+// Adjoint of the boxes in gather form. The owner elements read by the forward boxes of one
+// source field are cut into disjoint cells (boxes in the owner's coordinates); every element of
+// a cell was copied to the same ordered list of halo images. For an owner element o:
+//   acc = own[o]; for each image i in order: acc = acc (+|-) img_i[o]; img_i[o] = 0; own[o] = acc
+// which is the explicit transpose in receive order, with no two threads touching one element.
+constexpr int k_max_images = 8;
+
+struct gimage
+{
+    char* ptr;            // image of the cell's element (0,0,0)
+    int32_t t0, t1, t2;   // element strides of the image per cell axis
+    uint32_t neg;         // 1: the forward negated this image
+};
+
+struct alignas(16) gtile
+{
+    char* own;            // owner element (0,0,0) of the cell
+    uint32_t e0, count;   // elements [e0, e0 + count) of the cell
+    int32_t o0, o1, o2;   // owner element strides per cell axis (axis 0 fastest)
+    uint32_t n0, m0, n1, m1;
+    uint8_t l0, l1;
+    uint8_t esize;        // 4 or 8 (float or double)
+    uint8_t nimg;         // 1..k_max_images
+    gimage img[k_max_images];
+    uint8_t pad[16];
+};
+static_assert(sizeof(gtile) == 256, "gtile is sixteen 16-byte words");
+
+// Host form of a gather cell, relative to field slots so that it survives a rebind.
+struct gcell
+{
+    int own_slot;
+    int64_t own_off;        // owner element (0,0,0), elements from the field's data
+    int32_t n[3];           // extents along the cell axes (axis 0 fastest in the owner)
+    int32_t o[3];           // owner element strides
+    int nimg;
+    struct
+    {
+        int slot;
+        int64_t off;        // image of element (0,0,0), elements from the field's data
+        int32_t t[3];
+        uint32_t neg;
+    } img[k_max_images];
+    int esize;
+};
+
 // A contiguous range [start, start+count) of one descriptor's rows.
 struct alignas(16) tile
 {

@@ -1,4 +1,4 @@
-// Host launchers of the ghex_b200 device kernels (kernels.cu).
+// Host launchers of the phased adjoint kernels and the L2 flush (kernels.cu).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -7,18 +7,10 @@
 
 namespace ghexb
 {
-// Forward exchange over tiles[0, ntiles) of box descriptors (3-D boxes; `large`: elements of 8 and 4
-// bytes mixed freely, else of 2 and 1 bytes) and of list descriptors (`large`: units of 16 and 8
-// bytes, else of 4, 2 and 1 bytes). The large classes claim tiles dynamically through
-// counters[0..1] (zero before the launch, zero again after it); launches sharing counters must be
-// ordered on one stream.
-cudaError_t launch_box_exchange(const box_desc* boxes, const tile* tiles, int ntiles, bool large, unsigned* counters,
-    int grid, int block, cudaStream_t stream);
-cudaError_t launch_list_exchange(const list_desc* lists, const tile* tiles, int ntiles, bool large, unsigned* counters,
-    int grid, int block, cudaStream_t stream);
-
 // Adjoint over tiles[0, ntiles) whose owner elements are pairwise distinct:
 // owner += halo (owner -= halo for negated components); halo = 0. Float and double only.
+// CTAs claim tiles through counters[0..1] (zero before the launch, zero again after it);
+// launches sharing counters must be ordered on one stream. block <= 512.
 cudaError_t launch_box_adjoint(const box_desc* boxes, const tile* tiles, int ntiles, unsigned* counters, int grid,
     int block, cudaStream_t stream);
 cudaError_t launch_list_adjoint(const list_desc* lists, const tile* tiles, int ntiles, unsigned* counters, int grid,
@@ -28,6 +20,4 @@ cudaError_t launch_list_adjoint(const list_desc* lists, const tile* tiles, int n
 // `sink` receives a value only when the data sum to a sentinel that a zero-filled buffer never
 // produces, which keeps the loads alive.
 cudaError_t launch_l2_flush(const uint4* buf, size_t n16, unsigned* sink, int grid, cudaStream_t stream);
-
-constexpr int k_max_block = 512;
 } // namespace ghexb

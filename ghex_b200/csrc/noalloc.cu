@@ -8,8 +8,7 @@
 //
 // The array is k_noalloc_scratch_bytes large and exists once per device for as long as the
 // library is loaded. Every call rebuilds the tables on the host, copies them into the array on the
-// caller's stream (the scheduler counters, which must start at zero, are part of that copy) and
-// launches the batched kernels on the same stream. All calls share the array, which keeps the
+// caller's stream and launches the batched kernel on the same stream. All calls share the array, which keeps the
 // contents of the last call: calls whose work overlaps on the GPU (on different streams, without
 // ordering between them) race on it and must not be made.
 #include <cuda_runtime.h>
@@ -18,7 +17,7 @@
 #include <map>
 #include <mutex>
 
-#include "kernels.hpp"
+#include "exchange.hpp"
 #include "plan.hpp"
 
 namespace
@@ -65,57 +64,27 @@ extern "C" int ghexb_exchange_noalloc(ghexb_context ctx, const ghexb_field* fiel
         // host tables of the batched form at the default tuning
         ghexb_plan_s plan;
         ghexb::build_tables(plan, ctx, fields, n);
-        ghexb::build_tiles(plan);
 
-        // layout: counters | boxes | lists | index lists | tiles of the four classes
-        constexpr int k_classes = ghexb_plan_s::k_classes;
-        const size_t off_ctr = 0;
-        const size_t off_box = align16(off_ctr + 2 * k_classes * sizeof(unsigned));
-        const size_t off_list = align16(off_box + plan.boxes.size() * sizeof(ghexb::box_desc));
-        const size_t off_idx = align16(off_list + plan.lists.size() * sizeof(ghexb::list_desc));
-        size_t off_tiles[k_classes];
-        size_t end = align16(off_idx + plan.idx.size() * sizeof(int32_t));
-        for (int c = 0; c < k_classes; ++c)
-        {
-            off_tiles[c] = end;
-            end = align16(end + plan.ftiles[c].size() * sizeof(ghexb::tile));
-        }
+        // layout: index lists | forward tiles (the tiles carry everything else the kernel needs)
+        const size_t off_idx = 0;
+        const size_t off_tiles = align16(off_idx + plan.idx.size() * sizeof(int32_t));
+        unsigned char* dev = scratch_address(ctx->device);
+        ghexb::build_tiles(plan, reinterpret_cast<const int32_t*>(dev + off_idx));
+        const size_t end = align16(off_tiles + plan.xf.size() * sizeof(ghexb::xtile));
         if (end > k_noalloc_scratch_bytes)
             throw ghexb::error(GHEXB_ERR_RANGE, "ghexb_exchange_noalloc: the exchange tables need " + std::to_string(end) +
                                                     " bytes, more than the " + std::to_string(k_noalloc_scratch_bytes) +
                                                     " bytes of the no-alloc scratch; use ghexb_co_exchange");
-
-        unsigned char* dev = scratch_address(ctx->device);
-        // device pointers of the index lists inside the scratch
-        auto* d_idx = reinterpret_cast<int32_t*>(dev + off_idx);
-        for (size_t i = 0; i < plan.lists.size(); ++i)
-        {
-            plan.lists[i].sidx = d_idx + plan.list_idx_off[i];
-            plan.lists[i].didx = d_idx + plan.list_idx_off[i] + plan.lists[i].count;
-        }
-        std::vector<unsigned char> host(end, 0); // counters start at zero
-        put(host, off_box, plan.boxes);
-        put(host, off_list, plan.lists);
+        std::vector<unsigned char> host(end, 0);
         put(host, off_idx, plan.idx);
-        for (int c = 0; c < k_classes; ++c) put(host, off_tiles[c], plan.ftiles[c]);
+        put(host, off_tiles, plan.xf);
 
         auto s = static_cast<cudaStream_t>(stream);
         // from pageable memory: the call returns once the data is staged, so `host` may go
         ghexb::check_cuda(cudaMemcpyAsync(dev, host.data(), end, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync(no-alloc tables)");
-        auto* counters = reinterpret_cast<unsigned*>(dev + off_ctr);
-        auto* boxes = reinterpret_cast<const ghexb::box_desc*>(dev + off_box);
-        auto* lists = reinterpret_cast<const ghexb::list_desc*>(dev + off_list);
-        for (int c = 0; c < k_classes; ++c)
-        {
-            const int nt = (int)plan.ftiles[c].size();
-            if (nt == 0) continue;
-            auto* tiles = reinterpret_cast<const ghexb::tile*>(dev + off_tiles[c]);
-            const int grid = std::min(nt, ctx->num_sms * plan.ctas_per_sm);
-            const cudaError_t e = c < 2
-                ? ghexb::launch_box_exchange(boxes, tiles, nt, c == 0, counters + 2 * c, grid, plan.block, s)
-                : ghexb::launch_list_exchange(lists, tiles, nt, c == 2, counters + 2 * c, grid, plan.block, s);
-            ghexb::check_cuda(e, "exchange kernel launch");
-        }
+        ghexb::check_cuda(ghexb::launch_exchange(reinterpret_cast<const ghexb::xtile*>(dev + off_tiles), (int)plan.xf.size(),
+                              plan.per_thread, plan.block, s),
+            "exchange kernel launch");
         return GHEXB_OK;
     }
     catch (const ghexb::error& e)

@@ -15,6 +15,7 @@
 #include <map>
 #include <unordered_map>
 
+#include "exchange.hpp"
 #include "kernels.hpp"
 #include "plan.hpp"
 
@@ -108,6 +109,8 @@ struct builder
             plan.boxes.push_back(b);
             plan.box_src_slot.push_back(src_slot);
             plan.box_dst_slot.push_back(dst_slot);
+            plan.box_src_off.push_back(b.src - src.data);
+            plan.box_dst_off.push_back(b.dst - dst.data);
             box_owner.push_back(reg);
             box_owner.back().field = src_slot;
         }
@@ -280,6 +283,8 @@ struct builder
             plan.list_idx_off.push_back(idx0);
             plan.list_src_slot.push_back(src_slot);
             plan.list_dst_slot.push_back(dst_slot);
+            plan.list_src_off.push_back(l.src - src.data);
+            plan.list_dst_off.push_back(l.dst - dst.data);
         }
         plan.halo_elements += cnt * L;
         plan.algorithmic_bytes += cnt * L * es * 2;
@@ -312,12 +317,226 @@ struct builder
                 plan.adj_didx_off.push_back(idx0 + cnt + b);
                 plan.adj_src_slot.push_back(src_slot);
                 plan.adj_dst_slot.push_back(dst_slot);
+                plan.adj_src_off.push_back(a.src - src.data);
+                plan.adj_dst_off.push_back(a.dst - dst.data);
                 list_src_field.push_back(src_slot);
             }
             b = e;
         }
     }
 };
+
+
+// ---- box adjoint in gather form ---------------------------------------------------------------
+// The owner elements of a field decompose uniquely into coordinates when its axes, sorted by
+// decreasing element stride, nest: every stride is at least the span of the axes below it.
+struct owner_geometry
+{
+    int nd = 0;
+    std::array<int64_t, 4> os{}, ext{};
+    std::array<int, 4> order{}; // axes by decreasing stride
+    bool ok = false;
+
+    static owner_geometry of(const ghexb_field_s& f)
+    {
+        owner_geometry g;
+        g.nd = f.ndim;
+        for (int a = 0; a < f.ndim; ++a)
+        {
+            if (f.byte_strides[a] <= 0 || f.byte_strides[a] % f.esize) return g;
+            g.os[a] = f.byte_strides[a] / f.esize;
+            g.ext[a] = f.extents[a];
+            g.order[a] = a;
+        }
+        std::stable_sort(g.order.begin(), g.order.begin() + g.nd, [&](int a, int b) { return g.os[a] > g.os[b]; });
+        for (int k = 0; k + 1 < g.nd; ++k)
+        {
+            const int hi = g.order[k], lo = g.order[k + 1];
+            if (g.os[hi] < g.os[lo] * g.ext[lo]) return g;
+        }
+        g.ok = g.nd >= 1 && g.os[g.order[g.nd - 1]] >= 1;
+        return g;
+    }
+
+    bool decompose(int64_t off, std::array<int64_t, 4>& c) const
+    {
+        c = {0, 0, 0, 0};
+        for (int k = 0; k < nd; ++k)
+        {
+            const int a = order[k];
+            c[a] = off / os[a];
+            off -= c[a] * os[a];
+            if (c[a] < 0 || c[a] >= ext[a]) return false;
+        }
+        return off == 0;
+    }
+};
+
+// Cuts the owner regions of the box descriptors of every source field into cells covered by the
+// same descriptors. Returns false (with the reason) when a field's layout has no unique
+// coordinates, a box stride matches no owner axis, or a cell has more than k_max_images images.
+bool build_cells(ghexb_plan_s& plan, std::string& why)
+{
+    plan.cells.clear();
+    struct omap
+    {
+        std::array<int64_t, 4> lo, hi, t;
+        int64_t dst_lo;
+        int dst_slot;
+        uint32_t neg;
+    };
+    std::vector<omap> maps(plan.boxes.size());
+    std::map<int, std::vector<int>> by_slot;
+    for (int i = 0; i < (int)plan.boxes.size(); ++i)
+    {
+        const auto& b = plan.boxes[i];
+        const int slot = plan.box_src_slot[i];
+        const auto& f = plan.fields[slot];
+        const owner_geometry G = owner_geometry::of(f);
+        if (!G.ok)
+        {
+            why = "a field's strides do not nest";
+            return false;
+        }
+        if (plan.box_src_off[i] % f.esize || plan.box_dst_off[i] % f.esize)
+        {
+            why = "a box origin is not element-aligned";
+            return false;
+        }
+        std::array<int64_t, 4> c;
+        if (!G.decompose(plan.box_src_off[i] / f.esize, c))
+        {
+            why = "a box origin has no owner coordinates";
+            return false;
+        }
+        omap m{c, c, {0, 0, 0, 0}, plan.box_dst_off[i] / f.esize, plan.box_dst_slot[i], b.xor_mask != 0 ? 1u : 0u};
+        const int64_t n[3] = {b.n0, b.n1, b.n2}, st[3] = {b.s0, b.s1, b.s2}, dt[3] = {b.d0, b.d1, b.d2};
+        std::array<bool, 4> used{};
+        for (int a = 0; a < 3; ++a)
+        {
+            if (n[a] <= 1) continue;
+            int ax = -1;
+            for (int q = 0; q < G.nd && ax < 0; ++q)
+                if (!used[q] && G.os[q] == (st[a] < 0 ? -st[a] : st[a]) && G.ext[q] >= n[a]) ax = q;
+            if (ax < 0)
+            {
+                why = "a box stride matches no owner axis";
+                return false;
+            }
+            used[ax] = true;
+            if (st[a] > 0) m.hi[ax] = c[ax] + n[a] - 1;
+            else
+            {
+                m.lo[ax] = c[ax] - (n[a] - 1);
+                m.dst_lo += (n[a] - 1) * dt[a];
+            }
+            m.t[ax] = st[a] > 0 ? dt[a] : -dt[a];
+            if (m.lo[ax] < 0 || m.hi[ax] >= G.ext[ax])
+            {
+                why = "a box leaves its owner field";
+                return false;
+            }
+        }
+        maps[i] = m;
+        by_slot[slot].push_back(i);
+    }
+    for (const auto& kv : by_slot)
+    {
+        const int slot = kv.first;
+        const auto& ids = kv.second;
+        const auto& f = plan.fields[slot];
+        const owner_geometry G = owner_geometry::of(f);
+        std::array<std::vector<int64_t>, 4> bp;
+        int64_t ncells = 1;
+        for (int a = 0; a < G.nd; ++a)
+        {
+            for (int i : ids)
+            {
+                bp[a].push_back(maps[i].lo[a]);
+                bp[a].push_back(maps[i].hi[a] + 1);
+            }
+            std::sort(bp[a].begin(), bp[a].end());
+            bp[a].erase(std::unique(bp[a].begin(), bp[a].end()), bp[a].end());
+            ncells *= (int64_t)bp[a].size() - 1;
+        }
+        if (ncells > (int64_t(1) << 22))
+        {
+            why = "too many adjoint cells";
+            return false;
+        }
+        std::array<int64_t, 4> j{0, 0, 0, 0};
+        for (int64_t cell = 0; cell < ncells; ++cell)
+        {
+            int64_t r = cell;
+            std::array<int64_t, 4> lo{0, 0, 0, 0}, hi{0, 0, 0, 0};
+            for (int a = 0; a < G.nd; ++a)
+            {
+                const int64_t m = (int64_t)bp[a].size() - 1;
+                j[a] = r % m;
+                r /= m;
+                lo[a] = bp[a][j[a]];
+                hi[a] = bp[a][j[a] + 1] - 1;
+            }
+            std::vector<int> cover;
+            for (int i : ids)
+            {
+                bool in = true;
+                for (int a = 0; a < G.nd && in; ++a) in = maps[i].lo[a] <= lo[a] && hi[a] <= maps[i].hi[a];
+                if (in) cover.push_back(i);
+            }
+            if (cover.empty()) continue;
+            if ((int)cover.size() > k_max_images)
+            {
+                why = "an owner element has more than " + std::to_string(k_max_images) + " halo images";
+                return false;
+            }
+            // cell axes: extents > 1 by increasing owner stride; axes beyond three are unrolled
+            std::vector<int> axes;
+            for (int a = 0; a < G.nd; ++a)
+                if (hi[a] > lo[a]) axes.push_back(a);
+            std::stable_sort(axes.begin(), axes.end(), [&](int a, int b) { return G.os[a] < G.os[b]; });
+            std::vector<int> extra(axes.begin() + std::min<size_t>(3, axes.size()), axes.end());
+            axes.resize(std::min<size_t>(3, axes.size()));
+            int64_t nsub = 1;
+            for (int a : extra) nsub *= hi[a] - lo[a] + 1;
+            for (int64_t sub = 0; sub < nsub; ++sub)
+            {
+                std::array<int64_t, 4> base = lo;
+                int64_t rr = sub;
+                for (int a : extra)
+                {
+                    base[a] = lo[a] + rr % (hi[a] - lo[a] + 1);
+                    rr /= hi[a] - lo[a] + 1;
+                }
+                gcell g{};
+                g.own_slot = slot;
+                g.esize = f.esize;
+                g.own_off = 0;
+                for (int a = 0; a < G.nd; ++a) g.own_off += base[a] * G.os[a];
+                for (int q = 0; q < 3; ++q)
+                {
+                    g.n[q] = q < (int)axes.size() ? (int32_t)(hi[axes[q]] - lo[axes[q]] + 1) : 1;
+                    g.o[q] = q < (int)axes.size() ? (int32_t)G.os[axes[q]] : 0;
+                }
+                g.nimg = (int)cover.size();
+                for (int k = 0; k < g.nimg; ++k)
+                {
+                    const omap& m = maps[cover[k]];
+                    auto& im = g.img[k];
+                    im.slot = m.dst_slot;
+                    im.off = m.dst_lo;
+                    for (int a = 0; a < G.nd; ++a) im.off += (base[a] - m.lo[a]) * m.t[a];
+                    for (int q = 0; q < 3; ++q) im.t[q] = q < (int)axes.size() ? (int32_t)m.t[axes[q]] : 0;
+                    im.neg = m.neg;
+                }
+                plan.cells.push_back(g);
+            }
+        }
+    }
+    // cells with the most images first: the longest CTAs start in the first wave
+    std::stable_sort(plan.cells.begin(), plan.cells.end(), [](const gcell& a, const gcell& b) { return a.nimg > b.nimg; });
+    return true;
+}
 
 } // namespace
 
@@ -461,7 +680,7 @@ void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* f
             plan.list_phase[i] = ph;
         }
     }
-
+    plan.gather_ok = plan.adjoint_ok && build_cells(plan, plan.gather_reason);
 }
 
 void upload_plan(ghexb_plan_s& plan)
@@ -480,11 +699,12 @@ void upload_plan(ghexb_plan_s& plan)
     }
     upload(plan.d_boxes, plan.boxes);
     upload(plan.d_lists, plan.lists);
-    // two scheduler counters per forward tile class and per adjoint kernel
-    upload(plan.d_counters, std::vector<unsigned>(2 * (ghexb_plan_s::k_classes + 2), 0u));
+    // two scheduler counters per phased adjoint kernel
+    upload(plan.d_counters, std::vector<unsigned>(4, 0u));
     upload(plan.d_adj_lists, plan.adj_lists);
     check_cuda(cudaStreamCreateWithFlags(&plan.cap_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     retile(plan);
+    check_cuda(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
 }
 
 void build_plan(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* fields, int n)
@@ -517,148 +737,297 @@ void check_offset(const ghexb_field_s& f, const char* base, int64_t rel, int64_t
 }
 } // namespace
 
-int64_t check_tables(const ghexb_plan_s& plan)
+int64_t check_tables(ghexb_plan_s& plan)
 {
+    build_tiles(plan, plan.idx.data());
     int64_t checked = 0;
-    for (size_t i = 0; i < plan.boxes.size(); ++i)
-    {
-        const auto& b = plan.boxes[i];
-        const auto& sf = plan.fields[plan.box_src_slot[i]];
-        const auto& df = plan.fields[plan.box_dst_slot[i]];
+    // forward tiles, with the element decomposition of exchange.cu
+    auto replay = [&](const xtile& t, const ghexb_field_s& sf, const ghexb_field_s& df) {
+        const int64_t k = t.unit / sf.esize; // elements per unit
         const int64_t ss = field_span(sf), ds = field_span(df);
-        if (b.n0 < 1 || b.n0 > 256 || b.map.j * (1 << b.map.wlog) < b.n0 || b.map.p * b.map.j > 8)
-            throw error(GHEXB_ERR_INTERNAL, "invalid row mapping");
-        const uint32_t rows = (uint32_t)((int64_t)b.n1 * b.n2);
-        for (uint32_t r = 0; r < rows; ++r)
+        for (uint32_t e = 0; e < t.count; ++e)
         {
-            // the row decomposition of box_issue / box_drain / box_adjoint_rows in kernels.cu
-            const uint32_t q = b.div1.div(r);
-            const int64_t i1 = (int64_t)(r - q * (uint32_t)b.n1), i2 = q;
-            if (i1 >= b.n1 || i2 >= b.n2) throw error(GHEXB_ERR_INTERNAL, "box decomposition out of range");
-            for (int i0 = 0; i0 < b.n0; ++i0)
+            const uint32_t g = t.e0 + e;
+            int64_t so, dof;
+            if (t.kind == 0)
             {
-                check_offset(sf, b.src, i0 * (int64_t)b.s0 + i1 * b.s1 + i2 * b.s2, ss, "source");
-                check_offset(df, b.dst, i0 * (int64_t)b.d0 + i1 * b.d1 + i2 * b.d2, ds, "destination");
+                const uint32_t r = fast_div{t.n0, t.m0, t.l0}.div(g);
+                const int64_t i0 = g - r * t.n0;
+                const uint32_t i2 = fast_div{t.n1, t.m1, t.l1}.div(r);
+                const int64_t i1 = r - i2 * t.n1;
+                if (i0 < 0 || i0 >= t.n0 || i1 < 0 || i1 >= t.n1)
+                    throw error(GHEXB_ERR_INTERNAL, "box element decomposition out of range");
+                so = i0 * t.s0 + i1 * t.s1 + (int64_t)i2 * t.s2;
+                dof = i0 * t.d0 + i1 * t.d1 + (int64_t)i2 * t.d2;
             }
+            else
+            {
+                const uint32_t col = fast_div{t.n0, t.m0, t.l0}.div(g);
+                const int64_t lev = g - col * t.n0;
+                so = (int64_t)t.sidx[col] * t.s0 + lev * t.s1;
+                dof = (int64_t)t.didx[col] * t.d0 + lev * t.d1;
+            }
+            check_offset(sf, t.src, so * k, ss, "source");
+            check_offset(sf, t.src, so * k + k - 1, ss, "source");
+            check_offset(df, t.dst, dof * k, ds, "destination");
+            check_offset(df, t.dst, dof * k + k - 1, ds, "destination");
         }
-        checked += (int64_t)rows * b.n0;
+        return (int64_t)t.count;
+    };
+    const int cap = forward_per_thread(plan.per_thread, 8) * plan.block;
+    for (size_t i = 0; i < plan.boxes.size(); ++i)
+        for (int k = plan.xp_box[i].first; k < plan.xp_box[i].first + plan.xp_box[i].second; ++k)
+        {
+            if ((int)plan.xp[k].count > cap) throw error(GHEXB_ERR_INTERNAL, "forward tile too large");
+            checked += replay(plan.xp[k], plan.fields[plan.box_src_slot[i]], plan.fields[plan.box_dst_slot[i]]);
+        }
+    for (size_t i = 0; i < plan.lists.size(); ++i)
+        for (int k = plan.xp_list[i].first; k < plan.xp_list[i].first + plan.xp_list[i].second; ++k)
+        {
+            if ((int)plan.xp[k].count > forward_per_thread(plan.per_thread, plan.xp[k].unit) * plan.block)
+                throw error(GHEXB_ERR_INTERNAL, "forward tile too large");
+            checked += replay(plan.xp[k], plan.fields[plan.list_src_slot[i]], plan.fields[plan.list_dst_slot[i]]);
+        }
+    if (plan.xf.size() != plan.xp.size()) throw error(GHEXB_ERR_INTERNAL, "batched and per-field tables differ");
+
+    // gather cells: every element in bounds, every owner and every image touched exactly once,
+    // and the images are exactly the destination elements of the box descriptors
+    if (plan.gather_ok)
+    {
+        std::vector<std::pair<int, int64_t>> owners, images, box_dst;
+        for (const auto& g : plan.cells)
+        {
+            const auto& of = plan.fields[g.own_slot];
+            const int64_t os = field_span(of);
+            for (int32_t c = 0; c < g.n[2]; ++c)
+                for (int32_t b = 0; b < g.n[1]; ++b)
+                    for (int32_t a = 0; a < g.n[0]; ++a)
+                    {
+                        const int64_t o = g.own_off + (int64_t)a * g.o[0] + (int64_t)b * g.o[1] + (int64_t)c * g.o[2];
+                        if (o < 0 || o >= os) throw error(GHEXB_ERR_RANGE, "adjoint owner outside its field");
+                        owners.push_back({g.own_slot, o});
+                        for (int k = 0; k < g.nimg; ++k)
+                        {
+                            const auto& im = g.img[k];
+                            const int64_t h = im.off + (int64_t)a * im.t[0] + (int64_t)b * im.t[1] + (int64_t)c * im.t[2];
+                            if (h < 0 || h >= field_span(plan.fields[im.slot]))
+                                throw error(GHEXB_ERR_RANGE, "adjoint image outside its field");
+                            images.push_back({im.slot, h});
+                        }
+                    }
+        }
+        for (size_t i = 0; i < plan.boxes.size(); ++i)
+        {
+            const auto& b = plan.boxes[i];
+            const int slot = plan.box_dst_slot[i];
+            const int64_t base = plan.box_dst_off[i] / plan.fields[slot].esize;
+            for (int32_t c = 0; c < b.n2; ++c)
+                for (int32_t r = 0; r < b.n1; ++r)
+                    for (int32_t a = 0; a < b.n0; ++a)
+                        box_dst.push_back({slot, base + (int64_t)a * b.d0 + (int64_t)r * b.d1 + (int64_t)c * b.d2});
+        }
+        std::sort(owners.begin(), owners.end());
+        if (std::adjacent_find(owners.begin(), owners.end()) != owners.end())
+            throw error(GHEXB_ERR_INTERNAL, "an owner element lies in two adjoint cells");
+        std::sort(images.begin(), images.end());
+        std::sort(box_dst.begin(), box_dst.end());
+        if (images != box_dst) throw error(GHEXB_ERR_INTERNAL, "adjoint images differ from the forward destinations");
+        checked += (int64_t)images.size();
     }
-    auto check_list = [&](const list_desc& l, int64_t s_off, int64_t d_off, const ghexb_field_s& sf,
-                          const ghexb_field_s& df) {
-        const int64_t k = l.unit / sf.esize; // elements per unit
+    // phased adjoint lists
+    for (size_t i = 0; i < plan.adj_lists.size(); ++i)
+    {
+        const auto& l = plan.adj_lists[i];
+        const auto& sf = plan.fields[plan.adj_src_slot[i]];
+        const auto& df = plan.fields[plan.adj_dst_slot[i]];
+        const int64_t k = l.unit / sf.esize;
         const int64_t ss = field_span(sf), ds = field_span(df);
-        if (l.levels < 1 || l.levels > 256) throw error(GHEXB_ERR_INTERNAL, "invalid list descriptor");
         for (int32_t col = 0; col < l.count; ++col)
             for (int32_t lev = 0; lev < l.levels; ++lev)
             {
-                const int64_t so = ((int64_t)plan.idx[s_off + col] * l.s_is + (int64_t)lev * l.s_ls) * k;
-                const int64_t dof = ((int64_t)plan.idx[d_off + col] * l.d_is + (int64_t)lev * l.d_ls) * k;
-                check_offset(sf, l.src, so, ss, "source");
-                check_offset(sf, l.src, so + k - 1, ss, "source");
-                check_offset(df, l.dst, dof, ds, "destination");
-                check_offset(df, l.dst, dof + k - 1, ds, "destination");
+                check_offset(sf, l.src, ((int64_t)plan.idx[plan.adj_idx_off[i] + col] * l.s_is + (int64_t)lev * l.s_ls) * k, ss, "source");
+                check_offset(df, l.dst, ((int64_t)plan.idx[plan.adj_didx_off[i] + col] * l.d_is + (int64_t)lev * l.d_ls) * k, ds, "destination");
             }
-        return (int64_t)l.count * l.levels;
-    };
-    for (size_t i = 0; i < plan.lists.size(); ++i)
-        checked += check_list(plan.lists[i], plan.list_idx_off[i], plan.list_idx_off[i] + plan.lists[i].count,
-            plan.fields[plan.list_src_slot[i]], plan.fields[plan.list_dst_slot[i]]);
-    for (size_t i = 0; i < plan.adj_lists.size(); ++i)
-        checked += check_list(plan.adj_lists[i], plan.adj_idx_off[i], plan.adj_didx_off[i],
-            plan.fields[plan.adj_src_slot[i]], plan.fields[plan.adj_dst_slot[i]]);
+        checked += (int64_t)l.count * l.levels;
+    }
     return checked;
 }
 
-void retile(ghexb_plan_s& plan)
+namespace
+{
+// device buffer of at least n elements; returns true when it was (re)allocated
+template<typename T>
+bool ensure(T*& dptr, size_t& cap, size_t n)
+{
+    if (n <= cap && dptr) return false;
+    if (dptr) cudaFree(dptr), dptr = nullptr;
+    cap = 0;
+    if (n == 0) return true;
+    check_cuda(cudaMalloc(&dptr, n * sizeof(T)), "cudaMalloc(plan tiles)");
+    cap = n;
+    return true;
+}
+
+template<typename T>
+void copy_async(T* dptr, const std::vector<T>& v, cudaStream_t stream)
+{
+    if (!v.empty())
+        check_cuda(cudaMemcpyAsync(dptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream),
+            "cudaMemcpyAsync(plan tiles)");
+}
+} // namespace
+
+void retile(ghexb_plan_s& plan, cudaStream_t stream)
 {
     release_graph(plan);
-    build_tiles(plan);
-    for (int c = 0; c < ghexb_plan_s::k_classes; ++c)
-    {
-        upload(plan.d_ftiles[c], plan.ftiles[c]);
-        upload(plan.d_ptiles[c], plan.ptiles[c]);
-    }
+    build_tiles(plan, plan.d_idx);
+    size_t cap_xp = plan.cap_x;
+    ensure(plan.d_xf, plan.cap_x, plan.xf.size());
+    ensure(plan.d_xp, cap_xp, plan.xp.size());
+    ensure(plan.d_gt, plan.cap_gt, plan.gt.size());
+    copy_async(plan.d_xf, plan.xf, stream);
+    copy_async(plan.d_xp, plan.xp, stream);
+    copy_async(plan.d_gt, plan.gt, stream);
     upload(plan.d_adj_btiles, plan.adj_btiles);
     upload(plan.d_adj_ltiles, plan.adj_ltiles);
 }
 
-void build_tiles(ghexb_plan_s& plan)
+void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
 {
-    // Tiles are row ranges. A tile holds about tile_elems elements, fewer for short rows: a row of
-    // n0 elements touches at least one 32-byte sector, so the cost per element grows as rows
-    // shrink below 256 bytes.
-    auto box_rows = [&](int i) { return (int64_t)plan.boxes[i].n1 * plan.boxes[i].n2; };
-    auto box_len = [&](int i) {
-        const auto& b = plan.boxes[i];
-        const int64_t rb = std::min<int64_t>(std::max<int64_t>((int64_t)b.n0 * b.esize, 32), 256);
-        const int64_t elems = std::max<int64_t>(256, plan.tile_elems * rb / 256);
-        return std::max<int64_t>(1, elems / b.n0);
+    // ---- forward
+    const int B = plan.block;
+    auto cap = [&](int unit) { return (uint32_t)(forward_per_thread(plan.per_thread, unit) * B); };
+    // Short rows cost a memory request per row rather than per 32 elements: their tiles shrink by
+    // the row's useful bytes over the bytes of the sectors it touches, so that the requests of
+    // x-face boxes spread over as many CTAs (and SMs) as their bytes would.
+    auto row_cap = [&](int unit, int64_t row_elems) {
+        const int64_t w = row_elems * unit;
+        const int64_t c = (int64_t)cap(unit) * w / (w + 32);
+        return (uint32_t)std::max<int64_t>(B, std::min<int64_t>(cap(unit), c));
     };
-    auto list_len = [&](const list_desc& l) { return std::max<int64_t>(1, plan.tile_elems / l.levels); };
-    auto box_class = [&](int i) { return plan.boxes[i].esize >= 4 ? 0 : 1; };
-    auto list_class = [&](int i) { return plan.lists[i].unit >= 8 ? 2 : 3; };
+    auto box_tiles = [&](int i, std::vector<xtile>& out) {
+        const auto& b = plan.boxes[i];
+        const fast_div f0 = fast_div::make((uint32_t)b.n0), f1 = fast_div::make((uint32_t)b.n1);
+        const uint32_t n = (uint32_t)((int64_t)b.n0 * b.n1 * b.n2), c = row_cap((int)b.esize, b.n0);
+        for (uint32_t e0 = 0; e0 < n; e0 += c)
+        {
+            xtile t{};
+            t.src = b.src, t.dst = b.dst;
+            t.e0 = e0, t.count = std::min(c, n - e0);
+            t.s0 = b.s0, t.s1 = b.s1, t.s2 = b.s2;
+            t.d0 = b.d0, t.d1 = b.d1, t.d2 = b.d2;
+            t.n0 = f0.d, t.m0 = f0.m, t.l0 = (uint8_t)f0.l;
+            t.n1 = f1.d, t.m1 = f1.m, t.l1 = (uint8_t)f1.l;
+            t.unit = (uint8_t)b.esize;
+            t.kind = 0;
+            t.neg = b.xor_mask != 0;
+            out.push_back(t);
+        }
+    };
+    auto list_tiles = [&](int i, std::vector<xtile>& out) {
+        const auto& l = plan.lists[i];
+        const fast_div f0 = fast_div::make((uint32_t)l.levels);
+        const uint32_t n = (uint32_t)((int64_t)l.count * l.levels), c = row_cap((int)l.unit, l.levels);
+        for (uint32_t e0 = 0; e0 < n; e0 += c)
+        {
+            xtile t{};
+            t.src = l.src, t.dst = l.dst;
+            t.sidx = idx ? idx + plan.list_idx_off[i] : nullptr;
+            t.didx = idx ? idx + plan.list_idx_off[i] + l.count : nullptr;
+            t.e0 = e0, t.count = std::min(c, n - e0);
+            t.s0 = l.s_is, t.s1 = l.s_ls, t.d0 = l.d_is, t.d1 = l.d_ls;
+            t.n0 = f0.d, t.m0 = f0.m, t.l0 = (uint8_t)f0.l;
+            t.n1 = 1, t.m1 = 1, t.l1 = 0;
+            t.unit = (uint8_t)l.unit;
+            t.kind = 1;
+            out.push_back(t);
+        }
+    };
+    plan.xp.clear();
+    plan.xp_field.assign(plan.n_logical, {0, 0});
+    plan.xp_box.assign(plan.boxes.size(), {0, 0});
+    plan.xp_list.assign(plan.lists.size(), {0, 0});
+    for (int lg = 0; lg < plan.n_logical; ++lg)
+    {
+        const int begin = (int)plan.xp.size();
+        for (int i = 0; i < (int)plan.boxes.size(); ++i)
+            if ((int)plan.boxes[i].field == lg)
+            {
+                const int b0 = (int)plan.xp.size();
+                box_tiles(i, plan.xp);
+                plan.xp_box[i] = {b0, (int)plan.xp.size() - b0};
+            }
+        for (int i = 0; i < (int)plan.lists.size(); ++i)
+            if ((int)plan.lists[i].field == lg)
+            {
+                const int b0 = (int)plan.xp.size();
+                list_tiles(i, plan.xp);
+                plan.xp_list[i] = {b0, (int)plan.xp.size() - b0};
+            }
+        plan.xp_field[lg] = {begin, (int)plan.xp.size() - begin};
+    }
+    // batched: DRAM sectors per element first (a row of w bytes touches about w/32 + 1 sectors)
+    auto cost = [](const xtile& t) {
+        const double w = t.kind == 0 ? (double)t.n0 * t.unit : (double)t.n0 * t.unit;
+        return (w / 32.0 + 1.0) / w * t.unit;
+    };
+    plan.xf = plan.xp;
+    std::stable_sort(plan.xf.begin(), plan.xf.end(), [&](const xtile& a, const xtile& b) { return cost(a) > cost(b); });
+
+    // ---- box adjoint, gather form
+    plan.gt.clear();
+    if (plan.gather_ok)
+    {
+        for (const auto& g : plan.cells)
+        {
+            const uint32_t gc = (uint32_t)(gather_per_thread(g.nimg) * k_gather_block);
+            const auto& of = plan.fields[g.own_slot];
+            const fast_div f0 = fast_div::make((uint32_t)g.n[0]), f1 = fast_div::make((uint32_t)g.n[1]);
+            const uint32_t n = (uint32_t)((int64_t)g.n[0] * g.n[1] * g.n[2]);
+            for (uint32_t e0 = 0; e0 < n; e0 += gc)
+            {
+                gtile t{};
+                t.own = of.data + g.own_off * of.esize;
+                t.e0 = e0, t.count = std::min(gc, n - e0);
+                t.o0 = g.o[0], t.o1 = g.o[1], t.o2 = g.o[2];
+                t.n0 = f0.d, t.m0 = f0.m, t.l0 = (uint8_t)f0.l;
+                t.n1 = f1.d, t.m1 = f1.m, t.l1 = (uint8_t)f1.l;
+                t.esize = (uint8_t)g.esize;
+                t.nimg = (uint8_t)g.nimg;
+                for (int k = 0; k < g.nimg; ++k)
+                {
+                    const auto& df = plan.fields[g.img[k].slot];
+                    t.img[k].ptr = df.data + g.img[k].off * df.esize;
+                    t.img[k].t0 = g.img[k].t[0], t.img[k].t1 = g.img[k].t[1], t.img[k].t2 = g.img[k].t[2];
+                    t.img[k].neg = g.img[k].neg;
+                }
+                plan.gt.push_back(t);
+            }
+        }
+    }
+
+    // ---- phased adjoint kernels (boxes without a gather form, lists)
+    auto box_rows = [&](int i) { return (int64_t)plan.boxes[i].n1 * plan.boxes[i].n2; };
+    auto box_len = [&](int i) { return std::max<int64_t>(1, 4096 / plan.boxes[i].n0); };
+    auto list_len = [&](const list_desc& l) { return std::max<int64_t>(1, 4096 / l.levels); };
     auto split = [&](int desc, int kind, int64_t rows, int64_t len, std::vector<tile>& out) {
         for (int64_t st = 0; st < rows; st += len)
             out.push_back(tile{desc, kind, (uint32_t)st, (uint32_t)std::min<int64_t>(len, rows - st)});
     };
-    // the batched table hands out the most expensive descriptors (shortest rows) first
-    std::vector<int> box_order(plan.boxes.size());
-    for (size_t i = 0; i < box_order.size(); ++i) box_order[i] = (int)i;
-    std::stable_sort(box_order.begin(), box_order.end(), [&](int a, int b) {
-        return (int64_t)plan.boxes[a].n0 * plan.boxes[a].esize < (int64_t)plan.boxes[b].n0 * plan.boxes[b].esize;
-    });
-    plan.box_range.assign(plan.boxes.size(), {0, 0});
-    plan.list_range.assign(plan.lists.size(), {0, 0});
-    for (int c = 0; c < ghexb_plan_s::k_classes; ++c)
-    {
-        auto& F = plan.ftiles[c];
-        auto& P = plan.ptiles[c];
-        F.clear();
-        P.clear();
-        plan.logical_range[c].assign(plan.n_logical, {0, 0});
-        if (c < 2)
-        {
-            for (int i : box_order)
-                if (box_class(i) == c) split(i, 0, box_rows(i), box_len(i), F);
-        }
-        else
-            for (int i = 0; i < (int)plan.lists.size(); ++i)
-                if (list_class(i) == c) split(i, 1, plan.lists[i].count, list_len(plan.lists[i]), F);
-        for (int lg = 0; lg < plan.n_logical; ++lg)
-        {
-            const int begin = (int)P.size();
-            if (c < 2)
-                for (int i : box_order)
-                {
-                    if ((int)plan.boxes[i].field != lg || box_class(i) != c) continue;
-                    const int b0 = (int)P.size();
-                    split(i, 0, box_rows(i), box_len(i), P);
-                    plan.box_range[i] = {b0, (int)P.size() - b0};
-                }
-            else
-                for (int i = 0; i < (int)plan.lists.size(); ++i)
-                {
-                    if ((int)plan.lists[i].field != lg || list_class(i) != c) continue;
-                    const int b0 = (int)P.size();
-                    split(i, 1, plan.lists[i].count, list_len(plan.lists[i]), P);
-                    plan.list_range[i] = {b0, (int)P.size() - b0};
-                }
-            plan.logical_range[c][lg] = {begin, (int)P.size() - begin};
-        }
-    }
-    // adjoint: grouped by phase
     plan.adj_btiles.clear();
     plan.adj_ltiles.clear();
     plan.adj_bphase_range.clear();
     plan.adj_lphase_range.clear();
     int nph = 0;
-    for (int p : plan.box_phase) nph = std::max(nph, p + 1);
+    if (!plan.gather_ok)
+        for (int p : plan.box_phase) nph = std::max(nph, p + 1);
     for (int p : plan.list_phase) nph = std::max(nph, p + 1);
     for (int ph = 0; ph < nph; ++ph)
     {
         int begin = (int)plan.adj_btiles.size();
-        for (int i : box_order)
-            if (plan.box_phase[i] == ph) split(i, 0, box_rows(i), box_len(i), plan.adj_btiles);
+        if (!plan.gather_ok)
+            for (int i = 0; i < (int)plan.boxes.size(); ++i)
+                if (plan.box_phase[i] == ph) split(i, 0, box_rows(i), box_len(i), plan.adj_btiles);
         plan.adj_bphase_range.push_back({begin, (int)plan.adj_btiles.size() - begin});
         begin = (int)plan.adj_ltiles.size();
         for (int i = 0; i < (int)plan.adj_lists.size(); ++i)
@@ -675,30 +1044,19 @@ void release_graph(ghexb_plan_s& plan)
 
 void launch_plan(ghexb_plan_s& plan, int form, cudaStream_t stream)
 {
-    auto run = [&](int c, int begin, int count) {
-        if (count <= 0) return;
-        const tile* t = (form == GHEXB_FORM_BATCHED ? plan.d_ftiles[c] : plan.d_ptiles[c]) + begin;
-        unsigned* ctr = plan.d_counters + 2 * c;
-        const cudaError_t e = c < 2
-            ? launch_box_exchange(plan.d_boxes, t, count, c == 0, ctr, plan.grid(count), plan.block, stream)
-            : launch_list_exchange(plan.d_lists, t, count, c == 2, ctr, plan.grid(count), plan.block, stream);
-        check_cuda(e, "exchange kernel launch");
+    auto run = [&](const xtile* base, std::pair<int, int> r) {
+        if (r.second <= 0) return;
+        check_cuda(launch_exchange(base + r.first, r.second, plan.per_thread, plan.block, stream), "exchange kernel launch");
     };
     switch (form)
     {
-        case GHEXB_FORM_BATCHED:
-            for (int c = 0; c < ghexb_plan_s::k_classes; ++c) run(c, 0, (int)plan.ftiles[c].size());
-            break;
+        case GHEXB_FORM_BATCHED: run(plan.d_xf, {0, (int)plan.xf.size()}); break;
         case GHEXB_FORM_PER_FIELD:
-            for (int lg = 0; lg < plan.n_logical; ++lg)
-                for (int c = 0; c < ghexb_plan_s::k_classes; ++c)
-                    run(c, plan.logical_range[c][lg].first, plan.logical_range[c][lg].second);
+            for (const auto& r : plan.xp_field) run(plan.d_xp, r);
             break;
         case GHEXB_FORM_PER_BOX:
-            for (size_t i = 0; i < plan.boxes.size(); ++i)
-                run(plan.boxes[i].esize >= 4 ? 0 : 1, plan.box_range[i].first, plan.box_range[i].second);
-            for (size_t i = 0; i < plan.lists.size(); ++i)
-                run(plan.lists[i].unit >= 8 ? 2 : 3, plan.list_range[i].first, plan.list_range[i].second);
+            for (const auto& r : plan.xp_box) run(plan.d_xp, r);
+            for (const auto& r : plan.xp_list) run(plan.d_xp, r);
             break;
         default: throw error(GHEXB_ERR_INVALID, "unknown exchange form " + std::to_string(form));
     }
@@ -735,19 +1093,68 @@ void graph_launch_plan(ghexb_plan_s& plan, cudaStream_t stream)
 void adjoint_plan(ghexb_plan_s& plan, cudaStream_t stream)
 {
     if (!plan.adjoint_ok) throw error(GHEXB_ERR_INVALID, plan.adjoint_reason);
+    if (plan.gather_ok && !plan.gt.empty())
+        check_cuda(launch_gather(plan.d_gt, (int)plan.gt.size(), stream), "adjoint kernel launch");
+    const int sms = plan.ctx ? plan.ctx->num_sms : 148;
+    auto grid = [&](int n) { return std::min(n, 4 * sms); };
     for (size_t ph = 0; ph < plan.adj_bphase_range.size(); ++ph)
     {
         const auto rb = plan.adj_bphase_range[ph];
         const auto rl = plan.adj_lphase_range[ph];
         if (rb.second > 0)
-            check_cuda(launch_box_adjoint(plan.d_boxes, plan.d_adj_btiles + rb.first, rb.second,
-                           plan.d_counters + 2 * ghexb_plan_s::k_classes, plan.grid(rb.second), plan.block, stream),
+            check_cuda(launch_box_adjoint(plan.d_boxes, plan.d_adj_btiles + rb.first, rb.second, plan.d_counters,
+                           grid(rb.second), 256, stream),
                 "adjoint kernel launch");
         if (rl.second > 0)
-            check_cuda(launch_list_adjoint(plan.d_adj_lists, plan.d_adj_ltiles + rl.first, rl.second,
-                           plan.d_counters + 2 * ghexb_plan_s::k_classes + 2, plan.grid(rl.second), plan.block, stream),
+            check_cuda(launch_list_adjoint(plan.d_adj_lists, plan.d_adj_ltiles + rl.first, rl.second, plan.d_counters + 2,
+                           grid(rl.second), 256, stream),
                 "adjoint kernel launch");
     }
+}
+
+void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stream)
+{
+    if (n != (int)plan.fields.size())
+        throw error(GHEXB_ERR_INVALID, "rebind needs one pointer per field of the plan (" +
+                                           std::to_string(plan.fields.size()) + ")");
+    for (int i = 0; i < n; ++i)
+    {
+        if (!data[i]) throw error(GHEXB_ERR_INVALID, "null data pointer");
+        if (reinterpret_cast<uintptr_t>(data[i]) % plan.fields[i].esize != 0)
+            throw error(GHEXB_ERR_INVALID, "data pointer is not aligned to its element size");
+    }
+    for (size_t i = 0; i < plan.lists.size(); ++i)
+        if (plan.lists[i].unit == 16 && (reinterpret_cast<uintptr_t>(data[plan.list_src_slot[i]]) % 16 ||
+                                           reinterpret_cast<uintptr_t>(data[plan.list_dst_slot[i]]) % 16))
+            throw error(GHEXB_ERR_INVALID, "rebind: 16-byte column alignment of the plan is not met by the new memory");
+    for (int i = 0; i < n; ++i) plan.fields[i].data = static_cast<char*>(data[i]);
+    for (size_t i = 0; i < plan.boxes.size(); ++i)
+    {
+        plan.boxes[i].src = plan.fields[plan.box_src_slot[i]].data + plan.box_src_off[i];
+        plan.boxes[i].dst = plan.fields[plan.box_dst_slot[i]].data + plan.box_dst_off[i];
+    }
+    for (size_t i = 0; i < plan.lists.size(); ++i)
+    {
+        plan.lists[i].src = plan.fields[plan.list_src_slot[i]].data + plan.list_src_off[i];
+        plan.lists[i].dst = plan.fields[plan.list_dst_slot[i]].data + plan.list_dst_off[i];
+    }
+    for (size_t i = 0; i < plan.adj_lists.size(); ++i)
+    {
+        plan.adj_lists[i].src = plan.fields[plan.adj_src_slot[i]].data + plan.adj_src_off[i];
+        plan.adj_lists[i].dst = plan.fields[plan.adj_dst_slot[i]].data + plan.adj_dst_off[i];
+    }
+    // stream-ordered rewrite of the tables; from pageable memory the copies return once staged.
+    // The tile tables keep their size and device address, so a captured graph stays valid.
+    build_tiles(plan, plan.d_idx);
+    copy_async(plan.d_xf, plan.xf, stream);
+    copy_async(plan.d_xp, plan.xp, stream);
+    copy_async(plan.d_gt, plan.gt, stream);
+    auto put = [&](void* dst, const void* src, size_t bytes) {
+        if (bytes) check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync(rebind)");
+    };
+    put(plan.d_boxes, plan.boxes.data(), plan.boxes.size() * sizeof(box_desc));
+    put(plan.d_lists, plan.lists.data(), plan.lists.size() * sizeof(list_desc));
+    put(plan.d_adj_lists, plan.adj_lists.data(), plan.adj_lists.size() * sizeof(list_desc));
 }
 
 void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
@@ -755,13 +1162,11 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
     if (repeats < 1) repeats = 10;
     struct cand
     {
-        int tile, block, cps;
+        int k, block;
     };
     std::vector<cand> cands;
-    for (int tile : {2048, 4096, 8192, 16384, 32768})
-        for (int block : {128, 256, 512})
-            for (int cps : {2, 4, 8, 16})
-                if (block * cps <= 2048 && block * cps >= 512) cands.push_back({tile, block, cps});
+    for (int k : {4, 8, 16})
+        for (int block : {128, 256, 512}) cands.push_back({k, block});
 
     // every timed launch starts with a cold L2: read a buffer of twice the L2 size first
     int l2 = 0;
@@ -777,7 +1182,7 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         if (e1) cudaEventDestroy(e1);
     };
     float best = 1e30f;
-    cand bestc{plan.tile_elems, plan.block, plan.ctas_per_sm};
+    cand bestc{plan.per_thread, plan.block};
     try
     {
         check_cuda(cudaMalloc(&flush, flush_bytes), "cudaMalloc(l2 flush)");
@@ -788,8 +1193,8 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         const int fgrid = (plan.ctx ? plan.ctx->num_sms : 148) * 8;
         for (const auto& c : cands)
         {
-            plan.tile_elems = c.tile, plan.block = c.block, plan.ctas_per_sm = c.cps;
-            retile(plan);
+            plan.per_thread = c.k, plan.block = c.block;
+            retile(plan, stream);
             launch_plan(plan, GHEXB_FORM_BATCHED, stream); // warm-up
             float total = 0.f;
             for (int r = 0; r < repeats; ++r)
@@ -812,8 +1217,9 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         throw;
     }
     cleanup();
-    plan.tile_elems = bestc.tile, plan.block = bestc.block, plan.ctas_per_sm = bestc.cps;
-    retile(plan);
+    plan.per_thread = bestc.k, plan.block = bestc.block;
+    retile(plan, stream);
+    check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
 }
 } // namespace ghexb
 
@@ -821,15 +1227,15 @@ ghexb_plan_s::~ghexb_plan_s()
 {
     ghexb::release_graph(*this);
     if (cap_stream) cudaStreamDestroy(cap_stream);
-    for (void* p : {(void*)d_boxes, (void*)d_lists, (void*)d_adj_lists, (void*)d_idx, (void*)d_ftiles[0],
-             (void*)d_ftiles[1], (void*)d_ftiles[2], (void*)d_ftiles[3], (void*)d_ptiles[0], (void*)d_ptiles[1],
-             (void*)d_ptiles[2], (void*)d_ptiles[3], (void*)d_adj_btiles, (void*)d_adj_ltiles, (void*)d_counters})
+    for (void* p : {(void*)d_boxes, (void*)d_lists, (void*)d_adj_lists, (void*)d_idx, (void*)d_xf, (void*)d_xp,
+             (void*)d_gt, (void*)d_adj_btiles, (void*)d_adj_ltiles, (void*)d_counters})
         if (p) cudaFree(p);
 }
 
-int ghexb_plan_s::grid(int ntiles) const
+int ghexb_plan_s::adjoint_launches() const
 {
-    const int sms = ctx ? ctx->num_sms : 148;
-    const int g = sms * ctas_per_sm;
-    return ntiles < g ? ntiles : g;
+    int n = gather_ok && !gt.empty() ? 1 : 0;
+    for (size_t ph = 0; ph < adj_bphase_range.size(); ++ph)
+        n += (adj_bphase_range[ph].second > 0) + (adj_lphase_range[ph].second > 0);
+    return n;
 }

@@ -26,20 +26,24 @@ struct ghexb_plan_s
     std::vector<int> box_src_slot, box_dst_slot;   // field slots of each box descriptor
     std::vector<int> list_src_slot, list_dst_slot; // field slots of each forward list descriptor
     std::vector<int> adj_src_slot, adj_dst_slot;   // field slots of each adjoint list descriptor
+    std::vector<int64_t> box_src_off, box_dst_off; // byte offsets of descriptor pointers from their fields' data
+    std::vector<int64_t> list_src_off, list_dst_off;
+    std::vector<int64_t> adj_src_off, adj_dst_off;
     int n_logical = 0;
 
-    // Forward tiles in four classes, each with its own kernel instance: box descriptors of 8/4-byte
-    // and of 2/1-byte elements, list descriptors of 16/8-byte and of 4/2/1-byte units. Within a
-    // class, tiles are grouped by logical field, then by descriptor.
-    // ftiles: the batched form's table, most expensive tiles first (dynamic scheduling then fills
-    // the tail with cheap ones); ptiles: the same tiles grouped by logical field for the per-field
-    // and per-box forms.
-    static constexpr int k_classes = 4;
-    std::vector<ghexb::tile> ftiles[k_classes];
-    std::vector<ghexb::tile> ptiles[k_classes];
-    std::vector<std::pair<int, int>> logical_range[k_classes]; // [begin, count) in ptiles per logical field
-    std::vector<std::pair<int, int>> box_range, list_range;    // [begin, count) in ptiles per descriptor
-    // adjoint tiles (box, list) grouped by phase
+    // Forward work: one CTA per xtile (exchange.cu). xf is the batched form's table, the most
+    // expensive tiles (shortest rows: most DRAM sectors per byte) first so that the block
+    // scheduler starts them in the first wave; xp holds the same tiles grouped by logical field,
+    // then by descriptor, for the per-field and per-box forms.
+    std::vector<ghexb::xtile> xf, xp;
+    std::vector<std::pair<int, int>> xp_field;          // [begin, count) in xp per logical field
+    std::vector<std::pair<int, int>> xp_box, xp_list;   // [begin, count) in xp per descriptor
+    // Box adjoint in gather form (gather_ok), else by conflict-free phases of the box descriptors.
+    bool gather_ok = false;
+    std::string gather_reason;
+    std::vector<ghexb::gcell> cells;
+    std::vector<ghexb::gtile> gt;
+    // adjoint tiles of the phased kernels (boxes when !gather_ok, lists) grouped by phase
     std::vector<ghexb::tile> adj_btiles, adj_ltiles;
     std::vector<std::pair<int, int>> adj_bphase_range, adj_lphase_range;
     std::vector<int> box_phase, list_phase;
@@ -49,18 +53,16 @@ struct ghexb_plan_s
     ghexb::list_desc* d_lists = nullptr;
     ghexb::list_desc* d_adj_lists = nullptr;
     int32_t* d_idx = nullptr;
-    ghexb::tile* d_ftiles[k_classes] = {nullptr, nullptr, nullptr, nullptr};
-    ghexb::tile* d_ptiles[k_classes] = {nullptr, nullptr, nullptr, nullptr};
+    ghexb::xtile* d_xf = nullptr;
+    ghexb::xtile* d_xp = nullptr;
+    ghexb::gtile* d_gt = nullptr;
+    size_t cap_x = 0, cap_gt = 0; // elements allocated behind d_xf / d_xp and d_gt
     ghexb::tile* d_adj_btiles = nullptr;
     ghexb::tile* d_adj_ltiles = nullptr;
-    unsigned* d_counters = nullptr; // tile scheduler counters, two per tile class
+    unsigned* d_counters = nullptr; // tile scheduler counters of the phased adjoint kernels
 
-    int64_t num_tiles() const
-    {
-        int64_t n = 0;
-        for (const auto& t : ftiles) n += (int64_t)t.size();
-        return n;
-    }
+    int64_t num_tiles() const { return (int64_t)xf.size(); }
+    int adjoint_launches() const;
 
     // statistics
     int64_t halo_elements = 0;
@@ -69,10 +71,9 @@ struct ghexb_plan_s
     bool adjoint_ok = true;
     std::string adjoint_reason;
 
-    // tuning
-    int tile_elems = 8192;
+    // tuning: elements per thread (4, 8 or 16) and threads per CTA of the forward kernel
+    int per_thread = 8;
     int block = 256;
-    int ctas_per_sm = 4;
 
     // graph of the batched form
     cudaStream_t cap_stream = nullptr;
@@ -80,7 +81,6 @@ struct ghexb_plan_s
     cudaGraphExec_t exec = nullptr;
 
     ~ghexb_plan_s();
-    int grid(int ntiles) const;
 };
 
 namespace ghexb
@@ -93,16 +93,20 @@ void upload_plan(ghexb_plan_s& plan);
 void build_plan(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* fields, int n);
 // Replays on the host the address computation of every element the forward and adjoint kernels
 // touch and checks it against the memory span of its field; returns the number of elements.
-int64_t check_tables(const ghexb_plan_s& plan);
-// Host-only: tile tables of the current tuning (no device memory touched).
-void build_tiles(ghexb_plan_s& plan);
-// build_tiles + upload of the tile tables.
-void retile(ghexb_plan_s& plan);
+int64_t check_tables(ghexb_plan_s& plan);
+// Host-only: forward tiles of the current tuning and the adjoint tiles, addressing the fields'
+// current data; list tiles point into `idx` (the device copy of plan.idx, or any copy of it).
+void build_tiles(ghexb_plan_s& plan, const int32_t* idx);
+// build_tiles + copy of the tile tables to the device on `stream` (allocating only when they grew).
+void retile(ghexb_plan_s& plan, cudaStream_t stream = nullptr);
 void release_graph(ghexb_plan_s& plan);
 void launch_plan(ghexb_plan_s& plan, int form, cudaStream_t stream);
 void graph_launch_plan(ghexb_plan_s& plan, cudaStream_t stream);
 void adjoint_plan(ghexb_plan_s& plan, cudaStream_t stream);
 void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats);
+// Moves the plan to new field memory of the same layout (one pointer per field, in plan order):
+// recomputes the descriptor pointers and rewrites the device tables on `stream`.
+void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stream);
 void check_cuda(cudaError_t e, const char* what);
 // Records a failure for ghexb_last_error() (capi.cu).
 int set_last_error(int code, const std::string& msg);

@@ -61,11 +61,12 @@ typedef struct ghexb_plan_info_t
     int64_t halo_elements;     /* halo elements written per exchange */
     int64_t algorithmic_bytes; /* sum over halo elements of sizeof(T) * (1 read + 1 write) */
     int64_t index_bytes;       /* bytes of index lists read per exchange (unstructured) */
-    int64_t adjoint_phases;    /* conflict-free phases of the adjoint */
-    int32_t tile_elems;        /* current tuning: elements per tile */
+    int64_t adjoint_launches;  /* kernel launches of one adjoint */
+    int64_t adjoint_cells;     /* owner cells of the gather-form box adjoint (0: phased form) */
+    int32_t elems_per_thread;  /* current tuning: elements a thread moves (4, 8 or 16) */
     int32_t block;             /* current tuning: threads per CTA */
-    int32_t ctas_per_sm;       /* current tuning: resident CTAs per SM for the persistent grid */
-    int32_t grid;              /* CTAs of the batched launch */
+    int32_t grid;              /* CTAs of the batched launch: one per tile */
+    int32_t reserved;
 } ghexb_plan_info_t;
 
 /* ---- errors / version ----------------------------------------------------------------- */
@@ -173,8 +174,10 @@ int ghexb_plan_destroy(ghexb_plan plan);
  * GHEXB_ERR_RANGE if one falls outside its field's memory span. */
 int ghexb_plan_check(ghexb_context ctx, const ghexb_field* fields, int n, int64_t* elements_checked);
 int ghexb_plan_get_info(ghexb_plan plan, ghexb_plan_info_t* info);
-/* tile_elems/block/ctas_per_sm <= 0 keep the current value. Invalidates the captured graph. */
-int ghexb_plan_set_tuning(ghexb_plan plan, int tile_elems, int block, int ctas_per_sm);
+/* elems_per_thread (4, 8 or 16) and block (a multiple of 32, at most 512); values <= 0 keep the
+ * current one. A tile holds elems_per_thread * block elements (half as many 16-byte units).
+ * Invalidates the captured graph. */
+int ghexb_plan_set_tuning(ghexb_plan plan, int elems_per_thread, int block);
 /* One forward exchange in the given form, stream-ordered. */
 int ghexb_plan_launch(ghexb_plan plan, int form, void* stream);
 /* The batched form captured once into a CUDA graph and replayed on `stream`. */
@@ -183,7 +186,12 @@ int ghexb_plan_graph_launch(ghexb_plan plan, void* stream);
  * from (negated where the forward negated it), in a fixed order, then the halo is zeroed.
  * Float fields only. */
 int ghexb_plan_adjoint_launch(ghexb_plan plan, void* stream);
-/* Times the candidate tilings on `stream` with CUDA events and keeps the fastest one; the
+/* Moves a plan to new field memory: data[i] replaces the data pointer of the plan's i-th field
+ * (same shape, strides and dtype; the caller guarantees it). The device tables are rewritten on
+ * `stream`, ordered with the plan's launches on that stream. Used by the differentiable exchange,
+ * whose fields and gradients are new tensors at every step. */
+int ghexb_plan_rebind(ghexb_plan plan, void* const* data, int n, void* stream);
+/* Times the candidate tunings on `stream` with CUDA events and keeps the fastest one; the
  * chosen tuning is returned through `info` when it is not NULL. Runs real exchanges. */
 int ghexb_plan_autotune(ghexb_plan plan, void* stream, int repeats, ghexb_plan_info_t* info);
 
@@ -199,6 +207,16 @@ int ghexb_plan_autotune(ghexb_plan plan, void* stream, int repeats, ghexb_plan_i
  * stream capture. All calls share the array and it keeps the last call's tables: calls that
  * overlap on the GPU race on it. */
 int ghexb_exchange_noalloc(ghexb_context ctx, const ghexb_field* fields, int n, void* stream);
+
+/* ---- the compute step of the differentiable-exchange program. No counterpart in GHEX, which
+ * has no stencil: this is the 7-point update x <- x + alpha * L(x) on the interior of each of n
+ * 3-D domains (output halo set to 0), or with adjoint != 0 its transpose (gradient of the
+ * output's interior in, gradient of the whole input array out). dtype GHEXB_F32 or GHEXB_F64;
+ * extents (3 per domain, halo included) and element strides (3 per domain) in x, y, z order;
+ * every extent > 2 * halo, halo >= 1; in[i] and out[i] must not overlap. Arithmetic is
+ * round-to-nearest in a fixed order without fused multiply-adds. */
+int ghexb_stencil7(int dtype, int n, const void* const* in, void* const* out, const int64_t* extents,
+                   const int64_t* strides, int halo, double alpha, int adjoint, void* stream);
 
 #ifdef __cplusplus
 }

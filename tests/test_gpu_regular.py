@@ -50,14 +50,25 @@ def test_cfg1_full_size_bitexact(cuda):
     assert info["algorithmic_bytes"] == 3 * n64 * 16 + 2 * n32 * 8
 
 
-@pytest.mark.parametrize("tile,block,cps", [(64, 32, 1), (1000, 128, 3), (1 << 20, 512, 2)])
-def test_tunings_bitexact(cuda, tile, block, cps):
+@pytest.mark.parametrize("per_thread,block", [(4, 32), (8, 128), (16, 512), (16, 96)])
+def test_tunings_bitexact(cuda, per_thread, block):
     run = RegularRun(W.config1(shape=(50, 40, 12)), cuda)
     expected = run.oracle()
     plan = R.make_exchange_plan(run.ctx, run.bis)
-    plan.set_tuning(tile, block, cps)
-    plan.launch()
-    assert run.mismatches(expected) == {}
+    plan.set_tuning(per_thread, block)
+    for form in (plan.BATCHED, plan.PER_FIELD, plan.PER_BOX):
+        run.reset()
+        plan.launch(form)
+        assert run.mismatches(expected) == {}
+
+
+def test_bad_tuning_rejected(cuda):
+    run = RegularRun(W.config1(shape=(50, 40, 12)), cuda)
+    plan = R.make_exchange_plan(run.ctx, run.bis)
+    with pytest.raises(Exception, match="4, 8 or 16"):
+        plan.set_tuning(5, 128)
+    with pytest.raises(Exception, match="multiple of 32"):
+        plan.set_tuning(8, 100)
 
 
 def test_autotune_then_bitexact(cuda):
@@ -65,7 +76,7 @@ def test_autotune_then_bitexact(cuda):
     expected = run.oracle()
     plan = R.make_exchange_plan(run.ctx, run.bis)
     info = plan.autotune(repeats=2)
-    assert info["tile_elems"] > 0 and info["block"] in (128, 256, 512)
+    assert info["elems_per_thread"] in (4, 8, 16) and info["block"] in (128, 256, 512)
     run.reset()
     plan.graph_launch()
     assert run.mismatches(expected) == {}
@@ -142,7 +153,8 @@ def test_adjoint_bitexact(cuda, cfg):
             grads[name].append(g)
     torch.cuda.synchronize()
     plan = R.make_exchange_plan(run.ctx, run.bis)
-    assert plan.info()["adjoint_phases"] >= 1
+    info = plan.info()
+    assert info["adjoint_launches"] == 1 and info["adjoint_cells"] > 0
     plan.adjoint()
     for halos, specs in w.halo_groups().items():
         doms = [O.Domain(i, f, l) for i, f, l in w.domains]

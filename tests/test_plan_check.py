@@ -55,12 +55,20 @@ def regular_handles(w):
 
 @pytest.mark.parametrize("cfg", ["cfg0", "cfg1", "cfg4"])
 def test_regular_plan_accesses_in_bounds(cfg):
+    """The replay covers every forward element once and, in the gather-form adjoint, every halo
+    image once (owners pairwise distinct, images equal to the forward destinations)."""
+    from oracle import regular as O
     w = {"cfg0": W.config0, "cfg1": W.config1, "cfg4": W.config4}[cfg]()
     ctx, keep, handles = regular_handles(w)
     arr = (C.c_void_p * len(handles))(*handles)
     n = C.c_int64()
     _capi.call("ghexb_plan_check", ctx._h, arr, len(handles), C.byref(n))
-    assert n.value > 0
+    halo = 0
+    for halos, specs in w.halo_groups().items():
+        doms = [O.Domain(i, f, l) for i, f, l in w.domains]
+        pat = O.make_pattern((0,) * w.dim, tuple(k - 1 for k in w.shape), halos, w.periodic, doms)
+        halo += O.halo_cells(pat) * len(specs)
+    assert n.value == 2 * halo
 
 
 def test_check_rejects_too_small_memory():
