@@ -129,7 +129,8 @@ struct alignas(16) xtile
     uint8_t unit;     // bytes per element: 1, 2, 4, 8 or 16
     uint8_t kind;     // 0 box, 1 list
     uint8_t neg;      // 1: flip the sign bit (negated cubed-sphere vector components)
-    uint8_t pad[11];
+    uint8_t cls;      // element class (exchange.hpp): kind, unit and neg in one value
+    uint8_t pad[10];
 };
 static_assert(sizeof(xtile) == 96, "xtile is six 16-byte words");
 
@@ -157,7 +158,8 @@ struct alignas(16) gtile
     uint8_t esize;        // 4 or 8 (float or double)
     uint8_t nimg;         // 1..k_max_images
     gimage img[k_max_images];
-    uint8_t pad[16];
+    uint8_t cls;          // element class (exchange.hpp): esize and nimg in one value
+    uint8_t pad[15];
 };
 static_assert(sizeof(gtile) == 256, "gtile is sixteen 16-byte words");
 

@@ -3,11 +3,13 @@
 // The exchange is pure data movement, latency-bound at halo sizes: a kernel's time is a few
 // dependent memory round trips plus the bytes over HBM bandwidth. The kernels are built for few
 // round trips and many bytes in flight:
-//  * one CTA per tile, no tile loop: the grid is the tile table, CTAs never wait on each other
-//    or on a scheduler, and the hardware block scheduler balances the waves;
+//  * one launch covers every tile; a CTA runs a unit of k_unit_tiles consecutive tiles of one
+//    element class (box or list, element size, negation; for the adjoint the number of images)
+//    in a loop specialised for that class, and the hardware block scheduler balances units
+//    across SMs: no scheduler of ours, no atomics, CTAs never wait on each other;
 //  * a tile record carries everything needed to address its elements (96 bytes forward, 256
-//    bytes adjoint), read once by a few threads into shared memory: one round trip before the
-//    data loads;
+//    bytes adjoint); the next record of the unit is fetched while the current tile's data loads
+//    are in flight, so only a unit's first record costs a round trip of its own;
 //  * every thread issues all of its K loads before its first store, so K elements per thread
 //    are in flight; consecutive threads take consecutive elements, so rows along the
 //    destination's contiguous dimension are coalesced;
@@ -16,6 +18,10 @@
 // A halo element moves from the source interior to the destination halo with one read and one
 // write; no intermediate buffer exists.
 #include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdint>
 
 #include "exchange.hpp"
 
@@ -39,16 +45,45 @@ template<> struct sign_bit<unsigned long long>
 };
 
 template<typename T> __device__ __forceinline__ T ld_stream(const T* p) { return __ldcg(p); }
-template<> __device__ __forceinline__ uint16_t ld_stream(const uint16_t* p) { return __ldcg(reinterpret_cast<const unsigned short*>(p)); }
-template<> __device__ __forceinline__ uint8_t ld_stream(const uint8_t* p) { return __ldcg(reinterpret_cast<const unsigned char*>(p)); }
-
-// Loads the record of this CTA into shared memory (W 16-byte words).
-template<int W, typename R>
-__device__ __forceinline__ void load_record(R& sh, const R* __restrict__ g)
+template<> __device__ __forceinline__ uint16_t ld_stream(const uint16_t* p)
 {
-    if (threadIdx.x < W)
-        reinterpret_cast<uint4*>(&sh)[threadIdx.x] = __ldg(reinterpret_cast<const uint4*>(g) + threadIdx.x);
+    return __ldcg(reinterpret_cast<const unsigned short*>(p));
+}
+template<> __device__ __forceinline__ uint8_t ld_stream(const uint8_t* p)
+{
+    return __ldcg(reinterpret_cast<const unsigned char*>(p));
+}
+
+// Runs body(t) on the k_unit_tiles tiles of this CTA's unit, starting from the record already in
+// shared memory. The next record is fetched into registers (by W threads) before the current
+// tile's body, so that its round trip overlaps the tile's data loads, and replaces the shared
+// record between two barriers after it.
+template<int W, typename R, typename Body>
+__device__ __forceinline__ void unit_loop(R& t, const R* __restrict__ unit, Body body)
+{
+#pragma unroll 1
+    for (int j = 0;; ++j)
+    {
+        const bool more = j + 1 < k_unit_tiles;
+        const bool fetch = more && threadIdx.x < W;
+        uint4 pre = make_uint4(0u, 0u, 0u, 0u);
+        if (fetch) pre = __ldg(reinterpret_cast<const uint4*>(unit + j + 1) + threadIdx.x);
+        body(t);
+        if (!more) break;
+        __syncthreads();
+        if (fetch) reinterpret_cast<uint4*>(&t)[threadIdx.x] = pre;
+        __syncthreads();
+    }
+}
+
+// Loads the first record of this CTA's unit into shared memory.
+template<int W, typename R>
+__device__ __forceinline__ const R* first_record(R& t, const R* __restrict__ tiles)
+{
+    const R* unit = tiles + (size_t)blockIdx.x * k_unit_tiles;
+    if (threadIdx.x < W) reinterpret_cast<uint4*>(&t)[threadIdx.x] = __ldg(reinterpret_cast<const uint4*>(unit) + threadIdx.x);
     __syncthreads();
+    return unit;
 }
 
 // ---- forward ---------------------------------------------------------------------------------
@@ -63,7 +98,7 @@ __device__ __forceinline__ void box_elements(const xtile& t)
     for (int k = 0; k < K; ++k)
     {
         const uint32_t e = k * blockDim.x + threadIdx.x;
-        doff[k] = -1;
+        doff[k] = 0;
         if (e < t.count)
         {
             const uint32_t g = t.e0 + e;
@@ -116,44 +151,33 @@ __device__ __forceinline__ void list_elements(const xtile& t)
 }
 
 template<int K>
-__global__ void __launch_bounds__(k_max_block) exchange_kernel(const xtile* __restrict__ tiles)
+__global__ void __launch_bounds__(k_max_block, K >= 16 ? 1 : 2) exchange_kernel(const xtile* __restrict__ tiles)
 {
     __shared__ xtile t;
-    load_record<6>(t, tiles + blockIdx.x);
-    if (t.kind == 0)
+    const xtile* unit = first_record<6>(t, tiles);
+    switch (t.cls)
     {
-        switch (t.unit)
-        {
-            case 8:
-                if (t.neg) box_elements<K, unsigned long long, true>(t);
-                else
-                    box_elements<K, unsigned long long, false>(t);
-                break;
-            case 4:
-                if (t.neg) box_elements<K, uint32_t, true>(t);
-                else
-                    box_elements<K, uint32_t, false>(t);
-                break;
-            case 2: box_elements<K, uint16_t, false>(t); break;
-            default: box_elements<K, uint8_t, false>(t); break;
-        }
-    }
-    else
-    {
-        switch (t.unit)
-        {
-            case 16: list_elements<(K > 1 ? K / 2 : 1), uint4>(t); break;
-            case 8: list_elements<K, unsigned long long>(t); break;
-            case 4: list_elements<K, uint32_t>(t); break;
-            case 2: list_elements<K, uint16_t>(t); break;
-            default: list_elements<K, uint8_t>(t); break;
-        }
+#define GHEXB_CASE(C, F)                                                                                               \
+    case C: unit_loop<6>(t, unit, [](const xtile& x) { F(x); }); break;
+        GHEXB_CASE(k_box8, (box_elements<K, unsigned long long, false>))
+        GHEXB_CASE(k_box8_neg, (box_elements<K, unsigned long long, true>))
+        GHEXB_CASE(k_box4, (box_elements<K, uint32_t, false>))
+        GHEXB_CASE(k_box4_neg, (box_elements<K, uint32_t, true>))
+        GHEXB_CASE(k_box2, (box_elements<K, uint16_t, false>))
+        GHEXB_CASE(k_box1, (box_elements<K, uint8_t, false>))
+        GHEXB_CASE(k_list16, (list_elements<forward_per_thread(K, 16), uint4>))
+        GHEXB_CASE(k_list8, (list_elements<K, unsigned long long>))
+        GHEXB_CASE(k_list4, (list_elements<K, uint32_t>))
+        GHEXB_CASE(k_list2, (list_elements<K, uint16_t>))
+        GHEXB_CASE(k_list1, (list_elements<K, uint8_t>))
+#undef GHEXB_CASE
+        default: break;
     }
 }
 
 // ---- box adjoint in gather form --------------------------------------------------------------
-// NI images per owner element (the cell's image count, dispatched at run time); all loads of a
-// thread's K owner elements and their images are issued before the first store.
+// NI images per owner element; all loads of a thread's K owner elements and their images are
+// issued before the first store.
 template<int K, int NI, typename F>
 __device__ __forceinline__ void gather_elements(const gtile& t)
 {
@@ -198,40 +222,44 @@ __device__ __forceinline__ void gather_elements(const gtile& t)
         }
 }
 
-template<typename F>
-__device__ __forceinline__ void gather_dispatch(const gtile& t)
-{
-    switch (t.nimg)
-    {
-        case 1: gather_elements<gather_per_thread(1), 1, F>(t); break;
-        case 2: gather_elements<gather_per_thread(2), 2, F>(t); break;
-        case 3: gather_elements<gather_per_thread(3), 3, F>(t); break;
-        case 4: gather_elements<gather_per_thread(4), 4, F>(t); break;
-        case 5: gather_elements<gather_per_thread(5), 5, F>(t); break;
-        case 6: gather_elements<gather_per_thread(6), 6, F>(t); break;
-        case 7: gather_elements<gather_per_thread(7), 7, F>(t); break;
-        default: gather_elements<gather_per_thread(8), 8, F>(t); break;
-    }
-}
-
 __global__ void __launch_bounds__(k_gather_block, 3) gather_kernel(const gtile* __restrict__ tiles)
 {
     __shared__ gtile t;
-    load_record<16>(t, tiles + blockIdx.x);
-    if (t.esize == 8) gather_dispatch<double>(t);
-    else
-        gather_dispatch<float>(t);
+    const gtile* unit = first_record<16>(t, tiles);
+    switch (t.cls)
+    {
+#define GHEXB_CASE(NI)                                                                                                 \
+    case gather_class(8, NI):                                                                                          \
+        unit_loop<16>(t, unit, [](const gtile& x) { gather_elements<gather_per_thread(NI), NI, double>(x); });       \
+        break;                                                                                                         \
+    case gather_class(4, NI):                                                                                          \
+        unit_loop<16>(t, unit, [](const gtile& x) { gather_elements<gather_per_thread(NI), NI, float>(x); });        \
+        break;
+        GHEXB_CASE(1)
+        GHEXB_CASE(2)
+        GHEXB_CASE(3)
+        GHEXB_CASE(4)
+        GHEXB_CASE(5)
+        GHEXB_CASE(6)
+        GHEXB_CASE(7)
+        GHEXB_CASE(8)
+#undef GHEXB_CASE
+        default: break;
+    }
 }
+
 } // namespace
 
 cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cudaStream_t stream)
 {
     if (ntiles <= 0) return cudaSuccess;
+    if (ntiles % k_unit_tiles || block < 32 || block > k_max_block || block % 32) return cudaErrorInvalidValue;
+    const int grid = ntiles / k_unit_tiles;
     switch (k)
     {
-        case 4: exchange_kernel<4><<<ntiles, block, 0, stream>>>(tiles); break;
-        case 8: exchange_kernel<8><<<ntiles, block, 0, stream>>>(tiles); break;
-        case 16: exchange_kernel<16><<<ntiles, block, 0, stream>>>(tiles); break;
+        case 4: exchange_kernel<4><<<grid, block, 0, stream>>>(tiles); break;
+        case 8: exchange_kernel<8><<<grid, block, 0, stream>>>(tiles); break;
+        case 16: exchange_kernel<16><<<grid, block, 0, stream>>>(tiles); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -240,7 +268,8 @@ cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cu
 cudaError_t launch_gather(const gtile* tiles, int ntiles, cudaStream_t stream)
 {
     if (ntiles <= 0) return cudaSuccess;
-    gather_kernel<<<ntiles, k_gather_block, 0, stream>>>(tiles);
+    if (ntiles % k_unit_tiles) return cudaErrorInvalidValue;
+    gather_kernel<<<ntiles / k_unit_tiles, k_gather_block, 0, stream>>>(tiles);
     return cudaGetLastError();
 }
 } // namespace ghexb

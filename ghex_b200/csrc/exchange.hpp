@@ -8,25 +8,62 @@
 namespace ghexb
 {
 constexpr int k_max_block = 512;
-// Elements per thread of a gather tile whose cell has `nimg` images: about sixteen loads in
-// flight per thread (the owner and its images of every element).
-constexpr int gather_per_thread(int nimg)
-{
-    return nimg <= 1 ? 8 : nimg <= 3 ? 4 : 2;
-}
+// Threads per CTA of the gather kernel.
+constexpr int k_gather_block = 256;
 
 // Elements a thread moves in a forward tile of `unit`-byte elements when the kernel runs with
 // K elements per thread (16-byte units take half: their registers are twice as wide).
-constexpr int forward_per_thread(int k, int unit)
+__host__ __device__ constexpr int forward_per_thread(int k, int unit)
 {
     return unit == 16 ? (k > 1 ? k / 2 : 1) : k;
 }
 
-// One CTA per tile: tiles[blockIdx.x] holds at most forward_per_thread(k, unit) * block elements.
-// k is 4, 8 or 16.
+// Elements per thread of a gather tile whose cell has `nimg` images: about sixteen loads in
+// flight per thread (the owner and its images of every element).
+__host__ __device__ constexpr int gather_per_thread(int nimg)
+{
+    return nimg <= 1 ? 8 : nimg <= 3 ? 4 : 2;
+}
+
+// Element classes: each runs its own specialised loop in the kernels.
+enum forward_class : int32_t
+{
+    k_box8 = 0,
+    k_box8_neg,
+    k_box4,
+    k_box4_neg,
+    k_box2,
+    k_box1,
+    k_list16,
+    k_list8,
+    k_list4,
+    k_list2,
+    k_list1,
+    k_forward_classes
+};
+__host__ __device__ constexpr int forward_class_of(int kind, int unit, bool neg)
+{
+    return kind == 0 ? (unit == 8 ? (neg ? k_box8_neg : k_box8)
+                           : unit == 4 ? (neg ? k_box4_neg : k_box4)
+                           : unit == 2 ? k_box2
+                                       : k_box1)
+                     : (unit == 16 ? k_list16 : unit == 8 ? k_list8 : unit == 4 ? k_list4 : unit == 2 ? k_list2 : k_list1);
+}
+// gather classes: (element size, images)
+__host__ __device__ constexpr int gather_class(int esize, int nimg)
+{
+    return (esize == 8 ? 0 : k_max_images) + (nimg - 1);
+}
+constexpr int k_gather_classes = 2 * k_max_images;
+
+// A CTA runs k_unit_tiles consecutive tiles of one class: the tile tables of every launch are
+// padded, per class, to a multiple of k_unit_tiles with empty tiles (count 0) of that class.
+constexpr int k_unit_tiles = 1;
+
+// Forward exchange of tiles[0, ntiles) (ntiles a multiple of k_unit_tiles): a tile holds at most
+// forward_per_thread(k, unit) * block elements; k is 4, 8 or 16.
 cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cudaStream_t stream);
-// Threads per CTA of the gather kernel.
-constexpr int k_gather_block = 256;
-// One CTA per tile: tiles[blockIdx.x] holds at most gather_per_thread(nimg) * k_gather_block elements.
+// Box adjoint of tiles[0, ntiles) (a multiple of k_unit_tiles): a tile holds at most
+// gather_per_thread(nimg) * k_gather_block elements.
 cudaError_t launch_gather(const gtile* tiles, int ntiles, cudaStream_t stream);
 } // namespace ghexb

@@ -737,6 +737,46 @@ void check_offset(const ghexb_field_s& f, const char* base, int64_t rel, int64_t
 }
 } // namespace
 
+namespace
+{
+// Approximate DRAM bytes of a run of `count` elements in rows of `row` elements of `unit` bytes:
+// a row touches about one 32-byte sector more than its bytes.
+double run_cost(int64_t count, int unit, int64_t row)
+{
+    const double w = (double)row * unit;
+    return (double)count * unit * (w + 32.0) / w;
+}
+
+double tile_cost(const xtile& t) { return run_cost(t.count, t.unit, t.n0); }
+
+double tile_cost(const gtile& t) { return run_cost(t.count, t.esize, t.n0) * 2.0 * (1 + t.nimg); }
+
+// Appends the tiles of one launch range, grouped by class (stable), padding every class to a
+// multiple of k_unit_tiles with empty tiles of that class. Returns [begin, count) in out.
+template<typename R, typename ClassOf>
+std::pair<int, int> append_units(std::vector<R>& out, std::vector<R> tiles, ClassOf class_of)
+{
+    std::stable_sort(tiles.begin(), tiles.end(), [&](const R& a, const R& b) { return class_of(a) < class_of(b); });
+    const int begin = (int)out.size();
+    for (size_t i = 0; i < tiles.size();)
+    {
+        size_t j = i;
+        while (j < tiles.size() && class_of(tiles[j]) == class_of(tiles[i])) out.push_back(tiles[j++]);
+        while ((out.size() - begin) % k_unit_tiles)
+        {
+            R pad{};
+            pad.cls = tiles[i].cls;
+            out.push_back(pad);
+        }
+        i = j;
+    }
+    return {begin, (int)out.size() - begin};
+}
+
+int class_of_x(const xtile& t) { return forward_class_of(t.kind, t.unit, t.neg != 0); }
+int class_of_g(const gtile& t) { return gather_class(t.esize, t.nimg); }
+} // namespace
+
 int64_t check_tables(ghexb_plan_s& plan)
 {
     build_tiles(plan, plan.idx.data());
@@ -774,21 +814,46 @@ int64_t check_tables(ghexb_plan_s& plan)
         }
         return (int64_t)t.count;
     };
-    const int cap = forward_per_thread(plan.per_thread, 8) * plan.block;
-    for (size_t i = 0; i < plan.boxes.size(); ++i)
-        for (int k = plan.xp_box[i].first; k < plan.xp_box[i].first + plan.xp_box[i].second; ++k)
+    auto replay_range = [&](std::pair<int, int> r, int src_slot, int dst_slot) {
+        for (int k = r.first; k < r.first + r.second; ++k)
         {
-            if ((int)plan.xp[k].count > cap) throw error(GHEXB_ERR_INTERNAL, "forward tile too large");
-            checked += replay(plan.xp[k], plan.fields[plan.box_src_slot[i]], plan.fields[plan.box_dst_slot[i]]);
-        }
-    for (size_t i = 0; i < plan.lists.size(); ++i)
-        for (int k = plan.xp_list[i].first; k < plan.xp_list[i].first + plan.xp_list[i].second; ++k)
-        {
-            if ((int)plan.xp[k].count > forward_per_thread(plan.per_thread, plan.xp[k].unit) * plan.block)
+            const xtile& t = plan.xb[k];
+            if ((int)t.count > forward_per_thread(plan.per_thread, t.unit) * plan.block)
                 throw error(GHEXB_ERR_INTERNAL, "forward tile too large");
-            checked += replay(plan.xp[k], plan.fields[plan.list_src_slot[i]], plan.fields[plan.list_dst_slot[i]]);
+            if (t.count) checked += replay(t, plan.fields[src_slot], plan.fields[dst_slot]);
         }
-    if (plan.xf.size() != plan.xp.size()) throw error(GHEXB_ERR_INTERNAL, "batched and per-field tables differ");
+    };
+    for (size_t i = 0; i < plan.boxes.size(); ++i) replay_range(plan.xb_box[i], plan.box_src_slot[i], plan.box_dst_slot[i]);
+    for (size_t i = 0; i < plan.lists.size(); ++i)
+        replay_range(plan.xb_list[i], plan.list_src_slot[i], plan.list_dst_slot[i]);
+    // every table: units of one class, tile classes consistent with their elements, and the same
+    // work in the batched, per-field and per-box tables
+    auto check_units = [](const auto& tiles, int begin, int count, auto class_of) {
+        if (count % k_unit_tiles) throw error(GHEXB_ERR_INTERNAL, "launch range not a whole number of units");
+        int64_t elems = 0;
+        for (int u = begin; u < begin + count; u += k_unit_tiles)
+            for (int j = 0; j < k_unit_tiles; ++j)
+            {
+                const auto& t = tiles[u + j];
+                if (t.cls != tiles[u].cls || (t.count && class_of(t) != t.cls))
+                    throw error(GHEXB_ERR_INTERNAL, "a unit mixes element classes");
+                elems += t.count;
+            }
+        return elems;
+    };
+    const int64_t nf = check_units(plan.xf, 0, (int)plan.xf.size(), class_of_x);
+    int64_t np = 0, nb = 0;
+    for (const auto& r : plan.xp_field) np += check_units(plan.xp, r.first, r.second, class_of_x);
+    for (const auto& r : plan.xb_box) nb += check_units(plan.xb, r.first, r.second, class_of_x);
+    for (const auto& r : plan.xb_list) nb += check_units(plan.xb, r.first, r.second, class_of_x);
+    if (nf != nb || np != nb) throw error(GHEXB_ERR_INTERNAL, "batched, per-field and per-box tables differ");
+    if (plan.gather_ok)
+    {
+        check_units(plan.gt, 0, (int)plan.gt.size(), class_of_g);
+        for (const auto& t : plan.gt)
+            if ((int)t.count > gather_per_thread(t.nimg) * k_gather_block)
+                throw error(GHEXB_ERR_INTERNAL, "gather tile too large");
+    }
 
     // gather cells: every element in bounds, every owner and every image touched exactly once,
     // and the images are exactly the destination elements of the box descriptors
@@ -881,12 +946,13 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
 {
     release_graph(plan);
     build_tiles(plan, plan.d_idx);
-    size_t cap_xp = plan.cap_x;
-    ensure(plan.d_xf, plan.cap_x, plan.xf.size());
-    ensure(plan.d_xp, cap_xp, plan.xp.size());
+    ensure(plan.d_xf, plan.cap_xf, plan.xf.size());
+    ensure(plan.d_xp, plan.cap_xp, plan.xp.size());
+    ensure(plan.d_xb, plan.cap_xb, plan.xb.size());
     ensure(plan.d_gt, plan.cap_gt, plan.gt.size());
     copy_async(plan.d_xf, plan.xf, stream);
     copy_async(plan.d_xp, plan.xp, stream);
+    copy_async(plan.d_xb, plan.xb, stream);
     copy_async(plan.d_gt, plan.gt, stream);
     upload(plan.d_adj_btiles, plan.adj_btiles);
     upload(plan.d_adj_ltiles, plan.adj_ltiles);
@@ -943,41 +1009,53 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
             out.push_back(t);
         }
     };
+    // tiles per descriptor, with their element class
+    std::vector<std::vector<xtile>> btiles(plan.boxes.size()), ltiles(plan.lists.size());
+    for (size_t i = 0; i < plan.boxes.size(); ++i)
+    {
+        box_tiles((int)i, btiles[i]);
+        for (auto& t : btiles[i]) t.cls = (uint8_t)class_of_x(t);
+    }
+    for (size_t i = 0; i < plan.lists.size(); ++i)
+    {
+        list_tiles((int)i, ltiles[i]);
+        for (auto& t : ltiles[i]) t.cls = (uint8_t)class_of_x(t);
+    }
+    // per box: one range per descriptor
+    plan.xb.clear();
+    plan.xb_box.assign(plan.boxes.size(), {0, 0});
+    plan.xb_list.assign(plan.lists.size(), {0, 0});
+    for (size_t i = 0; i < plan.boxes.size(); ++i) plan.xb_box[i] = append_units(plan.xb, btiles[i], class_of_x);
+    for (size_t i = 0; i < plan.lists.size(); ++i) plan.xb_list[i] = append_units(plan.xb, ltiles[i], class_of_x);
+    // per field: one range per logical field
     plan.xp.clear();
     plan.xp_field.assign(plan.n_logical, {0, 0});
-    plan.xp_box.assign(plan.boxes.size(), {0, 0});
-    plan.xp_list.assign(plan.lists.size(), {0, 0});
     for (int lg = 0; lg < plan.n_logical; ++lg)
     {
-        const int begin = (int)plan.xp.size();
-        for (int i = 0; i < (int)plan.boxes.size(); ++i)
-            if ((int)plan.boxes[i].field == lg)
-            {
-                const int b0 = (int)plan.xp.size();
-                box_tiles(i, plan.xp);
-                plan.xp_box[i] = {b0, (int)plan.xp.size() - b0};
-            }
-        for (int i = 0; i < (int)plan.lists.size(); ++i)
-            if ((int)plan.lists[i].field == lg)
-            {
-                const int b0 = (int)plan.xp.size();
-                list_tiles(i, plan.xp);
-                plan.xp_list[i] = {b0, (int)plan.xp.size() - b0};
-            }
-        plan.xp_field[lg] = {begin, (int)plan.xp.size() - begin};
+        std::vector<xtile> f;
+        for (size_t i = 0; i < plan.boxes.size(); ++i)
+            if ((int)plan.boxes[i].field == lg) f.insert(f.end(), btiles[i].begin(), btiles[i].end());
+        for (size_t i = 0; i < plan.lists.size(); ++i)
+            if ((int)plan.lists[i].field == lg) f.insert(f.end(), ltiles[i].begin(), ltiles[i].end());
+        plan.xp_field[lg] = append_units(plan.xp, std::move(f), class_of_x);
     }
-    // batched: DRAM sectors per element first (a row of w bytes touches about w/32 + 1 sectors)
-    auto cost = [](const xtile& t) {
-        const double w = t.kind == 0 ? (double)t.n0 * t.unit : (double)t.n0 * t.unit;
-        return (w / 32.0 + 1.0) / w * t.unit;
-    };
-    plan.xf = plan.xp;
-    std::stable_sort(plan.xf.begin(), plan.xf.end(), [&](const xtile& a, const xtile& b) { return cost(a) > cost(b); });
+    // batched: one range; within a class the most DRAM bytes per element (short rows) first, so
+    // that the first wave of CTAs starts on the most expensive tiles
+    {
+        std::vector<xtile> all;
+        for (const auto& v : btiles) all.insert(all.end(), v.begin(), v.end());
+        for (const auto& v : ltiles) all.insert(all.end(), v.begin(), v.end());
+        auto per_elem = [](const xtile& t) { return tile_cost(t) / std::max<uint32_t>(1u, t.count); };
+        std::stable_sort(all.begin(), all.end(), [&](const xtile& x, const xtile& y) { return per_elem(x) > per_elem(y); });
+        plan.xf.clear();
+        append_units(plan.xf, std::move(all), class_of_x);
+    }
 
     // ---- box adjoint, gather form
     plan.gt.clear();
     if (plan.gather_ok)
     {
+        std::vector<gtile> all;
         for (const auto& g : plan.cells)
         {
             const uint32_t gc = (uint32_t)(gather_per_thread(g.nimg) * k_gather_block);
@@ -1001,9 +1079,11 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
                     t.img[k].t0 = g.img[k].t[0], t.img[k].t1 = g.img[k].t[1], t.img[k].t2 = g.img[k].t[2];
                     t.img[k].neg = g.img[k].neg;
                 }
-                plan.gt.push_back(t);
+                t.cls = (uint8_t)class_of_g(t);
+                all.push_back(t);
             }
         }
+        append_units(plan.gt, std::move(all), class_of_g);
     }
 
     // ---- phased adjoint kernels (boxes without a gather form, lists)
@@ -1055,8 +1135,8 @@ void launch_plan(ghexb_plan_s& plan, int form, cudaStream_t stream)
             for (const auto& r : plan.xp_field) run(plan.d_xp, r);
             break;
         case GHEXB_FORM_PER_BOX:
-            for (const auto& r : plan.xp_box) run(plan.d_xp, r);
-            for (const auto& r : plan.xp_list) run(plan.d_xp, r);
+            for (const auto& r : plan.xb_box) run(plan.d_xb, r);
+            for (const auto& r : plan.xb_list) run(plan.d_xb, r);
             break;
         default: throw error(GHEXB_ERR_INVALID, "unknown exchange form " + std::to_string(form));
     }
@@ -1148,6 +1228,7 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
     build_tiles(plan, plan.d_idx);
     copy_async(plan.d_xf, plan.xf, stream);
     copy_async(plan.d_xp, plan.xp, stream);
+    copy_async(plan.d_xb, plan.xb, stream);
     copy_async(plan.d_gt, plan.gt, stream);
     auto put = [&](void* dst, const void* src, size_t bytes) {
         if (bytes) check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync(rebind)");
@@ -1228,8 +1309,15 @@ ghexb_plan_s::~ghexb_plan_s()
     ghexb::release_graph(*this);
     if (cap_stream) cudaStreamDestroy(cap_stream);
     for (void* p : {(void*)d_boxes, (void*)d_lists, (void*)d_adj_lists, (void*)d_idx, (void*)d_xf, (void*)d_xp,
-             (void*)d_gt, (void*)d_adj_btiles, (void*)d_adj_ltiles, (void*)d_counters})
+             (void*)d_xb, (void*)d_gt, (void*)d_adj_btiles, (void*)d_adj_ltiles, (void*)d_counters})
         if (p) cudaFree(p);
+}
+
+int64_t ghexb_plan_s::num_tiles() const
+{
+    int64_t n = 0;
+    for (const auto& t : xf) n += t.count > 0;
+    return n;
 }
 
 int ghexb_plan_s::adjoint_launches() const

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "core.hpp"
+#include "exchange.hpp"
 
 struct ghexb_plan_s
 {
@@ -31,13 +32,13 @@ struct ghexb_plan_s
     std::vector<int64_t> adj_src_off, adj_dst_off;
     int n_logical = 0;
 
-    // Forward work: one CTA per xtile (exchange.cu). xf is the batched form's table, the most
-    // expensive tiles (shortest rows: most DRAM sectors per byte) first so that the block
-    // scheduler starts them in the first wave; xp holds the same tiles grouped by logical field,
-    // then by descriptor, for the per-field and per-box forms.
-    std::vector<ghexb::xtile> xf, xp;
+    // Forward work (exchange.cu): a CTA runs k_unit_tiles consecutive tiles of one element
+    // class. xf is the batched form's table (by class, the most expensive tiles first within a
+    // class), xp the per-field form's (grouped by logical field, then class) and xb the per-box
+    // form's (grouped by descriptor); each launch range is padded per class with empty tiles.
+    std::vector<ghexb::xtile> xf, xp, xb;
     std::vector<std::pair<int, int>> xp_field;          // [begin, count) in xp per logical field
-    std::vector<std::pair<int, int>> xp_box, xp_list;   // [begin, count) in xp per descriptor
+    std::vector<std::pair<int, int>> xb_box, xb_list;   // [begin, count) in xb per descriptor
     // Box adjoint in gather form (gather_ok), else by conflict-free phases of the box descriptors.
     bool gather_ok = false;
     std::string gather_reason;
@@ -55,13 +56,14 @@ struct ghexb_plan_s
     int32_t* d_idx = nullptr;
     ghexb::xtile* d_xf = nullptr;
     ghexb::xtile* d_xp = nullptr;
+    ghexb::xtile* d_xb = nullptr;
     ghexb::gtile* d_gt = nullptr;
-    size_t cap_x = 0, cap_gt = 0; // elements allocated behind d_xf / d_xp and d_gt
+    size_t cap_xf = 0, cap_xp = 0, cap_xb = 0, cap_gt = 0; // elements allocated behind the tables
     ghexb::tile* d_adj_btiles = nullptr;
     ghexb::tile* d_adj_ltiles = nullptr;
     unsigned* d_counters = nullptr; // tile scheduler counters of the phased adjoint kernels
 
-    int64_t num_tiles() const { return (int64_t)xf.size(); }
+    int64_t num_tiles() const; // non-empty tiles of the batched table
     int adjoint_launches() const;
 
     // statistics
