@@ -1,22 +1,32 @@
 #!/usr/bin/env python
 """Benchmark of the batched halo exchange on B200.
 
-Workload (N = 1 line): the batched structured exchange of uneven domains — global grid
+Workload of the headline line: the batched structured exchange of uneven domains — global grid
 400x300x96 split 3x3x3 at seeded uneven points into 27 domains, three float64 fields with halo
 (3,3,3,3,0,0) and two float32 fields with halo (2,2,2,2,1,1), x fastest, periodic in y only,
 splitmix64 interiors, NaN halos. One step = one exchange of all five fields of all 27 domains.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config cfg1|cfg0|cfg4]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config cfg1|...]
 
-value      effective GB/s of the batched, graph-captured exchange (algorithmic bytes = halo cells x
-           sizeof(T) x (1 read + 1 write)) summed over all ranks; every timed exchange starts with a
-           cold L2 (a 2 x L2 read of an unrelated buffer runs before it, outside its events)
-e2e        the same metric through the public API with the fields in pinned host memory:
-           host->device copy of every field, co.exchange(...).wait(), device->host copy back
-roofline   achieved GB/s of the exchange kernel (the only kernel of the batched form) against the
-           measured HBM copy bandwidth
-With --gpus N > 1 (torchrun, one process per GPU) every rank runs an independent replica of the
-workload: the path moves no data between GPUs.
+value        effective GB/s of the batched, graph-captured exchange (algorithmic bytes = halo
+             elements x sizeof(T) x (1 read + 1 write)) summed over all ranks; every timed exchange
+             starts with a cold L2 (a read of an unrelated buffer of twice the L2 size runs before
+             it, outside its events)
+e2e          the same metric through the public API (co.exchange(...).wait()) with the fields in
+             pinned host memory: host->device copy of every field, exchange, device->host copy
+roofline     achieved GB/s of the exchange kernel (the only kernel of the batched form) against the
+             measured HBM copy bandwidth; traffic = DRAM bytes per launch from an ncu capture
+cpu_baseline GHEX's own CPU exchange (single rank holding every domain, built from the reference
+             sources against single-process stand-ins), timed on one host core; it also checks the
+             device result bit for bit
+configs      the unstructured, cubed-sphere and differentiable workloads measured the same way
+             (batched and per-field forms, adjoint for the differentiable one)
+
+--impl reference times GHEX's CPU exchange alone on all host cores (one process per core, each
+exchanging its own copy of the workload) and prints the same metric.
+
+With --gpus N > 1 (torchrun, one process per GPU) every rank runs an independent replica: the path
+moves no data between GPUs.
 """
 from __future__ import annotations
 
@@ -44,18 +54,17 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["cfg0", "cfg1", "cfg4"], default="cfg1")
+    ap.add_argument("--config", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4"], default="cfg1")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other workloads")
     ap.add_argument("--baseline-seconds", type=float, default=10.0)
+    ap.add_argument("--calibrate", action="store_true",
+                    help="time torch's own strided copies of the exchange's access patterns (rows of n elements at a "
+                         "row stride) and a contiguous copy, cold L2, and print one JSON line")
     ap.add_argument("--profile", choices=["batched", "per_field", "adjoint"], default=None,
                     help="only run `--steps` launches of one form after `--warmup` (for ncu captures)")
     return ap.parse_args()
-
-
-def workload(cfg: str):
-    from ghex_b200 import workloads as W
-    return {"cfg0": W.config0, "cfg1": W.config1, "cfg4": W.config4}[cfg]()
 
 
 def peaks() -> tuple[float, str]:
@@ -130,79 +139,362 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------------------
-# CPU baseline: the oracle restatement of the reference's exchange, timed on the host
+# workloads on the host (numpy) and on the device (the drop-in API)
 # ------------------------------------------------------------------------------------------
-def _oracle_worker(cfg: str, seconds: float, queue):
+def workload(cfg: str):
+    from ghex_b200 import workloads as W
+    return {"cfg0": W.config0, "cfg1": W.config1, "cfg2": W.config2, "cfg3": W.config3, "cfg4": W.config4}[cfg]()
+
+
+class Case:
+    """One workload: host arrays, their device copies, buffer_infos and an exchange plan.
+    fields: (name, host arrays, device tensors, extra) with extra = (ncomp, is_vector) for the
+    cubed sphere."""
+
+    def __init__(self, cfg: str, dev, device_index: int = 0):
+        import torch
+        self.cfg = cfg
+        self.w = w = workload(cfg)
+        self.kind = {"cfg2": "unstructured", "cfg3": "cubed_sphere"}.get(cfg, "regular")
+        self.fields = []
+        self.bis = []
+        if self.kind == "regular":
+            from ghex_b200.structured import regular as R
+            self.api = R
+            self.ctx = R.make_context(device=device_index)
+            for halos, specs in w.halo_groups().items():
+                hg = R.HaloGenerator(((0,) * w.dim, tuple(n - 1 for n in w.shape)),
+                                     [(halos[2 * k], halos[2 * k + 1]) for k in range(w.dim)], w.periodic)
+                doms = [R.DomainDescriptor(i, (f, l)) for i, f, l in w.domains]
+                pat = R.make_pattern(self.ctx, hg, doms)
+                for s in specs:
+                    host = [w.domain_array(d, s) for d in w.domains]
+                    tens = [torch.from_numpy(a).to(dev) for a in host]
+                    self.fields.append((s.name, host, tens, None))
+                    self.bis += [pat(R.make_field_descriptor(dm, t, w.offsets(s), w.extents(d, s)))
+                                 for dm, d, t in zip(doms, w.domains, tens)]
+            names = sorted({np.dtype(s.dtype).name for s in w.fields}, reverse=True)
+            self.dtype = "+".join(n.replace("float", "f") for n in names)
+        elif self.kind == "cubed_sphere":
+            from ghex_b200.structured import cubed_sphere as C
+            self.api = C
+            self.ctx = C.make_context(device=device_index)
+            cube = C.cube(w.edge, w.levels)
+            doms = [C.DomainDescriptor(cube, *b) for b in w.domains]
+            pat = C.make_pattern(self.ctx, C.HaloGenerator(w.halo), doms)
+            for name, nc, vec, seed in (("scalar", 1, False, 1), ("vector", 2, True, 2)):
+                host = [w.domain_array(d, nc, seed) for d in w.domains]
+                tens = [torch.from_numpy(a).to(dev) for a in host]
+                self.fields.append((name, host, tens, (nc, vec)))
+                self.bis += [pat(C.make_field_descriptor(d, t, w.offsets(), a.shape[:3], nc, vec))
+                             for d, t, a in zip(doms, tens, host)]
+            self.dtype = "f64"
+        else:
+            from ghex_b200 import unstructured as U
+            self.api = U
+            self.ctx = U.make_context(device=device_index)
+            doms = [U.DomainDescriptor(*d) for d in w.domains]
+            pat = U.make_pattern(self.ctx, U.HaloGenerator(), doms)
+            for name, dt, seed in (("f64", np.float64, 1), ("f32", np.float32, 2)):
+                host = [w.domain_array(d, dt, seed) for d in w.domains]
+                tens = [torch.from_numpy(a).to(dev) for a in host]
+                self.fields.append((name, host, tens, None))
+                self.bis += [pat(U.make_field_descriptor(d, t)) for d, t in zip(doms, tens)]
+            self.dtype = "f64+f32"
+        for _, host, tens, _ in self.fields:
+            for a, t in zip(host, tens):
+                assert t.stride() == torch.from_numpy(a).stride()
+        self.plan = self.api.make_exchange_plan(self.ctx, self.bis)
+        self.alg = self.plan.info()["algorithmic_bytes"]
+
+    def reset(self):
+        import torch
+        for _, host, tens, _ in self.fields:
+            for t, a in zip(tens, host):
+                t.copy_(torch.from_numpy(a))
+        torch.cuda.synchronize()
+
+    # ---- the CPU side: GHEX's own exchange where built, else the numpy restatement ---------
+    def reference(self, iterations: int):
+        """Exchanges copies of the host arrays on the CPU; returns (seconds per exchange over
+        `iterations` timed exchanges after one untimed, the exchanged arrays, kind)."""
+        from oracle import reflib
+        w = self.w
+        arrays = [[a.copy(order="K") for a in f[1]] for f in self.fields]
+        if reflib.available():
+            if self.kind == "regular":
+                groups = list(w.halo_groups().items())
+                gi = {h: i for i, (h, _) in enumerate(groups)}
+                spec_of = {s.name: s for s in w.fields}
+                fl = [(gi[spec_of[f[0]].halos], w.offsets(spec_of[f[0]]), arrs) for f, arrs in zip(self.fields, arrays)]
+                sec = reflib.regular_exchange(w.shape, [(h, w.periodic) for h, _ in groups], w.domains, fl, iterations)
+            elif self.kind == "cubed_sphere":
+                fl = [(f[3][0], f[3][1], w.offsets(), arrs) for f, arrs in zip(self.fields, arrays)]
+                sec = reflib.cubed_exchange(w.edge, w.levels, (w.halo,) * 4, w.domains, fl, iterations)
+            else:
+                sec = reflib.unstructured_exchange(w.domains, [(w.levels, True, arrs) for arrs in arrays], iterations)
+            return sec, arrays, "reference"
+        t0 = time.perf_counter()
+        for it in range(iterations + 1):
+            if it == 1:
+                t0 = time.perf_counter()
+            self._port_exchange(arrays)
+        return (time.perf_counter() - t0) / max(1, iterations), arrays, "port"
+
+    def _port_exchange(self, arrays):
+        w = self.w
+        if self.kind == "regular":
+            from oracle import regular as O
+            spec_of = {s.name: s for s in w.fields}
+            for f, arrs in zip(self.fields, arrays):
+                s = spec_of[f[0]]
+                doms = [O.Domain(i, a, b) for i, a, b in w.domains]
+                pat = O.make_pattern((0,) * w.dim, tuple(n - 1 for n in w.shape), s.halos, w.periodic, doms)
+                O.exchange(pat, doms, arrs, [w.offsets(s)] * len(doms))
+        elif self.kind == "cubed_sphere":
+            from oracle import cubed_sphere as O
+            doms = [O.Domain(t, (x0, x1), (y0, y1), w.levels) for t, x0, x1, y0, y1 in w.domains]
+            pat = O.make_pattern(w.edge, (w.halo,) * 4, doms)
+            for f, arrs in zip(self.fields, arrays):
+                O.exchange(pat, doms, arrs, [w.offsets()] * len(doms), w.edge, f[3][1])
+        else:
+            from oracle import unstructured as O
+            doms = [O.Domain(*d) for d in w.domains]
+            recv, send, _ = O.make_pattern(doms)
+            for arrs in arrays:
+                O.exchange(recv, send, arrs)
+
+    def mismatches(self, expected) -> int:
+        bad = 0
+        for f, exp in zip(self.fields, expected):
+            for t, e in zip(f[2], exp):
+                got = t.cpu().numpy()
+                u = np.dtype(f"u{e.itemsize}")
+                bad += int(np.count_nonzero(np.ascontiguousarray(got).view(u) != np.ascontiguousarray(e).view(u)))
+        return bad
+
+
+# ------------------------------------------------------------------------------------------
+# reference arm: GHEX's CPU exchange on all host cores
+# ------------------------------------------------------------------------------------------
+def _reference_worker(cfg: str, iterations: int, queue):
+    try:
+        from oracle import reflib
+        w = workload(cfg)
+        groups = list(w.halo_groups().items())
+        fields = []
+        for gi, (h, specs) in enumerate(groups):
+            for s in specs:
+                fields.append((gi, w.offsets(s), [w.domain_array(d, s) for d in w.domains]))
+        if reflib.available():
+            sec = reflib.regular_exchange(w.shape, [(h, w.periodic) for h, _ in groups], w.domains, fields, iterations)
+            kind = "reference"
+        else:
+            from oracle import regular as O
+            pats = []
+            for h, _ in groups:
+                doms = [O.Domain(i, f, l) for i, f, l in w.domains]
+                pats.append((O.make_pattern((0,) * w.dim, tuple(n - 1 for n in w.shape), h, w.periodic, doms), doms))
+            t0 = time.perf_counter()
+            for it in range(iterations + 1):
+                if it == 1:
+                    t0 = time.perf_counter()
+                for gi, off, arrs in fields:
+                    pat, doms = pats[gi]
+                    O.exchange(pat, doms, arrs, [off] * len(doms))
+            sec = (time.perf_counter() - t0) / max(1, iterations)
+            kind = "port"
+        queue.put((sec, kind))
+    except Exception as e:  # reported by the parent
+        queue.put((None, repr(e)))
+
+
+def alg_bytes_host(cfg: str) -> int:
+    """Algorithmic bytes of a regular workload, from the restated pattern (no device needed)."""
     from oracle import regular as O
     w = workload(cfg)
-    groups = []
-    for halos, specs in w.halo_groups().items():
-        doms = [O.Domain(i, f, l) for i, f, l in w.domains]
-        pat = O.make_pattern((0,) * w.dim, tuple(n - 1 for n in w.shape), halos, w.periodic, doms)
-        groups.append((pat, doms, [([w.domain_array(d, s) for d in w.domains], w.offsets(s)) for s in specs]))
-    n = 0
-    t0 = time.perf_counter()
-    while True:
-        for pat, doms, fields in groups:
-            for arrays, off in fields:
-                O.exchange(pat, doms, arrays, [off] * len(doms))
-        n += 1
-        if time.perf_counter() - t0 >= seconds:
-            break
-    queue.put((n, time.perf_counter() - t0))
-
-
-def cpu_baseline(cfg: str, alg_bytes: int, seconds: float, processes: int = 1) -> dict:
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    q = ctx.Queue()
-    procs = [ctx.Process(target=_oracle_worker, args=(cfg, seconds, q)) for _ in range(processes)]
-    for p in procs:
-        p.start()
-    res = [q.get() for _ in procs]
-    for p in procs:
-        p.join()
-    rate = sum(n / t for n, t in res)  # exchanges per second, all processes
-    return {"value": rate * alg_bytes / 1e9, "unit": "GB/s", "cores": processes, "kind": "port",
-            "sample": f"{sum(n for n, _ in res)} exchanges of {cfg} by the numpy oracle "
-                      f"({processes} process(es), {seconds:.0f} s each)",
-            "exchanges_per_s": rate}
-
-
-# ------------------------------------------------------------------------------------------
-# reference arm
-# ------------------------------------------------------------------------------------------
-def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
-    w = workload(args.config)
-    from oracle import regular as O
     alg = 0
     for halos, specs in w.halo_groups().items():
         doms = [O.Domain(i, f, l) for i, f, l in w.domains]
         pat = O.make_pattern((0,) * w.dim, tuple(n - 1 for n in w.shape), halos, w.periodic, doms)
         for s in specs:
             alg += O.halo_cells(pat) * np.dtype(s.dtype).itemsize * 2
-    procs = min(os.cpu_count() or 1, 16)
-    per_step = max(1.0, 30.0 / max(1, args.steps + args.warmup))
-    b = cpu_baseline(args.config, alg, seconds=per_step * args.steps, processes=procs)
-    line = {"impl": "reference", "metric": METRIC, "value": b["value"], "unit": "GB/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / b["exchanges_per_s"] * procs,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
-            "data": "synthetic (seeded splitmix64)", "config": {"workload": w.name},
-            "cpu_baseline": {k: b[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": b["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return alg
+
+
+def run_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    import multiprocessing as mp
+    cfg = args.config if args.config in ("cfg0", "cfg1", "cfg4") else "cfg1"
+    procs = max(1, min(os.cpu_count() or 1, 32))
+    # every process exchanges its own copy; bounded to about a minute in all
+    iters = max(2, min(200, (args.steps + procs - 1) // procs))
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_reference_worker, args=(cfg, iters, q)) for _ in range(procs)]
+    for p in ps:
+        p.start()
+    res = [q.get() for _ in ps]
+    for p in ps:
+        p.join()
+    good = [r for r in res if r[0]]
+    if not good:
+        print(json.dumps({"impl": "reference", "unavailable": f"the CPU exchange failed: {res[0][1]}"}), flush=True)
+        return
+    alg = alg_bytes_host(cfg)
+    rate = sum(1.0 / s for s, _ in good)  # exchanges per second, all processes
+    value = rate * alg / 1e9
+    kind = good[0][1]
+    sample = (f"{len(good)} processes x {iters} timed exchanges (after 1 untimed) of {cfg}, each process on its "
+              f"own copy of the workload; GHEX's CPU exchange "
+              + ("built from the reference sources" if kind == "reference" else "restated in numpy"))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / rate, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic (seeded splitmix64)",
+            "config": {"workload": workload(cfg).name, "processes": len(good)},
+            "exchanges_per_s": rate,
+            "cpu_baseline": {"value": value, "unit": "GB/s", "cores": len(good), "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------------------------------------
 # our arm
 # ------------------------------------------------------------------------------------------
+class Timer:
+    """Device time of `launch` per step with CUDA events on `stream`, max over ranks; every timed
+    step starts with a cold L2 (a read of `flush`, outside the events)."""
+
+    def __init__(self, stream, flush, world, dev):
+        self.stream, self.flush, self.world, self.dev = stream, flush, world, dev
+
+    def __call__(self, launch, steps, warmup):
+        import torch
+        import torch.distributed as dist
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        with torch.cuda.stream(self.stream):
+            for _ in range(warmup):
+                launch()
+            self.stream.synchronize()
+            if self.world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            for k in range(steps):
+                if self.flush is not None:
+                    self.flush.sum()
+                ev[k][0].record(self.stream)
+                launch()
+                ev[k][1].record(self.stream)
+            torch.cuda.synchronize()
+            if self.world > 1:
+                dist.barrier()
+        ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+        if self.world > 1:
+            t = torch.tensor([ms], device=self.dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+
+def e2e_ms(case, stream, steps, world, dev):
+    """Public API end to end: pinned host fields -> device, co.exchange(...).wait(), device -> host."""
+    import torch
+    import torch.distributed as dist
+    co = case.api.make_communication_object(case.ctx)
+    pinned = [[torch.from_numpy(a).pin_memory() for a in f[1]] for f in case.fields]
+    outs = [[torch.empty_like(p).pin_memory() for p in ps] for ps in pinned]
+    h2d = sum(p.numel() * p.element_size() for ps in pinned for p in ps)
+    with torch.cuda.stream(stream):
+        for it in range(steps + 2):
+            if it == 2:
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            for f, ps in zip(case.fields, pinned):
+                for t, p in zip(f[2], ps):
+                    t.copy_(p, non_blocking=True)
+            co.exchange(case.bis).wait()
+            for f, os_ in zip(case.fields, outs):
+                for t, o in zip(f[2], os_):
+                    o.copy_(t, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, h2d
+
+
+def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline=True) -> dict:
+    """Batched and per-field exchange of one workload (plus the adjoint of the differentiable one)."""
+    case = Case(cfg, dev, dev.index)
+    plan = case.plan
+    tuning = plan.autotune(repeats=3) if autotune else plan.info()
+    s = timer.stream.cuda_stream
+    ms_b = timer(lambda: plan.graph_launch(s), steps, warmup)
+    ms_f = timer(lambda: plan.launch(plan.PER_FIELD, s), max(10, steps // 2), warmup)
+    out = {"workload": case.w.name, "algorithmic_bytes": case.alg, "dtype": case.dtype,
+           "batched": {"ms": ms_b, "GB/s": case.alg / ms_b / 1e6, "exchanges_per_s": 1e3 / ms_b,
+                       "roofline_frac": case.alg / ms_b / 1e6 / peak},
+           "per_field": {"ms": ms_f, "GB/s": case.alg / ms_f / 1e6, "exchanges_per_s": 1e3 / ms_f},
+           "batched_vs_per_field": ms_f / ms_b,
+           "tuning": {k: tuning[k] for k in ("elems_per_thread", "block", "grid")}}
+    if cfg == "cfg4":
+        ms_a = timer(lambda: plan.adjoint(s), steps, warmup)
+        out["adjoint"] = {"ms": ms_a, "vs_forward": ms_a / ms_b, "launches": plan.info()["adjoint_launches"]}
+    if baseline:
+        case.reset()
+        plan.launch(plan.BATCHED, s)
+        sec, expected, kind = case.reference(1 if cfg in ("cfg2", "cfg3") else 3)
+        out["bitexact"] = case.mismatches(expected) == 0
+        out["cpu_baseline"] = {"value": case.alg / sec / 1e9, "unit": "GB/s", "cores": 1, "kind": kind, "ms": sec * 1e3}
+    return out
+
+
+def calibrate(args):
+    """The access-pattern roofline: how fast a library copy kernel (torch's strided copy_) moves
+    rows of n float64 elements spaced one x-row of a halo field apart (stride 139 elements, as in
+    the x faces of the 400x300x96 workload), against a contiguous copy of the same bytes. Every
+    timed copy starts with a cold L2."""
+    import torch
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    l2 = torch.cuda.get_device_properties(dev).L2_cache_size
+    flush = torch.ones(max(2 * l2, 64 << 20) // 4, dtype=torch.float32, device=dev)
+    timer = Timer(stream, flush, 1, dev)
+    warm = Timer(stream, None, 1, dev)
+    out = {"calibration": "torch copy_ of views, CUDA events; cold: after an L2 flush, warm: the rows' lines "
+                          "resident in L2 from the previous copy", "rows": {}}
+    a = torch.zeros(96, 3000, 139, dtype=torch.float64, device=dev)
+    b = torch.zeros_like(a)
+    for n in (1, 3, 8, 32, 128):
+        src, dst = a[:, :, 3:3 + n], b[:, :, 0:n]
+        rows = src.shape[0] * src.shape[1]
+        ms = timer(lambda: dst.copy_(src), 20, 3)
+        out["rows"][f"n={n}"] = {"rows": rows, "us": ms * 1e3, "rows_per_ns": rows / (ms * 1e6),
+                                 "useful_GB/s": 2 * rows * n * 8 / (ms * 1e-3) / 1e9}
+        if n <= 8:
+            ms = warm(lambda: dst.copy_(src), 20, 3)
+            out["rows"][f"n={n}"]["warm_rows_per_ns"] = rows / (ms * 1e6)
+    for mb in (8, 35, 70):
+        x = torch.ones(mb * (1 << 20) // 8, dtype=torch.float64, device=dev)
+        y = torch.empty_like(x)
+        ms = timer(lambda: y.copy_(x), 20, 3)
+        out[f"contiguous_{mb}MB"] = {"us": ms * 1e3, "GB/s (read+write)": 2 * x.numel() * 8 / (ms * 1e-3) / 1e9}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.calibrate:
+        calibrate(args)
         return
     import torch
     import torch.distributed as dist
@@ -216,141 +508,85 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
-    from ghex_b200.structured import regular as R
-    sys.path.insert(0, str(ROOT / "tests"))
-
-    w = workload(args.config)
-    ctx = R.make_context(device=local)
-    host, tens, bis = {}, {}, []
-    for halos, specs in w.halo_groups().items():
-        hg = R.HaloGenerator(((0,) * w.dim, tuple(n - 1 for n in w.shape)),
-                             [(halos[2 * k], halos[2 * k + 1]) for k in range(w.dim)], w.periodic)
-        doms = [R.DomainDescriptor(i, (f, l)) for i, f, l in w.domains]
-        pat = R.make_pattern(ctx, hg, doms)
-        for s in specs:
-            host[s.name] = [w.domain_array(d, s) for d in w.domains]
-            tens[s.name] = [torch.from_numpy(a).to(dev) for a in host[s.name]]
-            bis += [pat(R.make_field_descriptor(dm, t, w.offsets(s), w.extents(d, s)))
-                    for dm, d, t in zip(doms, w.domains, tens[s.name])]
-    plan = R.make_exchange_plan(ctx, bis)
+    case = Case(args.config, dev, local)
+    plan = case.plan
     if args.profile:
         launch = {"batched": lambda: plan.launch(plan.BATCHED), "per_field": lambda: plan.launch(plan.PER_FIELD),
                   "adjoint": lambda: plan.adjoint()}[args.profile]
         for _ in range(args.warmup + args.steps):
             launch()
         torch.cuda.synchronize()
-        print(json.dumps({"profile": args.profile, "config": w.name, "launches": args.warmup + args.steps,
+        print(json.dumps({"profile": args.profile, "config": case.w.name, "launches": args.warmup + args.steps,
                           "plan": plan.info()}), flush=True)
         return
     tuning = plan.info() if args.no_autotune else plan.autotune(repeats=5)
     info = plan.info()
-    alg = info["algorithmic_bytes"]
+    alg = case.alg
     stream = torch.cuda.Stream(device=dev)
     l2 = torch.cuda.get_device_properties(dev).L2_cache_size
     flush = torch.ones(max(2 * l2, 64 << 20) // 4, dtype=torch.float32, device=dev)
-
-    def timed(launch, steps, kernels_per_step):
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-        with torch.cuda.stream(stream):
-            for _ in range(args.warmup):
-                launch()
-            stream.synchronize()
-            if world > 1:
-                dist.barrier()
-            torch.cuda.synchronize()
-            for k in range(steps):
-                flush.sum()
-                ev[k][0].record(stream)
-                launch()
-                ev[k][1].record(stream)
-            torch.cuda.synchronize()
-            if world > 1:
-                dist.barrier()
-        ms = sum(a.elapsed_time(b) for a, b in ev)
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms / steps, steps * kernels_per_step
+    timer = Timer(stream, flush, world, dev)
+    peak, peak_kind = peaks()
+    s = stream.cuda_stream
 
     sampler = ClockSampler(dev.index)
     with sampler:
-        ms_batched, launches = timed(lambda: plan.graph_launch(stream.cuda_stream), args.steps, 1)
+        ms_batched = timer(lambda: plan.graph_launch(s), args.steps, max(3, args.warmup))
     clocks = sampler.summary()
+    launches = args.steps  # one kernel per graph launch
     k_small = max(10, min(args.steps, 200))
-    ms_field, _ = timed(lambda: plan.launch(plan.PER_FIELD, stream.cuda_stream), k_small, 0)
-    ms_box, _ = timed(lambda: plan.launch(plan.PER_BOX, stream.cuda_stream), max(5, k_small // 4), 0)
+    ms_field = timer(lambda: plan.launch(plan.PER_FIELD, s), k_small, max(3, args.warmup))
+    ms_box = timer(lambda: plan.launch(plan.PER_BOX, s), max(5, k_small // 4), 3)
+    e2e, h2d = e2e_ms(case, stream, max(3, min(args.steps, 20)), world, dev)
 
-    # bit-exact check of the exchanged halos against the oracle on this rank's data
-    import oracle.regular as O
-    bad = 0
-    for halos, specs in w.halo_groups().items():
-        doms = [O.Domain(i, f, l) for i, f, l in w.domains]
-        pat = O.make_pattern((0,) * w.dim, tuple(n - 1 for n in w.shape), halos, w.periodic, doms)
-        for s in specs:
-            exp = [a.copy(order="K") for a in host[s.name]]
-            O.exchange(pat, doms, exp, [w.offsets(s)] * len(doms))
-            for t, e in zip(tens[s.name], exp):
-                got = t.cpu().numpy()
-                u = np.dtype(f"u{e.itemsize}")
-                bad += int(np.count_nonzero(np.ascontiguousarray(got).view(u) != np.ascontiguousarray(e).view(u)))
-
-    # end to end through the public API with host buffers
-    co = R.make_communication_object(ctx)
-    pinned = {k: [torch.from_numpy(a).pin_memory() for a in v] for k, v in host.items()}
-    outs = {k: [torch.empty_like(p).pin_memory() for p in v] for k, v in pinned.items()}
-    h2d = sum(p.numel() * p.element_size() for v in pinned.values() for p in v)
-    e2e_steps = max(3, min(args.steps, 20))
-    with torch.cuda.stream(stream):
-        for it in range(e2e_steps + 2):
-            if it == 2:
-                torch.cuda.synchronize()
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-            for k in tens:
-                for t, p in zip(tens[k], pinned[k]):
-                    t.copy_(p, non_blocking=True)
-            co.exchange(bis).wait()
-            for k in tens:
-                for t, o in zip(tens[k], outs[k]):
-                    o.copy_(t, non_blocking=True)
-        e1.record(stream)
-        torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-
-    peak, peak_kind = peaks()
     achieved = alg / (ms_batched * 1e-3) / 1e9
-    value = world * alg / (ms_batched * 1e-3) / 1e9
+    traffic = ncu_traffic(args.config)
+    n_logical = len({f[0] for f in case.fields})
     line = {
-        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": world * achieved, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_batched, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic (seeded splitmix64 interiors, NaN halos)",
-        "config": {"workload": w.name, "form": "batched persistent kernel, CUDA graph", "domains": len(w.domains),
-                   "fields": len(w.fields), "algorithmic_bytes_per_exchange": alg,
-                   "l2": "cold: a 2 x L2 read of an unrelated buffer before every timed exchange, outside its events",
-                   "parallelism": f"replicas x{world}", "tuning": {k: tuning[k] for k in ("elems_per_thread", "block", "grid")}},
+        "vs_baseline": None, "dtype": case.dtype, "data": "synthetic (seeded splitmix64 interiors, NaN halos)",
+        "config": {"workload": case.w.name, "form": "batched kernel, CUDA graph", "domains": len(case.w.domains),
+                   "algorithmic_bytes_per_exchange": alg,
+                   "l2": "cold: a read of an unrelated buffer of twice the L2 size before every timed exchange, "
+                         "outside its events",
+                   "parallelism": f"replicas x{world}",
+                   "tuning": {k: tuning[k] for k in ("elems_per_thread", "block", "grid")}},
         "exchanges_per_s": world * 1e3 / ms_batched,
         "per_field": {"ms_per_step": ms_field, "GB/s": world * alg / (ms_field * 1e-3) / 1e9,
-                      "exchanges_per_s": world * 1e3 / ms_field, "launches_per_exchange": len(w.fields)},
+                      "exchanges_per_s": world * 1e3 / ms_field, "launches_per_exchange": n_logical},
         "per_box": {"ms_per_step": ms_box, "GB/s": world * alg / (ms_box * 1e-3) / 1e9,
                     "exchanges_per_s": world * 1e3 / ms_box, "launches_per_exchange": info["num_descriptors"]},
         "batched_vs_per_field": ms_field / ms_batched,
-        "bitexact": bad == 0, "mismatched_elements": bad,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_kind, "traffic": ncu_traffic(args.config)},
-        "e2e": {"value": world * alg / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": h2d, "ms_per_step": e2e_ms},
+                     "peak_source": peak_kind, "traffic": traffic},
+        "e2e": {"value": world * alg / (e2e * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": h2d, "ms_per_step": e2e},
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if traffic:
+        line["roofline"]["dram_frac"] = traffic / (ms_batched * 1e-3) / 1e9 / peak
     if rank == 0 and world == 1 and not args.no_baseline:
-        line["cpu_baseline"] = cpu_baseline(args.config, alg, args.baseline_seconds, 1)
-        line["cpu_baseline"].pop("exchanges_per_s", None)
+        case.reset()
+        plan.launch(plan.BATCHED, s)
+        torch.cuda.synchronize()
+        est, _, _ = case.reference(1)
+        iters = max(1, int(args.baseline_seconds / max(est, 1e-6)))
+        sec, expected, kind = case.reference(iters)
+        line["bitexact"] = case.mismatches(expected) == 0
+        line["cpu_baseline"] = {
+            "value": alg / sec / 1e9, "unit": "GB/s", "cores": 1, "kind": kind,
+            "sample": f"{iters} timed exchanges (after 1 untimed) of the full workload by GHEX's CPU exchange "
+                      + ("built from the reference sources" if kind == "reference" else "restated in numpy")
+                      + ", one process, one core"}
+    if rank == 0 and world == 1 and not args.no_configs:
+        del case
+        line["configs"] = {}
+        for cfg in ("cfg2", "cfg3", "cfg4"):
+            if cfg != args.config:
+                line["configs"][cfg] = measure_config(cfg, dev, timer, peak, min(args.steps, 200), max(3, args.warmup),
+                                                      not args.no_autotune, not args.no_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
