@@ -362,6 +362,17 @@ def run_reference(args):
 # ------------------------------------------------------------------------------------------
 # our arm
 # ------------------------------------------------------------------------------------------
+def max_over_ranks(value: float, world: int, device) -> float:
+    """The largest value over all ranks (every rank calls it at the same point)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 class Timer:
     """Device time of `launch` per step with CUDA events on `stream`, max over ranks; every timed
     step starts with a cold L2 (a read of `flush`, outside the events)."""
@@ -389,18 +400,12 @@ class Timer:
             torch.cuda.synchronize()
             if self.world > 1:
                 dist.barrier()
-        ms = sum(a.elapsed_time(b) for a, b in ev) / steps
-        if self.world > 1:
-            t = torch.tensor([ms], device=self.dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / steps, self.world, self.dev)
 
 
 def e2e_ms(case, stream, steps, world, dev):
     """Public API end to end: pinned host fields -> device, co.exchange(...).wait(), device -> host."""
     import torch
-    import torch.distributed as dist
     co = case.api.make_communication_object(case.ctx)
     pinned = [[torch.from_numpy(a).pin_memory() for a in f[1]] for f in case.fields]
     outs = [[torch.empty_like(p).pin_memory() for p in ps] for ps in pinned]
@@ -421,12 +426,7 @@ def e2e_ms(case, stream, steps, world, dev):
                     o.copy_(t, non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    return ms, h2d
+    return max_over_ranks(e0.elapsed_time(e1) / steps, world, dev), h2d
 
 
 def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline=True) -> dict:

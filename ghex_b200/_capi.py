@@ -17,6 +17,21 @@ if not LIB_PATH.exists():
 
 lib = C.CDLL(str(LIB_PATH))
 
+
+def _make_release(library):
+    def release(name: str, handle) -> None:
+        """Destroys a handle with ghexb_<...>_destroy; the library is held by this closure, so the
+        call also works while the interpreter tears modules down."""
+        if handle:
+            try:
+                getattr(library, name)(handle)
+            except Exception:
+                pass
+    return release
+
+
+release = _make_release(lib)
+
 OK = 0
 ERR_INVALID = 1
 ERR_CUDA = 2

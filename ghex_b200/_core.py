@@ -114,11 +114,9 @@ class context:
     def size(self) -> int:
         return 1
 
-    def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            _capi.lib.ghexb_context_destroy(h)
-            self._h = None
+    def __del__(self, _release=_capi.release):
+        _release("ghexb_context_destroy", getattr(self, "_h", None))
+        self._h = None
 
 
 def make_context(comm: Any = None, thread_safe: bool = False, device: int | None = None) -> context:
@@ -204,11 +202,9 @@ class PatternContainer:
             out.append((nb.value, list(buf)[: cnt.value]))
         return out
 
-    def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            _capi.lib.ghexb_pattern_destroy(h)
-            self._h = None
+    def __del__(self, _release=_capi.release):
+        _release("ghexb_pattern_destroy", getattr(self, "_h", None))
+        self._h = None
 
 
 class FieldDescriptorBase:
@@ -233,9 +229,9 @@ class FieldDescriptorBase:
             self._patterns = getattr(self, "_patterns", []) + [pattern]  # keep patterns alive
         return h
 
-    def __del__(self):
+    def __del__(self, _release=_capi.release):
         for h in getattr(self, "_handles", {}).values():
-            _capi.lib.ghexb_field_destroy(h)
+            _release("ghexb_field_destroy", h)
         self._handles = {}
 
 
@@ -279,11 +275,9 @@ class Handle:
     def progress(self) -> None:
         self.is_ready()
 
-    def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            _capi.lib.ghexb_handle_destroy(h)
-            self._h = None
+    def __del__(self, _release=_capi.release):
+        _release("ghexb_handle_destroy", getattr(self, "_h", None))
+        self._h = None
 
 
 class CommunicationObject:
@@ -309,11 +303,9 @@ class CommunicationObject:
         call("ghexb_co_exchange", self._h, handles, len(bis), stream_of(arrays), C.byref(h))
         return Handle(self, h, [bis, arrays])
 
-    def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            _capi.lib.ghexb_co_destroy(h)
-            self._h = None
+    def __del__(self, _release=_capi.release):
+        _release("ghexb_co_destroy", getattr(self, "_h", None))
+        self._h = None
 
 
 def make_communication_object(ctx: context) -> CommunicationObject:
@@ -396,11 +388,9 @@ class ExchangePlan:
         call("ghexb_plan_autotune", self._h, self._stream(stream), repeats, C.byref(i))
         return i.as_dict()
 
-    def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            _capi.lib.ghexb_plan_destroy(h)
-            self._h = None
+    def __del__(self, _release=_capi.release):
+        _release("ghexb_plan_destroy", getattr(self, "_h", None))
+        self._h = None
 
 
 def make_exchange_plan(ctx: context, buffer_infos: Sequence[BufferInfo]) -> ExchangePlan:
