@@ -433,7 +433,7 @@ def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline
     """Batched and per-field exchange of one workload (plus the adjoint of the differentiable one)."""
     case = Case(cfg, dev, dev.index)
     plan = case.plan
-    tuning = plan.autotune(repeats=3) if autotune else plan.info()
+    tuning = plan.autotune(repeats=5) if autotune else plan.info()
     s = timer.stream.cuda_stream
     ms_b = timer(lambda: plan.graph_launch(s), steps, warmup)
     ms_f = timer(lambda: plan.launch(plan.PER_FIELD, s), max(10, steps // 2), warmup)
@@ -442,7 +442,7 @@ def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline
                        "roofline_frac": case.alg / ms_b / 1e6 / peak},
            "per_field": {"ms": ms_f, "GB/s": case.alg / ms_f / 1e6, "exchanges_per_s": 1e3 / ms_f},
            "batched_vs_per_field": ms_f / ms_b,
-           "tuning": {k: tuning[k] for k in ("elems_per_thread", "block", "grid")}}
+           "tuning": {k: tuning[k] for k in ("elems_per_thread", "block", "grid", "pairs", "use_pairs")}}
     if cfg == "cfg4":
         ms_a = timer(lambda: plan.adjoint(s), steps, warmup)
         out["adjoint"] = {"ms": ms_a, "vs_forward": ms_a / ms_b, "launches": plan.info()["adjoint_launches"]}
@@ -551,7 +551,7 @@ def main():
                    "l2": "cold: a read of an unrelated buffer of twice the L2 size before every timed exchange, "
                          "outside its events",
                    "parallelism": f"replicas x{world}",
-                   "tuning": {k: tuning[k] for k in ("elems_per_thread", "block", "grid")}},
+                   "tuning": {k: tuning[k] for k in ("elems_per_thread", "block", "grid", "pairs", "use_pairs")}},
         "exchanges_per_s": world * 1e3 / ms_batched,
         "per_field": {"ms_per_step": ms_field, "GB/s": world * alg / (ms_field * 1e-3) / 1e9,
                       "exchanges_per_s": world * 1e3 / ms_field, "launches_per_exchange": n_logical},

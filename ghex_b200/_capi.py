@@ -64,6 +64,8 @@ class PlanInfo(C.Structure):
         ("elems_per_thread", C.c_int32),
         ("block", C.c_int32),
         ("grid", C.c_int32),
+        ("pairs", C.c_int32),
+        ("use_pairs", C.c_int32),
         ("reserved", C.c_int32),
     ]
 
@@ -101,7 +103,7 @@ SIGNATURES = {
     "ghexb_plan_destroy": [_vp],
     "ghexb_plan_check": [_vp, C.POINTER(_vp), _i, _pi64],
     "ghexb_plan_get_info": [_vp, C.POINTER(PlanInfo)],
-    "ghexb_plan_set_tuning": [_vp, _i, _i],
+    "ghexb_plan_set_tuning": [_vp, _i, _i, _i],
     "ghexb_plan_launch": [_vp, _i, _vp],
     "ghexb_plan_graph_launch": [_vp, _vp],
     "ghexb_plan_adjoint_launch": [_vp, _vp],

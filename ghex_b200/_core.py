@@ -339,9 +339,10 @@ class ExchangePlan:
         call("ghexb_plan_get_info", self._h, C.byref(i))
         return i.as_dict()
 
-    def set_tuning(self, elems_per_thread: int = 0, block: int = 0) -> None:
-        """Elements per thread (4, 8 or 16) and threads per CTA of the forward kernel; 0 keeps."""
-        call("ghexb_plan_set_tuning", self._h, elems_per_thread, block)
+    def set_tuning(self, elems_per_thread: int = 0, block: int = 0, use_pairs: int = -1) -> None:
+        """Elements per thread (4, 8 or 16) and threads per CTA of the forward kernel (0 keeps), and
+        whether x-face pairs move as contiguous segments (1), as separate boxes (0) or as before (-1)."""
+        call("ghexb_plan_set_tuning", self._h, elems_per_thread, block, use_pairs)
 
     def _stream(self, stream):
         if stream is None:

@@ -524,11 +524,13 @@ int ghexb_plan_get_info(ghexb_plan plan, ghexb_plan_info_t* info)
         info->elems_per_thread = plan->per_thread;
         info->block = plan->block;
         info->grid = (int32_t)(plan->xf.size() / ghexb::k_unit_tiles);
+        info->pairs = (int32_t)plan->pairs.size();
+        info->use_pairs = plan->use_pairs ? 1 : 0;
         info->reserved = 0;
     });
 }
 
-int ghexb_plan_set_tuning(ghexb_plan plan, int elems_per_thread, int block)
+int ghexb_plan_set_tuning(ghexb_plan plan, int elems_per_thread, int block, int use_pairs)
 {
     return guarded([&] {
         require(plan != nullptr, "null plan");
@@ -543,6 +545,7 @@ int ghexb_plan_set_tuning(ghexb_plan plan, int elems_per_thread, int block)
             require(block % 32 == 0 && block <= ghexb::k_max_block, "block must be a multiple of 32 and at most 512");
             plan->block = block;
         }
+        if (use_pairs >= 0) plan->use_pairs = use_pairs != 0;
         ghexb::retile(*plan);
         ghexb::check_cuda(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
     });

@@ -106,13 +106,21 @@ struct alignas(16) list_desc
     row_map map;
 };
 
-// A forward work item: the elements [e0, e0 + count) of one box or list descriptor, with all
-// the kernel needs to address them, so that a CTA reads one 96-byte record and nothing else
-// before its data loads.
+// A forward work item: the elements [e0, e0 + count) of one box or list descriptor, or of a
+// pair of x-face boxes, with all the kernel needs to address them, so that a CTA reads one
+// 112-byte record and nothing else before its data loads.
 //  * box:  element e -> i0 = e mod n0, r = e / n0, i1 = r mod n1, i2 = r / n1;
 //          dst[i0*d0 + i1*d1 + i2*d2] = src[i0*s0 + i1*s1 + i2*s2]  (sign bit flipped if neg)
 //  * list: element e -> k = e / n0 (column), l = e mod n0 (level);
 //          dst[didx[k]*d0 + l*d1] = src[sidx[k]*s0 + l*s1]
+//  * pair: two boxes A and B of short rows in one destination field whose rows interleave in
+//          memory: row r of A ends where row r + 1 of B begins (the high-x halo of a row and the
+//          low-x halo of the next). Element e -> segment q = e / n0 (n0 = na + nb elements),
+//          c = e mod n0, plane i2 = q / n1, s = q mod n1 (n1 = rows + 1); the segment is
+//          contiguous in the destination: dst[c + (s - 1)*d1 + i2*d2]. Its first na elements
+//          come from A row s - 1 (s >= 1): src[c*s0 + (s-1)*s1 + i2*s2], the others from B row
+//          s (s < rows): src2[(c-na)*u0 + s*u1 + i2*u2]. Writing both halos of a row boundary
+//          in one coalesced store turns partial-sector writes into whole-sector ones.
 // Offsets are in units of `unit` bytes (the element size; 16 for aligned list columns).
 struct alignas(16) xtile
 {
@@ -120,19 +128,24 @@ struct alignas(16) xtile
     char* dst;
     const int32_t* sidx;
     const int32_t* didx;
+    const char* src2; // pair: source of box B
     uint32_t e0, count;
     int32_t s0, s1, s2;
     int32_t d0, d1, d2;
-    uint32_t n0, m0;  // first extent and its fast-division magic
-    uint32_t n1, m1;  // second extent (boxes)
-    uint8_t l0, l1;   // fast-division shifts
-    uint8_t unit;     // bytes per element: 1, 2, 4, 8 or 16
-    uint8_t kind;     // 0 box, 1 list
-    uint8_t neg;      // 1: flip the sign bit (negated cubed-sphere vector components)
-    uint8_t cls;      // element class (exchange.hpp): kind, unit and neg in one value
-    uint8_t pad[10];
+    int32_t u0, u1, u2; // pair: source strides of box B
+    uint32_t n0, m0;    // first extent and its fast-division magic
+    uint32_t n1, m1;    // second extent (boxes, pairs)
+    uint32_t na;        // pair: row length of box A
+    uint8_t l0, l1;     // fast-division shifts
+    uint8_t unit;       // bytes per element: 1, 2, 4, 8 or 16
+    uint8_t kind;       // 0 box, 1 list, 2 pair
+    uint8_t neg;        // 1: flip the sign bit (negated cubed-sphere vector components); pair: of A
+    uint8_t neg2;       // pair: of B
+    uint8_t cls;        // element class (exchange.hpp): kind, unit and neg in one value
+    uint8_t pad[1];
 };
-static_assert(sizeof(xtile) == 96, "xtile is six 16-byte words");
+static_assert(sizeof(xtile) == 112, "xtile is seven 16-byte words");
+constexpr int k_xtile_words = 7;
 
 // Adjoint of the boxes in gather form. The owner elements read by the forward boxes of one
 // source field are cut into disjoint cells (boxes in the owner's coordinates); every element of

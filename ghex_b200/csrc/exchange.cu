@@ -150,15 +150,55 @@ __device__ __forceinline__ void list_elements(const xtile& t)
         if (k * blockDim.x + threadIdx.x < t.count) dst[doff[k]] = v[k];
 }
 
+// Pairs of x-face boxes: a segment of na + nb destination elements is contiguous, so the warp's
+// stores to it coalesce into whole sectors.
+template<int K, typename T>
+__device__ __forceinline__ void pair_elements(const xtile& t)
+{
+    T* __restrict__ dst = reinterpret_cast<T*>(t.dst);
+    T v[K];
+    int32_t doff[K];
+    bool ok[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+    {
+        const uint32_t e = k * blockDim.x + threadIdx.x;
+        ok[k] = false;
+        doff[k] = 0;
+        if (e < t.count)
+        {
+            const uint32_t g = t.e0 + e;
+            const uint32_t q = fdiv(g, t.m0, t.l0);
+            const int32_t c = (int32_t)(g - q * t.n0);
+            const uint32_t i2 = fdiv(q, t.m1, t.l1);
+            const int32_t s = (int32_t)(q - i2 * t.n1);
+            const bool a = c < (int32_t)t.na;
+            if (a ? s >= 1 : s + 1 < (int32_t)t.n1)
+            {
+                const T* src = reinterpret_cast<const T*>(a ? t.src : t.src2);
+                const int32_t so = a ? c * t.s0 + (s - 1) * t.s1 + (int32_t)i2 * t.s2
+                                     : (c - (int32_t)t.na) * t.u0 + s * t.u1 + (int32_t)i2 * t.u2;
+                v[k] = ld_stream(src + so);
+                if (a ? t.neg : t.neg2) v[k] ^= sign_bit<T>::v;
+                doff[k] = c + (s - 1) * t.d1 + (int32_t)i2 * t.d2;
+                ok[k] = true;
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if (ok[k]) dst[doff[k]] = v[k];
+}
+
 template<int K>
 __global__ void __launch_bounds__(k_max_block, K >= 16 ? 1 : 2) exchange_kernel(const xtile* __restrict__ tiles)
 {
     __shared__ xtile t;
-    const xtile* unit = first_record<6>(t, tiles);
+    const xtile* unit = first_record<k_xtile_words>(t, tiles);
     switch (t.cls)
     {
 #define GHEXB_CASE(C, F)                                                                                               \
-    case C: unit_loop<6>(t, unit, [](const xtile& x) { F(x); }); break;
+    case C: unit_loop<k_xtile_words>(t, unit, [](const xtile& x) { F(x); }); break;
         GHEXB_CASE(k_box8, (box_elements<K, unsigned long long, false>))
         GHEXB_CASE(k_box8_neg, (box_elements<K, unsigned long long, true>))
         GHEXB_CASE(k_box4, (box_elements<K, uint32_t, false>))
@@ -170,6 +210,8 @@ __global__ void __launch_bounds__(k_max_block, K >= 16 ? 1 : 2) exchange_kernel(
         GHEXB_CASE(k_list4, (list_elements<K, uint32_t>))
         GHEXB_CASE(k_list2, (list_elements<K, uint16_t>))
         GHEXB_CASE(k_list1, (list_elements<K, uint8_t>))
+        GHEXB_CASE(k_pair8, (pair_elements<K, unsigned long long>))
+        GHEXB_CASE(k_pair4, (pair_elements<K, uint32_t>))
 #undef GHEXB_CASE
         default: break;
     }

@@ -39,11 +39,14 @@ enum forward_class : int32_t
     k_list4,
     k_list2,
     k_list1,
+    k_pair8,
+    k_pair4,
     k_forward_classes
 };
 __host__ __device__ constexpr int forward_class_of(int kind, int unit, bool neg)
 {
-    return kind == 0 ? (unit == 8 ? (neg ? k_box8_neg : k_box8)
+    return kind == 2 ? (unit == 8 ? k_pair8 : k_pair4)
+         : kind == 0 ? (unit == 8 ? (neg ? k_box8_neg : k_box8)
                            : unit == 4 ? (neg ? k_box4_neg : k_box4)
                            : unit == 2 ? k_box2
                                        : k_box1)

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <unordered_map>
 
 #include "exchange.hpp"
@@ -538,6 +539,36 @@ bool build_cells(ghexb_plan_s& plan, std::string& why)
     return true;
 }
 
+// Pairs of x-face boxes in one destination field whose rows interleave in memory: rows of at most
+// 64 bytes along the destination's contiguous axis, the same rows and planes, and B's row r + 1
+// starting where A's row r ends. Each box joins at most one pair.
+void find_pairs(ghexb_plan_s& plan)
+{
+    plan.pairs.clear();
+    plan.box_pair.assign(plan.boxes.size(), -1);
+    std::map<std::pair<int, int64_t>, int> by_dst; // (destination slot, byte offset) -> box
+    auto short_row = [&](const box_desc& b) {
+        return (b.esize == 8 || b.esize == 4) && b.d0 == 1 && (int64_t)b.n0 * b.esize <= 64 && b.n1 >= 2;
+    };
+    for (int i = 0; i < (int)plan.boxes.size(); ++i)
+        if (short_row(plan.boxes[i])) by_dst[{plan.box_dst_slot[i], plan.box_dst_off[i]}] = i;
+    for (int a = 0; a < (int)plan.boxes.size(); ++a)
+    {
+        const auto& A = plan.boxes[a];
+        if (!short_row(A) || plan.box_pair[a] >= 0) continue;
+        const int64_t want = plan.box_dst_off[a] + ((int64_t)A.n0 - A.d1) * A.esize;
+        auto it = by_dst.find({plan.box_dst_slot[a], want});
+        if (it == by_dst.end()) continue;
+        const int b = it->second;
+        const auto& B = plan.boxes[b];
+        if (b == a || plan.box_pair[b] >= 0 || B.esize != A.esize || B.n1 != A.n1 || B.n2 != A.n2 ||
+            B.d1 != A.d1 || B.d2 != A.d2 || B.field != A.field)
+            continue;
+        plan.box_pair[a] = plan.box_pair[b] = (int)plan.pairs.size();
+        plan.pairs.push_back({a, b});
+    }
+}
+
 } // namespace
 
 void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* fields, int n)
@@ -681,6 +712,7 @@ void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* f
         }
     }
     plan.gather_ok = plan.adjoint_ok && build_cells(plan, plan.gather_reason);
+    find_pairs(plan);
 }
 
 void upload_plan(ghexb_plan_s& plan)
@@ -774,6 +806,34 @@ std::pair<int, int> append_units(std::vector<R>& out, std::vector<R> tiles, Clas
 }
 
 int class_of_x(const xtile& t) { return forward_class_of(t.kind, t.unit, t.neg != 0); }
+
+// The elements of a pair tile that exist, with the decomposition of exchange.cu's pair_elements:
+// fn(a, c, s, i2) with a = element of box A.
+template<typename F>
+void for_pair_elements(const xtile& t, F&& fn)
+{
+    for (uint32_t e = 0; e < t.count; ++e)
+    {
+        const uint32_t g = t.e0 + e;
+        const uint32_t q = fast_div{t.n0, t.m0, t.l0}.div(g);
+        const int64_t c = g - (int64_t)q * t.n0;
+        const uint32_t i2 = fast_div{t.n1, t.m1, t.l1}.div(q);
+        const int64_t s = q - (int64_t)i2 * t.n1;
+        if (c < 0 || c >= t.n0 || s < 0 || s >= t.n1) throw error(GHEXB_ERR_INTERNAL, "pair element decomposition out of range");
+        const bool a = c < (int64_t)t.na;
+        if (a ? s >= 1 : s + 1 < (int64_t)t.n1) fn(a, c, s, (int64_t)i2);
+    }
+}
+
+int64_t valid_elements(const gtile& t) { return t.count; }
+
+int64_t valid_elements(const xtile& t)
+{
+    if (t.kind != 2) return t.count;
+    int64_t n = 0;
+    for_pair_elements(t, [&](bool, int64_t, int64_t, int64_t) { ++n; });
+    return n;
+}
 int class_of_g(const gtile& t) { return gather_class(t.esize, t.nimg); }
 } // namespace
 
@@ -826,6 +886,44 @@ int64_t check_tables(ghexb_plan_s& plan)
     for (size_t i = 0; i < plan.boxes.size(); ++i) replay_range(plan.xb_box[i], plan.box_src_slot[i], plan.box_dst_slot[i]);
     for (size_t i = 0; i < plan.lists.size(); ++i)
         replay_range(plan.xb_list[i], plan.list_src_slot[i], plan.list_dst_slot[i]);
+    // pairs: every element's source and destination, against the two boxes' own mapping
+    for (size_t p = 0; p < plan.pairs.size(); ++p)
+    {
+        const int ia = plan.pairs[p].first, ib = plan.pairs[p].second;
+        const auto& A = plan.boxes[ia];
+        const auto& Bx = plan.boxes[ib];
+        std::vector<std::tuple<const char*, const char*, int>> want, got;
+        for (int which = 0; which < 2; ++which)
+        {
+            const auto& b = which ? Bx : A;
+            for (int32_t i2 = 0; i2 < b.n2; ++i2)
+                for (int32_t i1 = 0; i1 < b.n1; ++i1)
+                    for (int32_t i0 = 0; i0 < b.n0; ++i0)
+                        want.emplace_back(b.dst + ((int64_t)i0 * b.d0 + (int64_t)i1 * b.d1 + (int64_t)i2 * b.d2) * b.esize,
+                            b.src + ((int64_t)i0 * b.s0 + (int64_t)i1 * b.s1 + (int64_t)i2 * b.s2) * b.esize,
+                            b.xor_mask != 0);
+        }
+        const auto& sa = plan.fields[plan.box_src_slot[ia]];
+        const auto& sb = plan.fields[plan.box_src_slot[ib]];
+        const auto& df = plan.fields[plan.box_dst_slot[ia]];
+        const int64_t spa = field_span(sa), spb = field_span(sb), spd = field_span(df);
+        for (int k = plan.xpair_range[p].first; k < plan.xpair_range[p].first + plan.xpair_range[p].second; ++k)
+        {
+            const xtile& t = plan.xpair[k];
+            if ((int)t.count > forward_per_thread(plan.per_thread, t.unit) * plan.block)
+                throw error(GHEXB_ERR_INTERNAL, "forward tile too large");
+            for_pair_elements(t, [&](bool a, int64_t c, int64_t s, int64_t i2) {
+                const int64_t so = a ? c * t.s0 + (s - 1) * t.s1 + i2 * t.s2 : (c - t.na) * t.u0 + s * t.u1 + i2 * t.u2;
+                const int64_t dof = c + (s - 1) * t.d1 + i2 * t.d2;
+                check_offset(a ? sa : sb, a ? t.src : t.src2, so, a ? spa : spb, "source");
+                check_offset(df, t.dst, dof, spd, "destination");
+                got.emplace_back(t.dst + dof * t.unit, (a ? t.src : t.src2) + so * t.unit, a ? t.neg : t.neg2);
+            });
+        }
+        std::sort(want.begin(), want.end());
+        std::sort(got.begin(), got.end());
+        if (want != got) throw error(GHEXB_ERR_INTERNAL, "a pair's segments differ from its two boxes");
+    }
     // every table: units of one class, tile classes consistent with their elements, and the same
     // work in the batched, per-field and per-box tables
     auto check_units = [](const auto& tiles, int begin, int count, auto class_of) {
@@ -837,7 +935,7 @@ int64_t check_tables(ghexb_plan_s& plan)
                 const auto& t = tiles[u + j];
                 if (t.cls != tiles[u].cls || (t.count && class_of(t) != t.cls))
                     throw error(GHEXB_ERR_INTERNAL, "a unit mixes element classes");
-                elems += t.count;
+                elems += valid_elements(t);
             }
         return elems;
     };
@@ -1009,6 +1107,39 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
             out.push_back(t);
         }
     };
+    auto pair_tiles = [&](int p, std::vector<xtile>& out) {
+        const auto& A = plan.boxes[plan.pairs[p].first];
+        const auto& Bx = plan.boxes[plan.pairs[p].second];
+        const uint32_t w = (uint32_t)(A.n0 + Bx.n0), segs = (uint32_t)A.n1 + 1;
+        const fast_div f0 = fast_div::make(w), f1 = fast_div::make(segs);
+        const uint32_t n = (uint32_t)((int64_t)w * segs * A.n2), c = row_cap((int)A.esize, std::max(A.n0, Bx.n0));
+        for (uint32_t e0 = 0; e0 < n; e0 += c)
+        {
+            xtile t{};
+            t.src = A.src, t.dst = A.dst, t.src2 = Bx.src;
+            t.e0 = e0, t.count = std::min(c, n - e0);
+            t.s0 = A.s0, t.s1 = A.s1, t.s2 = A.s2;
+            t.u0 = Bx.s0, t.u1 = Bx.s1, t.u2 = Bx.s2;
+            t.d0 = 1, t.d1 = A.d1, t.d2 = A.d2;
+            t.n0 = f0.d, t.m0 = f0.m, t.l0 = (uint8_t)f0.l;
+            t.n1 = f1.d, t.m1 = f1.m, t.l1 = (uint8_t)f1.l;
+            t.na = (uint32_t)A.n0;
+            t.unit = (uint8_t)A.esize;
+            t.kind = 2;
+            t.neg = A.xor_mask != 0, t.neg2 = Bx.xor_mask != 0;
+            t.cls = (uint8_t)class_of_x(t);
+            out.push_back(t);
+        }
+    };
+    std::vector<std::vector<xtile>> ptiles(plan.pairs.size());
+    plan.xpair.clear();
+    plan.xpair_range.clear();
+    for (size_t p = 0; p < plan.pairs.size(); ++p)
+    {
+        pair_tiles((int)p, ptiles[p]);
+        plan.xpair_range.push_back({(int)plan.xpair.size(), (int)ptiles[p].size()});
+        plan.xpair.insert(plan.xpair.end(), ptiles[p].begin(), ptiles[p].end());
+    }
     // tiles per descriptor, with their element class
     std::vector<std::vector<xtile>> btiles(plan.boxes.size()), ltiles(plan.lists.size());
     for (size_t i = 0; i < plan.boxes.size(); ++i)
@@ -1034,7 +1165,10 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
     {
         std::vector<xtile> f;
         for (size_t i = 0; i < plan.boxes.size(); ++i)
-            if ((int)plan.boxes[i].field == lg) f.insert(f.end(), btiles[i].begin(), btiles[i].end());
+            if ((int)plan.boxes[i].field == lg && (!plan.use_pairs || plan.box_pair[i] < 0))
+                f.insert(f.end(), btiles[i].begin(), btiles[i].end());
+        for (size_t p = 0; p < plan.pairs.size() && plan.use_pairs; ++p)
+            if ((int)plan.boxes[plan.pairs[p].first].field == lg) f.insert(f.end(), ptiles[p].begin(), ptiles[p].end());
         for (size_t i = 0; i < plan.lists.size(); ++i)
             if ((int)plan.lists[i].field == lg) f.insert(f.end(), ltiles[i].begin(), ltiles[i].end());
         plan.xp_field[lg] = append_units(plan.xp, std::move(f), class_of_x);
@@ -1043,7 +1177,10 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
     // that the first wave of CTAs starts on the most expensive tiles
     {
         std::vector<xtile> all;
-        for (const auto& v : btiles) all.insert(all.end(), v.begin(), v.end());
+        for (size_t i = 0; i < plan.boxes.size(); ++i)
+            if (!plan.use_pairs || plan.box_pair[i] < 0) all.insert(all.end(), btiles[i].begin(), btiles[i].end());
+        if (plan.use_pairs)
+            for (const auto& v : ptiles) all.insert(all.end(), v.begin(), v.end());
         for (const auto& v : ltiles) all.insert(all.end(), v.begin(), v.end());
         auto per_elem = [](const xtile& t) { return tile_cost(t) / std::max<uint32_t>(1u, t.count); };
         std::stable_sort(all.begin(), all.end(), [&](const xtile& x, const xtile& y) { return per_elem(x) > per_elem(y); });
@@ -1244,10 +1381,13 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
     struct cand
     {
         int k, block;
+        bool pairs;
     };
     std::vector<cand> cands;
     for (int k : {4, 8, 16})
-        for (int block : {128, 256, 512}) cands.push_back({k, block});
+        for (int block : {128, 256, 512})
+            for (bool pairs : {false, true})
+                if (!pairs || !plan.pairs.empty()) cands.push_back({k, block, pairs});
 
     // every timed launch starts with a cold L2: read a buffer of twice the L2 size first
     int l2 = 0;
@@ -1263,7 +1403,7 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         if (e1) cudaEventDestroy(e1);
     };
     float best = 1e30f;
-    cand bestc{plan.per_thread, plan.block};
+    cand bestc{plan.per_thread, plan.block, plan.use_pairs};
     try
     {
         check_cuda(cudaMalloc(&flush, flush_bytes), "cudaMalloc(l2 flush)");
@@ -1274,7 +1414,7 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         const int fgrid = (plan.ctx ? plan.ctx->num_sms : 148) * 8;
         for (const auto& c : cands)
         {
-            plan.per_thread = c.k, plan.block = c.block;
+            plan.per_thread = c.k, plan.block = c.block, plan.use_pairs = c.pairs;
             retile(plan, stream);
             launch_plan(plan, GHEXB_FORM_BATCHED, stream); // warm-up
             float total = 0.f;
@@ -1298,7 +1438,7 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         throw;
     }
     cleanup();
-    plan.per_thread = bestc.k, plan.block = bestc.block;
+    plan.per_thread = bestc.k, plan.block = bestc.block, plan.use_pairs = bestc.pairs;
     retile(plan, stream);
     check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
 }

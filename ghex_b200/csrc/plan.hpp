@@ -37,6 +37,12 @@ struct ghexb_plan_s
     // class), xp the per-field form's (grouped by logical field, then class) and xb the per-box
     // form's (grouped by descriptor); each launch range is padded per class with empty tiles.
     std::vector<ghexb::xtile> xf, xp, xb;
+    // x-face boxes whose rows interleave (A's row r ends where B's row r + 1 begins): the
+    // batched and per-field tables move each pair as one set of contiguous segments
+    std::vector<std::pair<int, int>> pairs; // (A, B) box indices
+    std::vector<int> box_pair;              // per box: its pair, or -1
+    std::vector<ghexb::xtile> xpair;        // host only: the pairs' tiles, for the replay check
+    std::vector<std::pair<int, int>> xpair_range;
     std::vector<std::pair<int, int>> xp_field;          // [begin, count) in xp per logical field
     std::vector<std::pair<int, int>> xb_box, xb_list;   // [begin, count) in xb per descriptor
     // Box adjoint in gather form (gather_ok), else by conflict-free phases of the box descriptors.
@@ -76,6 +82,7 @@ struct ghexb_plan_s
     // tuning: elements per thread (4, 8 or 16) and threads per CTA of the forward kernel
     int per_thread = 8;
     int block = 256;
+    bool use_pairs = true; // batched and per-field tables move x-face pairs as segments
 
     // graph of the batched form
     cudaStream_t cap_stream = nullptr;

@@ -66,6 +66,9 @@ typedef struct ghexb_plan_info_t
     int32_t elems_per_thread;  /* current tuning: elements a thread moves (4, 8 or 16) */
     int32_t block;             /* current tuning: threads per CTA */
     int32_t grid;              /* CTAs of the batched launch: one per tile */
+    int32_t pairs;             /* pairs of x-face boxes whose rows interleave in memory */
+    int32_t use_pairs;         /* current tuning: 1 if the batched and per-field forms move those
+                                  pairs as contiguous row-boundary segments */
     int32_t reserved;
 } ghexb_plan_info_t;
 
@@ -176,8 +179,9 @@ int ghexb_plan_check(ghexb_context ctx, const ghexb_field* fields, int n, int64_
 int ghexb_plan_get_info(ghexb_plan plan, ghexb_plan_info_t* info);
 /* elems_per_thread (4, 8 or 16) and block (a multiple of 32, at most 512); values <= 0 keep the
  * current one. A tile holds elems_per_thread * block elements (half as many 16-byte units).
+ * use_pairs: 1 moves the x-face pairs as contiguous segments, 0 as separate boxes, < 0 keeps.
  * Invalidates the captured graph. */
-int ghexb_plan_set_tuning(ghexb_plan plan, int elems_per_thread, int block);
+int ghexb_plan_set_tuning(ghexb_plan plan, int elems_per_thread, int block, int use_pairs);
 /* One forward exchange in the given form, stream-ordered. */
 int ghexb_plan_launch(ghexb_plan plan, int form, void* stream);
 /* The batched form captured once into a CUDA graph and replayed on `stream`. */

@@ -55,7 +55,7 @@ def test_tunings_bitexact(cuda, per_thread, block):
     run = RegularRun(W.config1(shape=(50, 40, 12)), cuda)
     expected = run.oracle()
     plan = R.make_exchange_plan(run.ctx, run.bis)
-    plan.set_tuning(per_thread, block)
+    plan.set_tuning(per_thread, block, 1)
     for form in (plan.BATCHED, plan.PER_FIELD, plan.PER_BOX):
         run.reset()
         plan.launch(form)
@@ -162,3 +162,27 @@ def test_adjoint_bitexact(cuda, cfg):
         for spec in specs:
             O.adjoint(pat, doms, grads[spec.name], [w.offsets(spec)] * len(doms))
     assert run.mismatches(grads) == {}
+
+
+@pytest.mark.parametrize("halos", [(2, 1, 1, 1, 0, 0), (3, 3, 1, 2, 1, 1), (1, 1, 1, 1, 1, 1)])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_paired_x_faces_bitexact(cuda, halos, dtype):
+    """x-face boxes of both sides of a row boundary move as one contiguous segment (equal and
+    unequal halo widths): every form bit-exact against the oracle."""
+    shape = (24, 20, 10)
+    w = W.RegularWorkload("pairs", shape, (True, True, False), W.regular_decomposition(shape, (3, 2, 1), 7))
+    w.fields = [W.FieldSpec("f", dtype, halos, 5), W.FieldSpec("g", dtype, halos, 6)]
+    run = RegularRun(w, cuda)
+    expected = run.oracle()
+    plan = R.make_exchange_plan(run.ctx, run.bis)
+    assert plan.info()["pairs"] >= 2 * len(w.domains)
+    for pairs in (1, 0):
+        plan.set_tuning(0, 0, pairs)
+        assert plan.info()["use_pairs"] == pairs
+        for form in (plan.BATCHED, plan.PER_FIELD, plan.PER_BOX):
+            run.reset()
+            plan.launch(form)
+            assert run.mismatches(expected) == {}
+    run.reset()
+    plan.graph_launch()
+    assert run.mismatches(expected) == {}
