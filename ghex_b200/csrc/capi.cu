@@ -523,7 +523,7 @@ int ghexb_plan_get_info(ghexb_plan plan, ghexb_plan_info_t* info)
         info->adjoint_cells = plan->gather_ok ? (int64_t)plan->cells.size() : 0;
         info->elems_per_thread = plan->per_thread;
         info->block = plan->block;
-        info->grid = (int32_t)(plan->xf.size() / ghexb::k_unit_tiles);
+        info->grid = (int32_t)plan->xf.size();
         info->pairs = (int32_t)plan->pairs.size();
         info->use_pairs = plan->use_pairs ? 1 : 0;
         info->reserved = 0;

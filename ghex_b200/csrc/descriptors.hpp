@@ -152,6 +152,9 @@ constexpr int k_xtile_words = 7;
 // a cell was copied to the same ordered list of halo images. For an owner element o:
 //   acc = own[o]; for each image i in order: acc = acc (+|-) img_i[o]; img_i[o] = 0; own[o] = acc
 // which is the explicit transpose in receive order, with no two threads touching one element.
+// Unstructured columns take the same form: a group of owner columns with the same number of
+// images; the column table holds, per owner, the address of its column and of each image's
+// column (nimg + 1 addresses), and element e of the group is level e mod n0 of owner e / n0.
 constexpr int k_max_images = 8;
 
 struct gimage
@@ -163,16 +166,19 @@ struct gimage
 
 struct alignas(16) gtile
 {
-    char* own;            // owner element (0,0,0) of the cell
-    uint32_t e0, count;   // elements [e0, e0 + count) of the cell
-    int32_t o0, o1, o2;   // owner element strides per cell axis (axis 0 fastest)
+    char* own;            // box: owner element (0,0,0) of the cell
+    uint32_t e0, count;   // elements [e0, e0 + count) of the cell (list: of the owner group)
+    int32_t o0, o1, o2;   // owner element strides per cell axis (axis 0 fastest); list: o0 = level stride
     uint32_t n0, m0, n1, m1;
     uint8_t l0, l1;
     uint8_t esize;        // 4 or 8 (float or double)
     uint8_t nimg;         // 1..k_max_images
-    gimage img[k_max_images];
-    uint8_t cls;          // element class (exchange.hpp): esize and nimg in one value
-    uint8_t pad[15];
+    gimage img[k_max_images]; // list: img[0].t0 = level stride of the images
+    uint8_t cls;          // element class (exchange.hpp): kind, esize and nimg in one value
+    uint8_t kind;         // 0 box cell, 1 group of unstructured owner columns
+    uint8_t pad0[2];
+    uint32_t col0;        // list: first entry of the group in the column table
+    uint8_t pad[8];
 };
 static_assert(sizeof(gtile) == 256, "gtile is sixteen 16-byte words");
 

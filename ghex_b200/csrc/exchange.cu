@@ -3,13 +3,12 @@
 // The exchange is pure data movement, latency-bound at halo sizes: a kernel's time is a few
 // dependent memory round trips plus the bytes over HBM bandwidth. The kernels are built for few
 // round trips and many bytes in flight:
-//  * one launch covers every tile; a CTA runs a unit of k_unit_tiles consecutive tiles of one
-//    element class (box or list, element size, negation; for the adjoint the number of images)
-//    in a loop specialised for that class, and the hardware block scheduler balances units
-//    across SMs: no scheduler of ours, no atomics, CTAs never wait on each other;
-//  * a tile record carries everything needed to address its elements (96 bytes forward, 256
-//    bytes adjoint); the next record of the unit is fetched while the current tile's data loads
-//    are in flight, so only a unit's first record costs a round trip of its own;
+//  * one launch covers every tile, one CTA per tile; a CTA runs the code specialised for its
+//    tile's element class (box, pair of x faces or list; element size; negation; for the
+//    adjoint the number of images), and the hardware block scheduler balances CTAs across SMs:
+//    no scheduler of ours, no atomics, CTAs never wait on each other;
+//  * a tile record carries everything needed to address its elements (112 bytes forward, 256
+//    bytes adjoint): one round trip before the data loads;
 //  * every thread issues all of its K loads before its first store, so K elements per thread
 //    are in flight; consecutive threads take consecutive elements, so rows along the
 //    destination's contiguous dimension are coalesced;
@@ -54,36 +53,13 @@ template<> __device__ __forceinline__ uint8_t ld_stream(const uint8_t* p)
     return __ldcg(reinterpret_cast<const unsigned char*>(p));
 }
 
-// Runs body(t) on the k_unit_tiles tiles of this CTA's unit, starting from the record already in
-// shared memory. The next record is fetched into registers (by W threads) before the current
-// tile's body, so that its round trip overlaps the tile's data loads, and replaces the shared
-// record between two barriers after it.
-template<int W, typename R, typename Body>
-__device__ __forceinline__ void unit_loop(R& t, const R* __restrict__ unit, Body body)
-{
-#pragma unroll 1
-    for (int j = 0;; ++j)
-    {
-        const bool more = j + 1 < k_unit_tiles;
-        const bool fetch = more && threadIdx.x < W;
-        uint4 pre = make_uint4(0u, 0u, 0u, 0u);
-        if (fetch) pre = __ldg(reinterpret_cast<const uint4*>(unit + j + 1) + threadIdx.x);
-        body(t);
-        if (!more) break;
-        __syncthreads();
-        if (fetch) reinterpret_cast<uint4*>(&t)[threadIdx.x] = pre;
-        __syncthreads();
-    }
-}
-
-// Loads the first record of this CTA's unit into shared memory.
+// Loads this CTA's record (W 16-byte words) into shared memory.
 template<int W, typename R>
-__device__ __forceinline__ const R* first_record(R& t, const R* __restrict__ tiles)
+__device__ __forceinline__ void load_record(R& t, const R* __restrict__ tiles)
 {
-    const R* unit = tiles + (size_t)blockIdx.x * k_unit_tiles;
-    if (threadIdx.x < W) reinterpret_cast<uint4*>(&t)[threadIdx.x] = __ldg(reinterpret_cast<const uint4*>(unit) + threadIdx.x);
+    if (threadIdx.x < W)
+        reinterpret_cast<uint4*>(&t)[threadIdx.x] = __ldg(reinterpret_cast<const uint4*>(tiles + blockIdx.x) + threadIdx.x);
     __syncthreads();
-    return unit;
 }
 
 // ---- forward ---------------------------------------------------------------------------------
@@ -194,11 +170,11 @@ template<int K>
 __global__ void __launch_bounds__(k_max_block, K >= 16 ? 1 : 2) exchange_kernel(const xtile* __restrict__ tiles)
 {
     __shared__ xtile t;
-    const xtile* unit = first_record<k_xtile_words>(t, tiles);
+    load_record<k_xtile_words>(t, tiles);
     switch (t.cls)
     {
 #define GHEXB_CASE(C, F)                                                                                               \
-    case C: unit_loop<k_xtile_words>(t, unit, [](const xtile& x) { F(x); }); break;
+    case C: F(t); break;
         GHEXB_CASE(k_box8, (box_elements<K, unsigned long long, false>))
         GHEXB_CASE(k_box8_neg, (box_elements<K, unsigned long long, true>))
         GHEXB_CASE(k_box4, (box_elements<K, uint32_t, false>))
@@ -264,18 +240,67 @@ __device__ __forceinline__ void gather_elements(const gtile& t)
         }
 }
 
-__global__ void __launch_bounds__(k_gather_block, 3) gather_kernel(const gtile* __restrict__ tiles)
+// Unstructured owner columns: element e is level e mod n0 of owner e / n0 of the group; the
+// owner's and its images' column addresses come from the column table.
+template<int K, int NI, typename F>
+__device__ __forceinline__ void list_gather_elements(const gtile& t, const uint64_t* __restrict__ cols)
+{
+    F h[K][NI];
+    F acc[K];
+    F* own[K];
+    F* img[K][NI];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+    {
+        const uint32_t e = k * blockDim.x + threadIdx.x;
+        if (e < t.count)
+        {
+            const uint32_t g = t.e0 + e;
+            const uint32_t j = fdiv(g, t.m0, t.l0);
+            const int32_t lev = (int32_t)(g - j * t.n0);
+            const uint64_t* p = cols + t.col0 + (size_t)j * (NI + 1);
+            own[k] = reinterpret_cast<F*>(__ldg(p)) + lev * t.o0;
+#pragma unroll
+            for (int i = 0; i < NI; ++i) img[k][i] = reinterpret_cast<F*>(__ldg(p + 1 + i)) + lev * t.img[0].t0;
+            acc[k] = __ldcg(own[k]);
+#pragma unroll
+            for (int i = 0; i < NI; ++i) h[k][i] = __ldcg(img[k][i]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if (k * blockDim.x + threadIdx.x < t.count)
+        {
+            F a = acc[k];
+#pragma unroll
+            for (int i = 0; i < NI; ++i)
+            {
+                a = a + h[k][i];
+                *img[k][i] = F(0);
+            }
+            *own[k] = a;
+        }
+}
+
+__global__ void __launch_bounds__(k_gather_block, 3) gather_kernel(const gtile* __restrict__ tiles,
+    const uint64_t* __restrict__ cols)
 {
     __shared__ gtile t;
-    const gtile* unit = first_record<16>(t, tiles);
+    load_record<16>(t, tiles);
     switch (t.cls)
     {
 #define GHEXB_CASE(NI)                                                                                                 \
     case gather_class(8, NI):                                                                                          \
-        unit_loop<16>(t, unit, [](const gtile& x) { gather_elements<gather_per_thread(NI), NI, double>(x); });       \
+        gather_elements<gather_per_thread(NI), NI, double>(t);                                                        \
         break;                                                                                                         \
     case gather_class(4, NI):                                                                                          \
-        unit_loop<16>(t, unit, [](const gtile& x) { gather_elements<gather_per_thread(NI), NI, float>(x); });        \
+        gather_elements<gather_per_thread(NI), NI, float>(t);                                                         \
+        break;                                                                                                         \
+    case list_gather_class(8, NI):                                                                                     \
+        list_gather_elements<gather_per_thread(NI), NI, double>(t, cols);                                             \
+        break;                                                                                                         \
+    case list_gather_class(4, NI):                                                                                     \
+        list_gather_elements<gather_per_thread(NI), NI, float>(t, cols);                                              \
         break;
         GHEXB_CASE(1)
         GHEXB_CASE(2)
@@ -295,8 +320,8 @@ __global__ void __launch_bounds__(k_gather_block, 3) gather_kernel(const gtile* 
 cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cudaStream_t stream)
 {
     if (ntiles <= 0) return cudaSuccess;
-    if (ntiles % k_unit_tiles || block < 32 || block > k_max_block || block % 32) return cudaErrorInvalidValue;
-    const int grid = ntiles / k_unit_tiles;
+    if (block < 32 || block > k_max_block || block % 32) return cudaErrorInvalidValue;
+    const int grid = ntiles;
     switch (k)
     {
         case 4: exchange_kernel<4><<<grid, block, 0, stream>>>(tiles); break;
@@ -307,11 +332,10 @@ cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cu
     return cudaGetLastError();
 }
 
-cudaError_t launch_gather(const gtile* tiles, int ntiles, cudaStream_t stream)
+cudaError_t launch_gather(const gtile* tiles, int ntiles, const uint64_t* cols, cudaStream_t stream)
 {
     if (ntiles <= 0) return cudaSuccess;
-    if (ntiles % k_unit_tiles) return cudaErrorInvalidValue;
-    gather_kernel<<<ntiles / k_unit_tiles, k_gather_block, 0, stream>>>(tiles);
+    gather_kernel<<<ntiles, k_gather_block, 0, stream>>>(tiles, cols);
     return cudaGetLastError();
 }
 } // namespace ghexb

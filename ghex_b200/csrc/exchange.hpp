@@ -57,16 +57,18 @@ __host__ __device__ constexpr int gather_class(int esize, int nimg)
 {
     return (esize == 8 ? 0 : k_max_images) + (nimg - 1);
 }
-constexpr int k_gather_classes = 2 * k_max_images;
+// classes of unstructured owner groups follow those of box cells
+__host__ __device__ constexpr int list_gather_class(int esize, int nimg)
+{
+    return 2 * k_max_images + gather_class(esize, nimg);
+}
+constexpr int k_gather_classes = 4 * k_max_images;
 
-// A CTA runs k_unit_tiles consecutive tiles of one class: the tile tables of every launch are
-// padded, per class, to a multiple of k_unit_tiles with empty tiles (count 0) of that class.
-constexpr int k_unit_tiles = 1;
-
-// Forward exchange of tiles[0, ntiles) (ntiles a multiple of k_unit_tiles): a tile holds at most
+// Forward exchange of tiles[0, ntiles), one CTA per tile: a tile holds at most
 // forward_per_thread(k, unit) * block elements; k is 4, 8 or 16.
 cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cudaStream_t stream);
-// Box adjoint of tiles[0, ntiles) (a multiple of k_unit_tiles): a tile holds at most
-// gather_per_thread(nimg) * k_gather_block elements.
-cudaError_t launch_gather(const gtile* tiles, int ntiles, cudaStream_t stream);
+// Adjoint in gather form of tiles[0, ntiles), one CTA per tile: a tile holds at most
+// gather_per_thread(nimg) * k_gather_block elements; `cols` is the column table of the
+// unstructured owner groups (may be null without them).
+cudaError_t launch_gather(const gtile* tiles, int ntiles, const uint64_t* cols, cudaStream_t stream);
 } // namespace ghexb

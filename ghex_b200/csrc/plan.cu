@@ -569,6 +569,53 @@ void find_pairs(ghexb_plan_s& plan)
     }
 }
 
+// Owner columns of the unstructured adjoint lists, each with its image columns in receive order.
+// Returns false when an owner has more than k_max_images images or its images differ in levels
+// or level stride.
+bool build_list_owners(ghexb_plan_s& plan, std::string& why)
+{
+    plan.lowners.clear();
+    std::map<std::pair<int, int64_t>, int> index; // (slot, byte offset) -> owner
+    for (size_t i = 0; i < plan.adj_lists.size(); ++i)
+    {
+        const auto& l = plan.adj_lists[i];
+        const int ss = plan.adj_src_slot[i], ds = plan.adj_dst_slot[i];
+        const int es = plan.fields[ss].esize;
+        for (int32_t k = 0; k < l.count; ++k)
+        {
+            const int64_t so = plan.adj_src_off[i] + (int64_t)plan.idx[plan.adj_idx_off[i] + k] * l.s_is * es;
+            const int64_t dof = plan.adj_dst_off[i] + (int64_t)plan.idx[plan.adj_didx_off[i] + k] * l.d_is * es;
+            auto it = index.find({ss, so});
+            if (it == index.end())
+            {
+                ghexb_plan_s::list_owner o{};
+                o.slot = ss, o.off = so, o.levels = l.levels, o.s_ls = l.s_ls, o.d_ls = l.d_ls, o.esize = es;
+                it = index.emplace(std::make_pair(ss, so), (int)plan.lowners.size()).first;
+                plan.lowners.push_back(o);
+            }
+            auto& o = plan.lowners[it->second];
+            if (o.levels != l.levels || o.s_ls != l.s_ls || o.d_ls != l.d_ls)
+            {
+                why = "an owner column's images differ in levels or level stride";
+                return false;
+            }
+            if (o.nimg == k_max_images)
+            {
+                why = "an owner column has more than " + std::to_string(k_max_images) + " images";
+                return false;
+            }
+            o.img_slot[o.nimg] = ds;
+            o.img_off[o.nimg] = dof;
+            ++o.nimg;
+        }
+    }
+    std::stable_sort(plan.lowners.begin(), plan.lowners.end(), [](const auto& a, const auto& b) {
+        return std::make_tuple(a.esize, a.nimg, a.levels, a.s_ls, a.d_ls) <
+               std::make_tuple(b.esize, b.nimg, b.levels, b.s_ls, b.d_ls);
+    });
+    return true;
+}
+
 } // namespace
 
 void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* fields, int n)
@@ -712,6 +759,8 @@ void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* f
         }
     }
     plan.gather_ok = plan.adjoint_ok && build_cells(plan, plan.gather_reason);
+    std::string list_reason;
+    plan.list_gather_ok = plan.adjoint_ok && build_list_owners(plan, list_reason);
     find_pairs(plan);
 }
 
@@ -783,26 +832,13 @@ double tile_cost(const xtile& t) { return run_cost(t.count, t.unit, t.n0); }
 
 double tile_cost(const gtile& t) { return run_cost(t.count, t.esize, t.n0) * 2.0 * (1 + t.nimg); }
 
-// Appends the tiles of one launch range, grouped by class (stable), padding every class to a
-// multiple of k_unit_tiles with empty tiles of that class. Returns [begin, count) in out.
-template<typename R, typename ClassOf>
-std::pair<int, int> append_units(std::vector<R>& out, std::vector<R> tiles, ClassOf class_of)
+// Appends the tiles of one launch range; returns [begin, count) in out.
+template<typename R>
+std::pair<int, int> append_range(std::vector<R>& out, const std::vector<R>& tiles)
 {
-    std::stable_sort(tiles.begin(), tiles.end(), [&](const R& a, const R& b) { return class_of(a) < class_of(b); });
     const int begin = (int)out.size();
-    for (size_t i = 0; i < tiles.size();)
-    {
-        size_t j = i;
-        while (j < tiles.size() && class_of(tiles[j]) == class_of(tiles[i])) out.push_back(tiles[j++]);
-        while ((out.size() - begin) % k_unit_tiles)
-        {
-            R pad{};
-            pad.cls = tiles[i].cls;
-            out.push_back(pad);
-        }
-        i = j;
-    }
-    return {begin, (int)out.size() - begin};
+    out.insert(out.end(), tiles.begin(), tiles.end());
+    return {begin, (int)tiles.size()};
 }
 
 int class_of_x(const xtile& t) { return forward_class_of(t.kind, t.unit, t.neg != 0); }
@@ -834,7 +870,7 @@ int64_t valid_elements(const xtile& t)
     for_pair_elements(t, [&](bool, int64_t, int64_t, int64_t) { ++n; });
     return n;
 }
-int class_of_g(const gtile& t) { return gather_class(t.esize, t.nimg); }
+int class_of_g(const gtile& t) { return t.kind ? list_gather_class(t.esize, t.nimg) : gather_class(t.esize, t.nimg); }
 } // namespace
 
 int64_t check_tables(ghexb_plan_s& plan)
@@ -924,30 +960,27 @@ int64_t check_tables(ghexb_plan_s& plan)
         std::sort(got.begin(), got.end());
         if (want != got) throw error(GHEXB_ERR_INTERNAL, "a pair's segments differ from its two boxes");
     }
-    // every table: units of one class, tile classes consistent with their elements, and the same
+    // every table: tile classes consistent with their elements, and the same
     // work in the batched, per-field and per-box tables
-    auto check_units = [](const auto& tiles, int begin, int count, auto class_of) {
-        if (count % k_unit_tiles) throw error(GHEXB_ERR_INTERNAL, "launch range not a whole number of units");
+    auto check_tiles = [](const auto& tiles, int begin, int count, auto class_of) {
         int64_t elems = 0;
-        for (int u = begin; u < begin + count; u += k_unit_tiles)
-            for (int j = 0; j < k_unit_tiles; ++j)
-            {
-                const auto& t = tiles[u + j];
-                if (t.cls != tiles[u].cls || (t.count && class_of(t) != t.cls))
-                    throw error(GHEXB_ERR_INTERNAL, "a unit mixes element classes");
-                elems += valid_elements(t);
-            }
+        for (int u = begin; u < begin + count; ++u)
+        {
+            const auto& t = tiles[u];
+            if (t.count == 0 || class_of(t) != t.cls) throw error(GHEXB_ERR_INTERNAL, "a tile's class differs from its elements");
+            elems += valid_elements(t);
+        }
         return elems;
     };
-    const int64_t nf = check_units(plan.xf, 0, (int)plan.xf.size(), class_of_x);
+    const int64_t nf = check_tiles(plan.xf, 0, (int)plan.xf.size(), class_of_x);
     int64_t np = 0, nb = 0;
-    for (const auto& r : plan.xp_field) np += check_units(plan.xp, r.first, r.second, class_of_x);
-    for (const auto& r : plan.xb_box) nb += check_units(plan.xb, r.first, r.second, class_of_x);
-    for (const auto& r : plan.xb_list) nb += check_units(plan.xb, r.first, r.second, class_of_x);
+    for (const auto& r : plan.xp_field) np += check_tiles(plan.xp, r.first, r.second, class_of_x);
+    for (const auto& r : plan.xb_box) nb += check_tiles(plan.xb, r.first, r.second, class_of_x);
+    for (const auto& r : plan.xb_list) nb += check_tiles(plan.xb, r.first, r.second, class_of_x);
     if (nf != nb || np != nb) throw error(GHEXB_ERR_INTERNAL, "batched, per-field and per-box tables differ");
     if (plan.gather_ok)
     {
-        check_units(plan.gt, 0, (int)plan.gt.size(), class_of_g);
+        check_tiles(plan.gt, 0, (int)plan.gt.size(), class_of_g);
         for (const auto& t : plan.gt)
             if ((int)t.count > gather_per_thread(t.nimg) * k_gather_block)
                 throw error(GHEXB_ERR_INTERNAL, "gather tile too large");
@@ -995,6 +1028,58 @@ int64_t check_tables(ghexb_plan_s& plan)
         std::sort(images.begin(), images.end());
         std::sort(box_dst.begin(), box_dst.end());
         if (images != box_dst) throw error(GHEXB_ERR_INTERNAL, "adjoint images differ from the forward destinations");
+        checked += (int64_t)images.size();
+    }
+    // unstructured owner columns: every level in bounds, owners pairwise distinct, images equal to
+    // the destinations of the adjoint lists, and the tiles cover every owner level once
+    if (plan.list_gather_ok)
+    {
+        std::vector<std::pair<int, int64_t>> owners, images, list_dst;
+        int64_t levels = 0;
+        for (const auto& o : plan.lowners)
+        {
+            const int64_t es = o.esize;
+            for (int32_t lev = 0; lev < o.levels; ++lev)
+            {
+                const int64_t oe = o.off / es + (int64_t)lev * o.s_ls;
+                if (o.off % es || oe < 0 || oe >= field_span(plan.fields[o.slot]))
+                    throw error(GHEXB_ERR_RANGE, "adjoint owner column outside its field");
+                owners.push_back({o.slot, oe});
+                for (int i = 0; i < o.nimg; ++i)
+                {
+                    const int64_t he = o.img_off[i] / es + (int64_t)lev * o.d_ls;
+                    if (o.img_off[i] % es || he < 0 || he >= field_span(plan.fields[o.img_slot[i]]))
+                        throw error(GHEXB_ERR_RANGE, "adjoint image column outside its field");
+                    images.push_back({o.img_slot[i], he});
+                }
+            }
+            levels += o.levels;
+        }
+        for (size_t i = 0; i < plan.adj_lists.size(); ++i)
+        {
+            const auto& l = plan.adj_lists[i];
+            const int slot = plan.adj_dst_slot[i];
+            const int64_t es = plan.fields[slot].esize;
+            for (int32_t k = 0; k < l.count; ++k)
+                for (int32_t lev = 0; lev < l.levels; ++lev)
+                    list_dst.push_back({slot, plan.adj_dst_off[i] / es + (int64_t)plan.idx[plan.adj_didx_off[i] + k] * l.d_is +
+                                                  (int64_t)lev * l.d_ls});
+        }
+        std::sort(owners.begin(), owners.end());
+        if (std::adjacent_find(owners.begin(), owners.end()) != owners.end())
+            throw error(GHEXB_ERR_INTERNAL, "an owner element appears in two adjoint columns");
+        std::sort(images.begin(), images.end());
+        std::sort(list_dst.begin(), list_dst.end());
+        if (images != list_dst) throw error(GHEXB_ERR_INTERNAL, "adjoint images differ from the list destinations");
+        int64_t covered = 0;
+        for (const auto& t : plan.gt)
+            if (t.kind == 1)
+            {
+                covered += t.count;
+                if ((int64_t)t.col0 + (int64_t)(t.e0 + t.count - 1) / t.n0 * (t.nimg + 1) + t.nimg >= (int64_t)plan.lcols.size())
+                    throw error(GHEXB_ERR_INTERNAL, "adjoint tile outside the column table");
+            }
+        if (covered != levels) throw error(GHEXB_ERR_INTERNAL, "adjoint tiles do not cover every owner level");
         checked += (int64_t)images.size();
     }
     // phased adjoint lists
@@ -1048,10 +1133,12 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
     ensure(plan.d_xp, plan.cap_xp, plan.xp.size());
     ensure(plan.d_xb, plan.cap_xb, plan.xb.size());
     ensure(plan.d_gt, plan.cap_gt, plan.gt.size());
+    ensure(plan.d_lcols, plan.cap_lcols, plan.lcols.size());
     copy_async(plan.d_xf, plan.xf, stream);
     copy_async(plan.d_xp, plan.xp, stream);
     copy_async(plan.d_xb, plan.xb, stream);
     copy_async(plan.d_gt, plan.gt, stream);
+    copy_async(plan.d_lcols, plan.lcols, stream);
     upload(plan.d_adj_btiles, plan.adj_btiles);
     upload(plan.d_adj_ltiles, plan.adj_ltiles);
 }
@@ -1156,8 +1243,8 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
     plan.xb.clear();
     plan.xb_box.assign(plan.boxes.size(), {0, 0});
     plan.xb_list.assign(plan.lists.size(), {0, 0});
-    for (size_t i = 0; i < plan.boxes.size(); ++i) plan.xb_box[i] = append_units(plan.xb, btiles[i], class_of_x);
-    for (size_t i = 0; i < plan.lists.size(); ++i) plan.xb_list[i] = append_units(plan.xb, ltiles[i], class_of_x);
+    for (size_t i = 0; i < plan.boxes.size(); ++i) plan.xb_box[i] = append_range(plan.xb, btiles[i]);
+    for (size_t i = 0; i < plan.lists.size(); ++i) plan.xb_list[i] = append_range(plan.xb, ltiles[i]);
     // per field: one range per logical field
     plan.xp.clear();
     plan.xp_field.assign(plan.n_logical, {0, 0});
@@ -1171,10 +1258,10 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
             if ((int)plan.boxes[plan.pairs[p].first].field == lg) f.insert(f.end(), ptiles[p].begin(), ptiles[p].end());
         for (size_t i = 0; i < plan.lists.size(); ++i)
             if ((int)plan.lists[i].field == lg) f.insert(f.end(), ltiles[i].begin(), ltiles[i].end());
-        plan.xp_field[lg] = append_units(plan.xp, std::move(f), class_of_x);
+        plan.xp_field[lg] = append_range(plan.xp, f);
     }
-    // batched: one range; within a class the most DRAM bytes per element (short rows) first, so
-    // that the first wave of CTAs starts on the most expensive tiles
+    // batched: one range, the most DRAM bytes per element (short rows) first, so that the first
+    // wave of CTAs starts on the most expensive tiles
     {
         std::vector<xtile> all;
         for (size_t i = 0; i < plan.boxes.size(); ++i)
@@ -1185,7 +1272,7 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
         auto per_elem = [](const xtile& t) { return tile_cost(t) / std::max<uint32_t>(1u, t.count); };
         std::stable_sort(all.begin(), all.end(), [&](const xtile& x, const xtile& y) { return per_elem(x) > per_elem(y); });
         plan.xf.clear();
-        append_units(plan.xf, std::move(all), class_of_x);
+        append_range(plan.xf, all);
     }
 
     // ---- box adjoint, gather form
@@ -1220,10 +1307,50 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
                 all.push_back(t);
             }
         }
-        append_units(plan.gt, std::move(all), class_of_g);
+        append_range(plan.gt, all);
+    }
+    // ---- unstructured adjoint, gather form: owner groups and their column table
+    plan.lcols.clear();
+    if (plan.list_gather_ok)
+    {
+        for (size_t a = 0; a < plan.lowners.size();)
+        {
+            const auto& o0 = plan.lowners[a];
+            size_t b = a;
+            while (b < plan.lowners.size() && plan.lowners[b].esize == o0.esize && plan.lowners[b].nimg == o0.nimg &&
+                   plan.lowners[b].levels == o0.levels && plan.lowners[b].s_ls == o0.s_ls && plan.lowners[b].d_ls == o0.d_ls)
+                ++b;
+            const uint32_t col0 = (uint32_t)plan.lcols.size();
+            for (size_t j = a; j < b; ++j)
+            {
+                const auto& o = plan.lowners[j];
+                plan.lcols.push_back((uint64_t)(uintptr_t)(plan.fields[o.slot].data + o.off));
+                for (int i = 0; i < o.nimg; ++i)
+                    plan.lcols.push_back((uint64_t)(uintptr_t)(plan.fields[o.img_slot[i]].data + o.img_off[i]));
+            }
+            const uint32_t gc = (uint32_t)(gather_per_thread(o0.nimg) * k_gather_block);
+            const uint32_t n = (uint32_t)((int64_t)(b - a) * o0.levels);
+            const fast_div f0 = fast_div::make((uint32_t)o0.levels);
+            for (uint32_t e0 = 0; e0 < n; e0 += gc)
+            {
+                gtile t{};
+                t.e0 = e0, t.count = std::min(gc, n - e0);
+                t.o0 = o0.s_ls;
+                t.img[0].t0 = o0.d_ls;
+                t.n0 = f0.d, t.m0 = f0.m, t.l0 = (uint8_t)f0.l;
+                t.n1 = 1, t.m1 = 1, t.l1 = 0;
+                t.esize = (uint8_t)o0.esize;
+                t.nimg = (uint8_t)o0.nimg;
+                t.kind = 1;
+                t.col0 = col0;
+                t.cls = (uint8_t)class_of_g(t);
+                plan.gt.push_back(t);
+            }
+            a = b;
+        }
     }
 
-    // ---- phased adjoint kernels (boxes without a gather form, lists)
+    // ---- phased adjoint kernels (boxes without a gather form, lists without one)
     auto box_rows = [&](int i) { return (int64_t)plan.boxes[i].n1 * plan.boxes[i].n2; };
     auto box_len = [&](int i) { return std::max<int64_t>(1, 4096 / plan.boxes[i].n0); };
     auto list_len = [&](const list_desc& l) { return std::max<int64_t>(1, 4096 / l.levels); };
@@ -1238,7 +1365,8 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
     int nph = 0;
     if (!plan.gather_ok)
         for (int p : plan.box_phase) nph = std::max(nph, p + 1);
-    for (int p : plan.list_phase) nph = std::max(nph, p + 1);
+    if (!plan.list_gather_ok)
+        for (int p : plan.list_phase) nph = std::max(nph, p + 1);
     for (int ph = 0; ph < nph; ++ph)
     {
         int begin = (int)plan.adj_btiles.size();
@@ -1247,8 +1375,9 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
                 if (plan.box_phase[i] == ph) split(i, 0, box_rows(i), box_len(i), plan.adj_btiles);
         plan.adj_bphase_range.push_back({begin, (int)plan.adj_btiles.size() - begin});
         begin = (int)plan.adj_ltiles.size();
-        for (int i = 0; i < (int)plan.adj_lists.size(); ++i)
-            if (plan.list_phase[i] == ph) split(i, 1, plan.adj_lists[i].count, list_len(plan.adj_lists[i]), plan.adj_ltiles);
+        if (!plan.list_gather_ok)
+            for (int i = 0; i < (int)plan.adj_lists.size(); ++i)
+                if (plan.list_phase[i] == ph) split(i, 1, plan.adj_lists[i].count, list_len(plan.adj_lists[i]), plan.adj_ltiles);
         plan.adj_lphase_range.push_back({begin, (int)plan.adj_ltiles.size() - begin});
     }
 }
@@ -1310,8 +1439,8 @@ void graph_launch_plan(ghexb_plan_s& plan, cudaStream_t stream)
 void adjoint_plan(ghexb_plan_s& plan, cudaStream_t stream)
 {
     if (!plan.adjoint_ok) throw error(GHEXB_ERR_INVALID, plan.adjoint_reason);
-    if (plan.gather_ok && !plan.gt.empty())
-        check_cuda(launch_gather(plan.d_gt, (int)plan.gt.size(), stream), "adjoint kernel launch");
+    if (!plan.gt.empty())
+        check_cuda(launch_gather(plan.d_gt, (int)plan.gt.size(), plan.d_lcols, stream), "adjoint kernel launch");
     const int sms = plan.ctx ? plan.ctx->num_sms : 148;
     auto grid = [&](int n) { return std::min(n, 4 * sms); };
     for (size_t ph = 0; ph < plan.adj_bphase_range.size(); ++ph)
@@ -1367,6 +1496,7 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
     copy_async(plan.d_xp, plan.xp, stream);
     copy_async(plan.d_xb, plan.xb, stream);
     copy_async(plan.d_gt, plan.gt, stream);
+    copy_async(plan.d_lcols, plan.lcols, stream);
     auto put = [&](void* dst, const void* src, size_t bytes) {
         if (bytes) check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync(rebind)");
     };
@@ -1449,7 +1579,7 @@ ghexb_plan_s::~ghexb_plan_s()
     ghexb::release_graph(*this);
     if (cap_stream) cudaStreamDestroy(cap_stream);
     for (void* p : {(void*)d_boxes, (void*)d_lists, (void*)d_adj_lists, (void*)d_idx, (void*)d_xf, (void*)d_xp,
-             (void*)d_xb, (void*)d_gt, (void*)d_adj_btiles, (void*)d_adj_ltiles, (void*)d_counters})
+             (void*)d_xb, (void*)d_gt, (void*)d_lcols, (void*)d_adj_btiles, (void*)d_adj_ltiles, (void*)d_counters})
         if (p) cudaFree(p);
 }
 
@@ -1462,7 +1592,7 @@ int64_t ghexb_plan_s::num_tiles() const
 
 int ghexb_plan_s::adjoint_launches() const
 {
-    int n = gather_ok && !gt.empty() ? 1 : 0;
+    int n = gt.empty() ? 0 : 1;
     for (size_t ph = 0; ph < adj_bphase_range.size(); ++ph)
         n += (adj_bphase_range[ph].second > 0) + (adj_lphase_range[ph].second > 0);
     return n;

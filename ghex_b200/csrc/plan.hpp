@@ -32,10 +32,9 @@ struct ghexb_plan_s
     std::vector<int64_t> adj_src_off, adj_dst_off;
     int n_logical = 0;
 
-    // Forward work (exchange.cu): a CTA runs k_unit_tiles consecutive tiles of one element
-    // class. xf is the batched form's table (by class, the most expensive tiles first within a
-    // class), xp the per-field form's (grouped by logical field, then class) and xb the per-box
-    // form's (grouped by descriptor); each launch range is padded per class with empty tiles.
+    // Forward work (exchange.cu), one CTA per tile: xf is the batched form's table (the most
+    // DRAM bytes per element first), xp the per-field form's (grouped by logical field) and xb
+    // the per-box form's (grouped by descriptor).
     std::vector<ghexb::xtile> xf, xp, xb;
     // x-face boxes whose rows interleave (A's row r ends where B's row r + 1 begins): the
     // batched and per-field tables move each pair as one set of contiguous segments
@@ -49,6 +48,20 @@ struct ghexb_plan_s
     bool gather_ok = false;
     std::string gather_reason;
     std::vector<ghexb::gcell> cells;
+    // Unstructured adjoint in gather form (list_gather_ok), else by phases: every owner column
+    // with its ordered image columns, grouped by (element size, images, levels, level strides).
+    struct list_owner
+    {
+        int slot;
+        int64_t off; // byte offset of the owner column from its field's data
+        int32_t levels, s_ls, d_ls;
+        int esize, nimg;
+        int img_slot[ghexb::k_max_images];
+        int64_t img_off[ghexb::k_max_images];
+    };
+    bool list_gather_ok = false;
+    std::vector<list_owner> lowners;
+    std::vector<uint64_t> lcols; // column table of the owner groups (addresses of the columns)
     std::vector<ghexb::gtile> gt;
     // adjoint tiles of the phased kernels (boxes when !gather_ok, lists) grouped by phase
     std::vector<ghexb::tile> adj_btiles, adj_ltiles;
@@ -64,7 +77,8 @@ struct ghexb_plan_s
     ghexb::xtile* d_xp = nullptr;
     ghexb::xtile* d_xb = nullptr;
     ghexb::gtile* d_gt = nullptr;
-    size_t cap_xf = 0, cap_xp = 0, cap_xb = 0, cap_gt = 0; // elements allocated behind the tables
+    uint64_t* d_lcols = nullptr;
+    size_t cap_xf = 0, cap_xp = 0, cap_xb = 0, cap_gt = 0, cap_lcols = 0; // elements allocated behind the tables
     ghexb::tile* d_adj_btiles = nullptr;
     ghexb::tile* d_adj_ltiles = nullptr;
     unsigned* d_counters = nullptr; // tile scheduler counters of the phased adjoint kernels
