@@ -13,7 +13,9 @@ value        effective GB/s of the batched, graph-captured exchange (algorithmic
              starts with a cold L2 (a read of an unrelated buffer of twice the L2 size runs before
              it, outside its events)
 e2e          the same metric through the public API (co.exchange(...).wait()) with the fields in
-             pinned host memory: host->device copy of every field, exchange, device->host copy
+             pinned host memory: host->device copy of every field, exchange, device->host copy of
+             every field, every step (consecutive steps on two device copies and two streams, so
+             that the two copy directions overlap)
 roofline     achieved GB/s of the exchange kernel (the only kernel of the batched form) against the
              measured HBM copy bandwidth; traffic = DRAM bytes per launch from an ncu capture
 cpu_baseline GHEX's own CPU exchange (single rank holding every domain, built from the reference
@@ -158,6 +160,7 @@ class Case:
         self.kind = {"cfg2": "unstructured", "cfg3": "cubed_sphere"}.get(cfg, "regular")
         self.fields = []
         self.bis = []
+        self.wrappers = []  # per field: device tensors of every domain -> their buffer_infos
         if self.kind == "regular":
             from ghex_b200.structured import regular as R
             self.api = R
@@ -171,8 +174,11 @@ class Case:
                     host = [w.domain_array(d, s) for d in w.domains]
                     tens = [torch.from_numpy(a).to(dev) for a in host]
                     self.fields.append((s.name, host, tens, None))
-                    self.bis += [pat(R.make_field_descriptor(dm, t, w.offsets(s), w.extents(d, s)))
-                                 for dm, d, t in zip(doms, w.domains, tens)]
+                    wrap = (lambda ts, pat=pat, doms=doms, s=s: [
+                        pat(R.make_field_descriptor(dm, t, w.offsets(s), w.extents(d, s)))
+                        for dm, d, t in zip(doms, w.domains, ts)])
+                    self.wrappers.append(wrap)
+                    self.bis += wrap(tens)
             names = sorted({np.dtype(s.dtype).name for s in w.fields}, reverse=True)
             self.dtype = "+".join(n.replace("float", "f") for n in names)
         elif self.kind == "cubed_sphere":
@@ -186,8 +192,11 @@ class Case:
                 host = [w.domain_array(d, nc, seed) for d in w.domains]
                 tens = [torch.from_numpy(a).to(dev) for a in host]
                 self.fields.append((name, host, tens, (nc, vec)))
-                self.bis += [pat(C.make_field_descriptor(d, t, w.offsets(), a.shape[:3], nc, vec))
-                             for d, t, a in zip(doms, tens, host)]
+                wrap = (lambda ts, host=host, nc=nc, vec=vec: [
+                    pat(C.make_field_descriptor(d, t, w.offsets(), a.shape[:3], nc, vec))
+                    for d, t, a in zip(doms, ts, host)])
+                self.wrappers.append(wrap)
+                self.bis += wrap(tens)
             self.dtype = "f64"
         else:
             from ghex_b200 import unstructured as U
@@ -199,7 +208,9 @@ class Case:
                 host = [w.domain_array(d, dt, seed) for d in w.domains]
                 tens = [torch.from_numpy(a).to(dev) for a in host]
                 self.fields.append((name, host, tens, None))
-                self.bis += [pat(U.make_field_descriptor(d, t)) for d, t in zip(doms, tens)]
+                wrap = lambda ts: [pat(U.make_field_descriptor(d, t)) for d, t in zip(doms, ts)]
+                self.wrappers.append(wrap)
+                self.bis += wrap(tens)
             self.dtype = "f64+f32"
         for _, host, tens, _ in self.fields:
             for a, t in zip(host, tens):
@@ -327,7 +338,14 @@ def run_reference(args):
         return
     import multiprocessing as mp
     cfg = args.config if args.config in ("cfg0", "cfg1", "cfg4") else "cfg1"
-    procs = max(1, min(os.cpu_count() or 1, 32))
+    # one process per host core, each holding its own copy of the workload (about 0.5 GB for the
+    # 400x300x96 case), as many as the free host memory allows
+    procs = max(1, os.cpu_count() or 1)
+    try:
+        import psutil
+        procs = max(1, min(procs, int(psutil.virtual_memory().available / (1.5 * 2**30))))
+    except Exception:
+        pass
     # every process exchanges its own copy; bounded to about a minute in all
     iters = max(2, min(200, (args.steps + procs - 1) // procs))
     ctx = mp.get_context("spawn")
@@ -404,28 +422,47 @@ class Timer:
 
 
 def e2e_ms(case, stream, steps, world, dev):
-    """Public API end to end: pinned host fields -> device, co.exchange(...).wait(), device -> host."""
+    """Public API end to end, every step: pinned host fields -> device, co.exchange(...).wait(),
+    device -> host. Consecutive steps alternate between two device copies of the fields (and two
+    communication objects) on two streams, so that a step's device -> host copy runs on one copy
+    engine while the next step's host -> device copy runs on the other."""
     import torch
-    co = case.api.make_communication_object(case.ctx)
     pinned = [[torch.from_numpy(a).pin_memory() for a in f[1]] for f in case.fields]
     outs = [[torch.empty_like(p).pin_memory() for p in ps] for ps in pinned]
     h2d = sum(p.numel() * p.element_size() for ps in pinned for p in ps)
-    with torch.cuda.stream(stream):
-        for it in range(steps + 2):
-            if it == 2:
-                torch.cuda.synchronize()
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-            for f, ps in zip(case.fields, pinned):
-                for t, p in zip(f[2], ps):
+    sets = []
+    for k in range(2):
+        tens = [f[2] for f in case.fields] if k == 0 else [[torch.empty_like(t) for t in f[2]] for f in case.fields]
+        bis = [bi for wrap, ts in zip(case.wrappers, tens) for bi in wrap(ts)]
+        sets.append((tens, bis, case.api.make_communication_object(case.ctx),
+                     stream if k == 0 else torch.cuda.Stream(device=dev)))
+
+    def step(it):
+        tens, bis, co, s = sets[it % 2]
+        with torch.cuda.stream(s):
+            for ts, ps in zip(tens, pinned):
+                for t, p in zip(ts, ps):
                     t.copy_(p, non_blocking=True)
-            co.exchange(case.bis).wait()
-            for f, os_ in zip(case.fields, outs):
-                for t, o in zip(f[2], os_):
+            co.exchange(bis).wait()
+            for ts, os_ in zip(tens, outs):
+                for t, o in zip(ts, os_):
                     o.copy_(t, non_blocking=True)
-        e1.record(stream)
-        torch.cuda.synchronize()
+
+    for it in range(2):
+        step(it)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(sets[0][3])
+    sets[1][3].wait_event(e0)
+    for it in range(steps):
+        step(it)
+    last, other = sets[(steps - 1) % 2][3], sets[steps % 2][3]
+    done = torch.cuda.Event()
+    done.record(other)
+    last.wait_event(done)  # e1 follows the work of both streams
+    e1.record(last)
+    torch.cuda.synchronize()
     return max_over_ranks(e0.elapsed_time(e1) / steps, world, dev), h2d
 
 
