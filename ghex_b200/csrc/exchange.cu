@@ -44,6 +44,17 @@ template<> struct sign_bit<unsigned long long>
 };
 
 template<typename T> __device__ __forceinline__ T ld_stream(const T* p) { return __ldcg(p); }
+// Stores through st.global: the compiler then knows that they cannot alias the tile record in
+// shared memory and keeps the record's fields in registers across them.
+template<typename T> __device__ __forceinline__ void st_global(T* p, T v) { __stcg(p, v); }
+template<> __device__ __forceinline__ void st_global(uint16_t* p, uint16_t v)
+{
+    __stcg(reinterpret_cast<unsigned short*>(p), (unsigned short)v);
+}
+template<> __device__ __forceinline__ void st_global(uint8_t* p, uint8_t v)
+{
+    __stcg(reinterpret_cast<unsigned char*>(p), (unsigned char)v);
+}
 template<> __device__ __forceinline__ uint16_t ld_stream(const uint16_t* p)
 {
     return __ldcg(reinterpret_cast<const unsigned short*>(p));
@@ -90,9 +101,9 @@ __device__ __forceinline__ void box_elements(const xtile& t)
     for (int k = 0; k < K; ++k)
         if (k * blockDim.x + threadIdx.x < t.count)
         {
-            if constexpr (NEG) dst[doff[k]] = v[k] ^ sign_bit<T>::v;
+            if constexpr (NEG) st_global(dst + doff[k], (T)(v[k] ^ sign_bit<T>::v));
             else
-                dst[doff[k]] = v[k];
+                st_global(dst + doff[k], v[k]);
         }
 }
 
@@ -123,7 +134,7 @@ __device__ __forceinline__ void list_elements(const xtile& t)
         if (k * blockDim.x + threadIdx.x < t.count) v[k] = ld_stream(src + so[k]);
 #pragma unroll
     for (int k = 0; k < K; ++k)
-        if (k * blockDim.x + threadIdx.x < t.count) dst[doff[k]] = v[k];
+        if (k * blockDim.x + threadIdx.x < t.count) st_global(dst + doff[k], v[k]);
 }
 
 // Pairs of x-face boxes: a segment of na + nb destination elements is contiguous, so the warp's
@@ -163,7 +174,7 @@ __device__ __forceinline__ void pair_elements(const xtile& t)
     }
 #pragma unroll
     for (int k = 0; k < K; ++k)
-        if (ok[k]) dst[doff[k]] = v[k];
+        if (ok[k]) st_global(dst + doff[k], v[k]);
 }
 
 template<int K>
@@ -234,9 +245,9 @@ __device__ __forceinline__ void gather_elements(const gtile& t)
             for (int i = 0; i < NI; ++i)
             {
                 a = t.img[i].neg ? a - h[k][i] : a + h[k][i];
-                reinterpret_cast<F*>(t.img[i].ptr)[hoff[k][i]] = F(0);
+                st_global(reinterpret_cast<F*>(t.img[i].ptr) + hoff[k][i], F(0));
             }
-            own[ooff[k]] = a;
+            st_global(own + ooff[k], a);
         }
 }
 
@@ -276,9 +287,9 @@ __device__ __forceinline__ void list_gather_elements(const gtile& t, const uint6
             for (int i = 0; i < NI; ++i)
             {
                 a = a + h[k][i];
-                *img[k][i] = F(0);
+                st_global(img[k][i], F(0));
             }
-            *own[k] = a;
+            st_global(own[k], a);
         }
 }
 
