@@ -293,7 +293,31 @@ __device__ __forceinline__ void list_gather_elements(const gtile& t, const uint6
         }
 }
 
-__global__ void __launch_bounds__(k_gather_block, 3) gather_kernel(const gtile* __restrict__ tiles,
+__global__ void __launch_bounds__(k_gather_block, 3) gather_kernel(const gtile* __restrict__ tiles)
+{
+    __shared__ gtile t;
+    load_record<16>(t, tiles);
+    switch (t.cls)
+    {
+#define GHEXB_CASE(NI)                                                                                                 \
+    case gather_class(8, NI): gather_elements<gather_per_thread(NI), NI, double>(t); break;                          \
+    case gather_class(4, NI): gather_elements<gather_per_thread(NI), NI, float>(t); break;
+        GHEXB_CASE(1)
+        GHEXB_CASE(2)
+        GHEXB_CASE(3)
+        GHEXB_CASE(4)
+        GHEXB_CASE(5)
+        GHEXB_CASE(6)
+        GHEXB_CASE(7)
+        GHEXB_CASE(8)
+#undef GHEXB_CASE
+        default: break;
+    }
+}
+
+// The unstructured owner groups have a kernel of their own, so that the box kernel's code (and
+// its instruction-cache footprint) stays that of the box classes.
+__global__ void __launch_bounds__(k_gather_block, 3) list_gather_kernel(const gtile* __restrict__ tiles,
     const uint64_t* __restrict__ cols)
 {
     __shared__ gtile t;
@@ -301,18 +325,8 @@ __global__ void __launch_bounds__(k_gather_block, 3) gather_kernel(const gtile* 
     switch (t.cls)
     {
 #define GHEXB_CASE(NI)                                                                                                 \
-    case gather_class(8, NI):                                                                                          \
-        gather_elements<gather_per_thread(NI), NI, double>(t);                                                        \
-        break;                                                                                                         \
-    case gather_class(4, NI):                                                                                          \
-        gather_elements<gather_per_thread(NI), NI, float>(t);                                                         \
-        break;                                                                                                         \
-    case list_gather_class(8, NI):                                                                                     \
-        list_gather_elements<gather_per_thread(NI), NI, double>(t, cols);                                             \
-        break;                                                                                                         \
-    case list_gather_class(4, NI):                                                                                     \
-        list_gather_elements<gather_per_thread(NI), NI, float>(t, cols);                                              \
-        break;
+    case list_gather_class(8, NI): list_gather_elements<gather_per_thread(NI), NI, double>(t, cols); break;          \
+    case list_gather_class(4, NI): list_gather_elements<gather_per_thread(NI), NI, float>(t, cols); break;
         GHEXB_CASE(1)
         GHEXB_CASE(2)
         GHEXB_CASE(3)
@@ -343,10 +357,17 @@ cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cu
     return cudaGetLastError();
 }
 
-cudaError_t launch_gather(const gtile* tiles, int ntiles, const uint64_t* cols, cudaStream_t stream)
+cudaError_t launch_gather(const gtile* tiles, int ntiles, cudaStream_t stream)
 {
     if (ntiles <= 0) return cudaSuccess;
-    gather_kernel<<<ntiles, k_gather_block, 0, stream>>>(tiles, cols);
+    gather_kernel<<<ntiles, k_gather_block, 0, stream>>>(tiles);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_list_gather(const gtile* tiles, int ntiles, const uint64_t* cols, cudaStream_t stream)
+{
+    if (ntiles <= 0) return cudaSuccess;
+    list_gather_kernel<<<ntiles, k_gather_block, 0, stream>>>(tiles, cols);
     return cudaGetLastError();
 }
 } // namespace ghexb

@@ -68,7 +68,8 @@ constexpr int k_gather_classes = 4 * k_max_images;
 // forward_per_thread(k, unit) * block elements; k is 4, 8 or 16.
 cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cudaStream_t stream);
 // Adjoint in gather form of tiles[0, ntiles), one CTA per tile: a tile holds at most
-// gather_per_thread(nimg) * k_gather_block elements; `cols` is the column table of the
-// unstructured owner groups (may be null without them).
-cudaError_t launch_gather(const gtile* tiles, int ntiles, const uint64_t* cols, cudaStream_t stream);
+// gather_per_thread(nimg) * k_gather_block elements. launch_gather takes box cells,
+// launch_list_gather unstructured owner groups with `cols`, their column table.
+cudaError_t launch_gather(const gtile* tiles, int ntiles, cudaStream_t stream);
+cudaError_t launch_list_gather(const gtile* tiles, int ntiles, const uint64_t* cols, cudaStream_t stream);
 } // namespace ghexb

@@ -534,8 +534,6 @@ bool build_cells(ghexb_plan_s& plan, std::string& why)
             }
         }
     }
-    // cells with the most images first: the longest CTAs start in the first wave
-    std::stable_sort(plan.cells.begin(), plan.cells.end(), [](const gcell& a, const gcell& b) { return a.nimg > b.nimg; });
     return true;
 }
 
@@ -828,9 +826,23 @@ double run_cost(int64_t count, int unit, int64_t row)
     return (double)count * unit * (w + 32.0) / w;
 }
 
-double tile_cost(const xtile& t) { return run_cost(t.count, t.unit, t.n0); }
+// A forward tile's rows run along its first axis where source and destination are both
+// contiguous along it (pairs: segments of n0 elements); otherwise every element is a row.
+double tile_cost(const xtile& t)
+{
+    auto unit_stride = [](int32_t v) { return v == 1 || v == -1; };
+    const bool contiguous = t.kind == 2 || (t.kind == 0 ? unit_stride(t.s0) && unit_stride(t.d0) : t.s1 == 1 && t.d1 == 1);
+    return run_cost(t.count, t.unit, contiguous ? t.n0 : 1);
+}
 
-double tile_cost(const gtile& t) { return run_cost(t.count, t.esize, t.n0) * 2.0 * (1 + t.nimg); }
+// A gather tile's accesses are rows along its first axis only where the owner and every image
+// are contiguous along it; otherwise every element is a row of its own.
+double tile_cost(const gtile& t)
+{
+    bool contiguous = t.o0 == 1;
+    for (int i = 0; i < t.nimg && contiguous; ++i) contiguous = t.kind ? t.img[0].t0 == 1 : (t.img[i].t0 == 1 || t.img[i].t0 == -1);
+    return run_cost(t.count, t.esize, contiguous ? t.n0 : 1) * 2.0 * (1 + t.nimg);
+}
 
 // Appends the tiles of one launch range; returns [begin, count) in out.
 template<typename R>
@@ -1307,8 +1319,11 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
                 all.push_back(t);
             }
         }
+        // the most expensive tiles (most bytes, short rows) first: the first wave starts on them
+        std::stable_sort(all.begin(), all.end(), [](const gtile& a, const gtile& b) { return tile_cost(a) > tile_cost(b); });
         append_range(plan.gt, all);
     }
+    plan.gt_boxes = (int)plan.gt.size();
     // ---- unstructured adjoint, gather form: owner groups and their column table
     plan.lcols.clear();
     if (plan.list_gather_ok)
@@ -1386,6 +1401,8 @@ void release_graph(ghexb_plan_s& plan)
 {
     if (plan.exec) cudaGraphExecDestroy(plan.exec), plan.exec = nullptr;
     if (plan.graph) cudaGraphDestroy(plan.graph), plan.graph = nullptr;
+    if (plan.adj_exec) cudaGraphExecDestroy(plan.adj_exec), plan.adj_exec = nullptr;
+    if (plan.adj_graph) cudaGraphDestroy(plan.adj_graph), plan.adj_graph = nullptr;
 }
 
 void launch_plan(ghexb_plan_s& plan, int form, cudaStream_t stream)
@@ -1436,11 +1453,14 @@ void graph_launch_plan(ghexb_plan_s& plan, cudaStream_t stream)
     check_cuda(cudaGraphLaunch(plan.exec, stream), "cudaGraphLaunch");
 }
 
-void adjoint_plan(ghexb_plan_s& plan, cudaStream_t stream)
+namespace
 {
-    if (!plan.adjoint_ok) throw error(GHEXB_ERR_INVALID, plan.adjoint_reason);
-    if (!plan.gt.empty())
-        check_cuda(launch_gather(plan.d_gt, (int)plan.gt.size(), plan.d_lcols, stream), "adjoint kernel launch");
+// Launches of one adjoint: the gather kernels, then the phases of what has no gather form.
+void adjoint_launches(ghexb_plan_s& plan, cudaStream_t stream)
+{
+    check_cuda(launch_gather(plan.d_gt, plan.gt_boxes, stream), "adjoint kernel launch");
+    check_cuda(launch_list_gather(plan.d_gt + plan.gt_boxes, (int)plan.gt.size() - plan.gt_boxes, plan.d_lcols, stream),
+        "adjoint kernel launch");
     const int sms = plan.ctx ? plan.ctx->num_sms : 148;
     auto grid = [&](int n) { return std::min(n, 4 * sms); };
     for (size_t ph = 0; ph < plan.adj_bphase_range.size(); ++ph)
@@ -1456,6 +1476,36 @@ void adjoint_plan(ghexb_plan_s& plan, cudaStream_t stream)
                            grid(rl.second), 256, stream),
                 "adjoint kernel launch");
     }
+}
+} // namespace
+
+void adjoint_plan(ghexb_plan_s& plan, cudaStream_t stream)
+{
+    if (!plan.adjoint_ok) throw error(GHEXB_ERR_INVALID, plan.adjoint_reason);
+    if (!plan.adj_exec)
+    {
+        check_cuda(cudaStreamBeginCapture(plan.cap_stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+        std::string err;
+        try
+        {
+            adjoint_launches(plan, plan.cap_stream);
+        }
+        catch (const error& e)
+        {
+            err = e.what();
+        }
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(plan.cap_stream, &g);
+        if (!err.empty())
+        {
+            if (g) cudaGraphDestroy(g);
+            throw error(GHEXB_ERR_CUDA, err);
+        }
+        check_cuda(ce, "cudaStreamEndCapture");
+        plan.adj_graph = g;
+        check_cuda(cudaGraphInstantiate(&plan.adj_exec, plan.adj_graph, 0), "cudaGraphInstantiate");
+    }
+    check_cuda(cudaGraphLaunch(plan.adj_exec, stream), "cudaGraphLaunch");
 }
 
 void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stream)
@@ -1592,7 +1642,7 @@ int64_t ghexb_plan_s::num_tiles() const
 
 int ghexb_plan_s::adjoint_launches() const
 {
-    int n = gt.empty() ? 0 : 1;
+    int n = (gt_boxes > 0) + ((int)gt.size() > gt_boxes);
     for (size_t ph = 0; ph < adj_bphase_range.size(); ++ph)
         n += (adj_bphase_range[ph].second > 0) + (adj_lphase_range[ph].second > 0);
     return n;

@@ -62,7 +62,8 @@ struct ghexb_plan_s
     bool list_gather_ok = false;
     std::vector<list_owner> lowners;
     std::vector<uint64_t> lcols; // column table of the owner groups (addresses of the columns)
-    std::vector<ghexb::gtile> gt;
+    std::vector<ghexb::gtile> gt; // box cells first (gt_boxes of them), then unstructured owner groups
+    int gt_boxes = 0;
     // adjoint tiles of the phased kernels (boxes when !gather_ok, lists) grouped by phase
     std::vector<ghexb::tile> adj_btiles, adj_ltiles;
     std::vector<std::pair<int, int>> adj_bphase_range, adj_lphase_range;
@@ -98,10 +99,12 @@ struct ghexb_plan_s
     int block = 256;
     bool use_pairs = true; // batched and per-field tables move x-face pairs as segments
 
-    // graph of the batched form
+    // graphs of the batched form and of the adjoint, captured on first use
     cudaStream_t cap_stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    cudaGraph_t adj_graph = nullptr;
+    cudaGraphExec_t adj_exec = nullptr;
 
     ~ghexb_plan_s();
 };
