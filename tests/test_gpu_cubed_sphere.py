@@ -84,3 +84,34 @@ def test_cubed_adjoint_bitexact(cuda):
     odoms = [O.Domain(t, (x0, x1), (y0, y1), w.levels) for t, x0, x1, y0, y1 in w.domains]
     O.adjoint(O.make_pattern(w.edge, (w.halo,) * 4, odoms), odoms, grads, [w.offsets()] * len(odoms), w.edge, True)
     assert sum(bits_equal(t.cpu().numpy(), g) for t, g in zip(ts, grads)) == 0
+
+
+@pytest.mark.parametrize("tuning", [(4, 128), (8, 256), (16, 512)])
+def test_every_form_and_tuning(cuda, tuning):
+    """Every launch form at several tunings (including the edges whose transform swaps x and y)
+    bit-exact against the oracle."""
+    w = W.config3(edge=48, levels=8, split=2)
+    s_host = [w.domain_array(d, 1, 1) for d in w.domains]
+    v_host = [w.domain_array(d, 2, 2) for d in w.domains]
+    ctx = C.make_context()
+    cube = C.cube(w.edge, w.levels)
+    doms = [C.DomainDescriptor(cube, *b) for b in w.domains]
+    pat = C.make_pattern(ctx, C.HaloGenerator(w.halo), doms)
+    ts = [to_device(a, cuda) for a in s_host]
+    tv = [to_device(a, cuda) for a in v_host]
+    bis = [pat(C.make_field_descriptor(d, t, w.offsets(), a.shape[:3], 1, False)) for d, t, a in zip(doms, ts, s_host)]
+    bis += [pat(C.make_field_descriptor(d, t, w.offsets(), a.shape[:3], 2, True)) for d, t, a in zip(doms, tv, v_host)]
+    plan = C.make_exchange_plan(ctx, bis)
+    plan.set_tuning(*tuning)
+    odoms = [O.Domain(t, (x0, x1), (y0, y1), w.levels) for t, x0, x1, y0, y1 in w.domains]
+    opat = O.make_pattern(w.edge, (w.halo,) * 4, odoms)
+    es = [a.copy(order="K") for a in s_host]
+    ev = [a.copy(order="K") for a in v_host]
+    O.exchange(opat, odoms, es, [w.offsets()] * len(odoms), w.edge, False)
+    O.exchange(opat, odoms, ev, [w.offsets()] * len(odoms), w.edge, True)
+    for form in (plan.BATCHED, plan.PER_FIELD, plan.PER_BOX):
+        for t, a in zip(ts + tv, s_host + v_host):
+            t.copy_(torch.from_numpy(a))
+        plan.launch(form)
+        torch.cuda.synchronize()
+        assert sum(bits_equal(t.cpu().numpy(), e) for t, e in zip(ts + tv, es + ev)) == 0
