@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4"], default="cfg1")
+    ap.add_argument("--config", choices=["cfg0", "cfg1", "cfg2", "cfg2_ipr", "cfg3", "cfg4"], default="cfg1")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-configs", action="store_true", help="skip the other workloads")
@@ -145,6 +145,8 @@ class ClockSampler:
 # ------------------------------------------------------------------------------------------
 def workload(cfg: str):
     from ghex_b200 import workloads as W
+    if cfg == "cfg2_ipr":
+        return W.config2(halo_by_owner=True)
     return {"cfg0": W.config0, "cfg1": W.config1, "cfg2": W.config2, "cfg3": W.config3, "cfg4": W.config4}[cfg]()
 
 
@@ -157,7 +159,8 @@ class Case:
         import torch
         self.cfg = cfg
         self.w = w = workload(cfg)
-        self.kind = {"cfg2": "unstructured", "cfg3": "cubed_sphere"}.get(cfg, "regular")
+        self.kind = {"cfg2": "unstructured", "cfg2_ipr": "unstructured", "cfg3": "cubed_sphere"}.get(cfg, "regular")
+        self.in_place = cfg == "cfg2_ipr"  # unstructured in-place receive
         self.fields = []
         self.bis = []
         self.wrappers = []  # per field: device tensors of every domain -> their buffer_infos
@@ -215,7 +218,7 @@ class Case:
         for _, host, tens, _ in self.fields:
             for a, t in zip(host, tens):
                 assert t.stride() == torch.from_numpy(a).stride()
-        self.plan = self.api.make_exchange_plan(self.ctx, self.bis)
+        self.plan = self.api.make_exchange_plan(self.ctx, self.bis, in_place_receive=self.in_place)
         self.alg = self.plan.info()["algorithmic_bytes"]
 
     def reset(self):
@@ -242,6 +245,8 @@ class Case:
             elif self.kind == "cubed_sphere":
                 fl = [(f[3][0], f[3][1], w.offsets(), arrs) for f, arrs in zip(self.fields, arrays)]
                 sec = reflib.cubed_exchange(w.edge, w.levels, (w.halo,) * 4, w.domains, fl, iterations)
+            elif self.in_place:  # one communication_object_ipr per domain and field
+                sec = sum(reflib.unstructured_exchange_ipr(w.domains, w.levels, arrs, iterations) for arrs in arrays)
             else:
                 sec = reflib.unstructured_exchange(w.domains, [(w.levels, True, arrs) for arrs in arrays], iterations)
             return sec, arrays, "reference"
@@ -273,7 +278,10 @@ class Case:
             doms = [O.Domain(*d) for d in w.domains]
             recv, send, _ = O.make_pattern(doms)
             for arrs in arrays:
-                O.exchange(recv, send, arrs)
+                if self.in_place:
+                    O.exchange_in_place(recv, send, arrs, doms)
+                else:
+                    O.exchange(recv, send, arrs)
 
     def mismatches(self, expected) -> int:
         bad = 0
@@ -486,7 +494,7 @@ def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline
     if baseline:
         case.reset()
         plan.launch(plan.BATCHED, s)
-        sec, expected, kind = case.reference(1 if cfg in ("cfg2", "cfg3") else 3)
+        sec, expected, kind = case.reference(1 if cfg in ("cfg2", "cfg2_ipr", "cfg3") else 3)
         out["bitexact"] = case.mismatches(expected) == 0
         out["cpu_baseline"] = {"value": case.alg / sec / 1e9, "unit": "GB/s", "cores": 1, "kind": kind, "ms": sec * 1e3}
     return out
@@ -620,7 +628,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_configs:
         del case
         line["configs"] = {}
-        for cfg in ("cfg2", "cfg3", "cfg4"):
+        for cfg in ("cfg2", "cfg2_ipr", "cfg3", "cfg4"):
             if cfg != args.config:
                 line["configs"][cfg] = measure_config(cfg, dev, timer, peak, min(args.steps, 200), max(3, args.warmup),
                                                       not args.no_autotune, not args.no_baseline)

@@ -94,12 +94,14 @@ SIGNATURES = {
     "ghexb_field_wrap_unstructured": [_vp, _i64, _i, _vp, _i64, _i, _i64, C.POINTER(_vp)],
     "ghexb_field_destroy": [_vp],
     "ghexb_co_create": [_vp, C.POINTER(_vp)],
+    "ghexb_co_create_ipr": [_vp, C.POINTER(_vp)],
     "ghexb_co_destroy": [_vp],
     "ghexb_co_exchange": [_vp, C.POINTER(_vp), _i, _vp, C.POINTER(_vp)],
     "ghexb_handle_wait": [_vp],
     "ghexb_handle_is_ready": [_vp, _pi],
     "ghexb_handle_destroy": [_vp],
     "ghexb_plan_create": [_vp, C.POINTER(_vp), _i, C.POINTER(_vp)],
+    "ghexb_plan_create_ipr": [_vp, C.POINTER(_vp), _i, C.POINTER(_vp)],
     "ghexb_plan_destroy": [_vp],
     "ghexb_plan_check": [_vp, C.POINTER(_vp), _i, _pi64],
     "ghexb_plan_get_info": [_vp, C.POINTER(PlanInfo)],

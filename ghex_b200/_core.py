@@ -289,10 +289,10 @@ class CommunicationObject:
     exchange again before wait() raises "earlier exchange operation was not finished".
     """
 
-    def __init__(self, ctx: context):
+    def __init__(self, ctx: context, in_place_receive: bool = False):
         self.context = ctx
         h = C.c_void_p()
-        call("ghexb_co_create", ctx._h, C.byref(h))
+        call("ghexb_co_create_ipr" if in_place_receive else "ghexb_co_create", ctx._h, C.byref(h))
         self._h = h
 
     def exchange(self, *buffer_infos) -> Handle:
@@ -323,7 +323,7 @@ class ExchangePlan:
     PER_FIELD = _capi.FORM_PER_FIELD
     PER_BOX = _capi.FORM_PER_BOX
 
-    def __init__(self, ctx: context, buffer_infos: Sequence[BufferInfo]):
+    def __init__(self, ctx: context, buffer_infos: Sequence[BufferInfo], in_place_receive: bool = False):
         self.context = ctx
         self._bis = _flatten(tuple(buffer_infos))
         self._arrays = [a for bi in self._bis for a in bi.arrays()]
@@ -331,7 +331,8 @@ class ExchangePlan:
         self._bound = tuple(array_info(a)["ptr"] for a in self._arrays)
         handles = (C.c_void_p * len(self._bis))(*[bi.handle() for bi in self._bis])
         h = C.c_void_p()
-        call("ghexb_plan_create", ctx._h, handles, len(self._bis), C.byref(h))
+        call("ghexb_plan_create_ipr" if in_place_receive else "ghexb_plan_create", ctx._h, handles,
+             len(self._bis), C.byref(h))
         self._h = h
 
     def info(self) -> dict:
@@ -394,5 +395,5 @@ class ExchangePlan:
         self._h = None
 
 
-def make_exchange_plan(ctx: context, buffer_infos: Sequence[BufferInfo]) -> ExchangePlan:
-    return ExchangePlan(ctx, buffer_infos)
+def make_exchange_plan(ctx: context, buffer_infos: Sequence[BufferInfo], in_place_receive: bool = False) -> ExchangePlan:
+    return ExchangePlan(ctx, buffer_infos, in_place_receive)

@@ -83,6 +83,7 @@ struct ghexb_co_s
 {
     ghexb_context_s* ctx = nullptr;
     std::map<std::vector<int64_t>, std::unique_ptr<ghexb_plan_s>> plans;
+    bool in_place_receive = false;
     bool busy = false;
     cudaEvent_t done = nullptr;
 
@@ -421,6 +422,17 @@ int ghexb_co_create(ghexb_context ctx, ghexb_co* out)
     });
 }
 
+int ghexb_co_create_ipr(ghexb_context ctx, ghexb_co* out)
+{
+    return guarded([&] {
+        require(ctx && out, "null argument");
+        auto co = std::make_unique<ghexb_co_s>();
+        co->ctx = ctx;
+        co->in_place_receive = true;
+        *out = co.release();
+    });
+}
+
 int ghexb_co_destroy(ghexb_co co)
 {
     if (!co) return GHEXB_OK;
@@ -446,6 +458,7 @@ int ghexb_co_exchange(ghexb_co co, const ghexb_field* fields, int n, void* strea
         {
             if (co->plans.size() >= 64) co->plans.clear();
             auto plan = std::make_unique<ghexb_plan_s>();
+            plan->in_place_receive = co->in_place_receive;
             ghexb::build_plan(*plan, co->ctx, fields, n);
             it = co->plans.emplace(std::move(key), std::move(plan)).first;
         }
@@ -488,6 +501,17 @@ int ghexb_plan_create(ghexb_context ctx, const ghexb_field* fields, int n, ghexb
     return guarded([&] {
         require(ctx && fields && out, "null argument");
         auto plan = std::make_unique<ghexb_plan_s>();
+        ghexb::build_plan(*plan, ctx, fields, n);
+        *out = plan.release();
+    });
+}
+
+int ghexb_plan_create_ipr(ghexb_context ctx, const ghexb_field* fields, int n, ghexb_plan* out)
+{
+    return guarded([&] {
+        require(ctx && fields && out, "null argument");
+        auto plan = std::make_unique<ghexb_plan_s>();
+        plan->in_place_receive = true;
         ghexb::build_plan(*plan, ctx, fields, n);
         *out = plan.release();
     });

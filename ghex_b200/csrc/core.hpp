@@ -85,6 +85,7 @@ struct domain_info
     coord4 last{};
     int tile = 0;     // cubed sphere
     int64_t size = 0; // unstructured: number of local ids
+    std::vector<int64_t> outer; // unstructured: outer (halo) local ids, ascending
     std::vector<struct_entry> recv, send;
     std::vector<list_entry> urecv, usend;
 };

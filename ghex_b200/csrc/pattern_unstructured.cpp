@@ -100,6 +100,8 @@ void build_unstructured(ghexb_pattern_s& p, int n, const int64_t* ids, const int
         }
         p.domains[i].id = d.id;
         p.domains[i].size = (int64_t)d.gids.size();
+        p.domains[i].outer.assign(outer_lids + outer_off[i], outer_lids + outer_off[i + 1]);
+        std::sort(p.domains[i].outer.begin(), p.domains[i].outer.end());
     }
     if (max_id > (int64_t)0x7fffffff) throw error(GHEXB_ERR_INVALID, "domain ids must fit into int");
 

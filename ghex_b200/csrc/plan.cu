@@ -15,6 +15,7 @@
 #include <map>
 #include <tuple>
 #include <unordered_map>
+#include <unordered_set>
 
 #include "exchange.hpp"
 #include "kernels.hpp"
@@ -614,6 +615,32 @@ bool build_list_owners(ghexb_plan_s& plan, std::string& why)
     return true;
 }
 
+// Receive rows of an in-place receive: GHEX receives the message of a neighbour as raw bytes at
+// the address of its first receive index (communication_object_ipr.hpp:127-141), so the k-th
+// value lands on row front + k whatever the receive list says. Those rows must be halo rows of
+// the domain, received once: otherwise the outcome would depend on the order of the copies.
+std::vector<std::vector<int64_t>> in_place_rows(const ghexb_pattern_s& P, int d)
+{
+    const auto& dom = P.domains[d];
+    std::vector<std::vector<int64_t>> rows;
+    std::unordered_set<int64_t> claimed;
+    for (const auto& re : dom.urecv)
+    {
+        std::vector<int64_t> r(re.lids.size());
+        for (size_t k = 0; k < r.size(); ++k)
+        {
+            r[k] = re.lids[0] + (int64_t)k;
+            if (!std::binary_search(dom.outer.begin(), dom.outer.end(), r[k]) || !claimed.insert(r[k]).second)
+                throw error(GHEXB_ERR_INVALID,
+                    "in-place receive: the halo of domain " + std::to_string(dom.id) + " received from domain " +
+                        std::to_string(P.domains[re.neighbor].id) + " is not stored on consecutive halo rows from " +
+                        "local index " + std::to_string(re.lids[0]));
+        }
+        rows.push_back(std::move(r));
+    }
+    return rows;
+}
+
 } // namespace
 
 void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* fields, int n)
@@ -671,10 +698,29 @@ void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* f
                     throw error(GHEXB_ERR_INCOMPATIBLE, "paired fields differ in components");
                 if (a.levels != b.levels) throw error(GHEXB_ERR_INCOMPATIBLE, "paired fields differ in levels");
             };
+            if (plan.in_place_receive && P.kind != pattern_kind::unstructured)
+                throw error(GHEXB_ERR_INVALID, "an in-place receive needs an unstructured pattern");
             if (P.kind == pattern_kind::unstructured)
             {
-                for (const auto& re : P.domains[d].urecv)
+                std::vector<std::vector<int64_t>> placed;
+                if (plan.in_place_receive)
                 {
+                    placed = in_place_rows(P, d);
+                    for (int slot : Fd)
+                    {
+                        const auto& f = plan.fields[slot];
+                        const bool rows = f.levels == 1 ? f.index_stride == 1
+                                                        : f.level_stride == 1 && f.index_stride == f.levels;
+                        if (!rows)
+                            throw error(GHEXB_ERR_INVALID,
+                                "in-place receive needs the levels of a halo element stored contiguously "
+                                "(levels first, rows without padding)");
+                    }
+                }
+                for (size_t ri = 0; ri < P.domains[d].urecv.size(); ++ri)
+                {
+                    const auto& re = P.domains[d].urecv[ri];
+                    const auto& rlids = plan.in_place_receive ? placed[ri] : re.lids;
                     const auto& Fe = partner(re.neighbor);
                     const list_entry* se = nullptr;
                     for (const auto& s : P.domains[re.neighbor].usend)
@@ -685,7 +731,7 @@ void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* f
                         const auto& dst = plan.fields[Fd[k]];
                         const auto& src = plan.fields[Fe[k]];
                         check_pair(dst, src);
-                        B.list_pair(dst, Fd[k], src, Fe[k], re.lids, se->lids, logical_of(pi, (int)k));
+                        B.list_pair(dst, Fd[k], src, Fe[k], rlids, se->lids, logical_of(pi, (int)k));
                     }
                 }
                 continue;

@@ -15,6 +15,9 @@ struct ghexb_plan_s
 {
     ghexb_context_s* ctx = nullptr;
     std::vector<ghexb_field_s> fields;
+    // unstructured in-place receive (unstructured/communication_object_ipr.hpp:127-141): the
+    // values received from a neighbour land on consecutive halo rows from its first receive index
+    bool in_place_receive = false;
 
     // host tables
     std::vector<ghexb::box_desc> boxes;

@@ -6,18 +6,23 @@
     co.exchange([pattern(f), ...]).wait()
 
 The halo generator may be one generator for every domain or a list with one per domain.
+
+In-place receive (unstructured/communication_object_ipr.hpp): one communication object per
+domain's field, ``co = make_communication_object_ipr(ctx, pattern(f)); co.exchange().wait()``.
 """
 from __future__ import annotations
 
 import ctypes as C
+import threading
 from typing import Any, Optional, Sequence, Union
 
 from ._capi import call, int64_array
-from ._core import (Architecture, FieldDescriptorBase, PatternContainer, array_info, context,
-                    make_communication_object, make_context, make_exchange_plan)
+from ._core import (Architecture, BufferInfo, CommunicationObject, FieldDescriptorBase, PatternContainer,
+                    _flatten, array_info, context, make_communication_object, make_context,
+                    make_exchange_plan)
 
 __all__ = ["DomainDescriptor", "HaloGenerator", "make_pattern", "make_field_descriptor", "wrap_field",
-           "make_communication_object", "make_context", "make_exchange_plan"]
+           "make_communication_object", "make_communication_object_ipr", "make_context", "make_exchange_plan"]
 
 
 class DomainDescriptor:
@@ -150,3 +155,141 @@ def make_field_descriptor(domain_desc: DomainDescriptor, field: Any, *,
 
 def wrap_field(*args, **kwargs) -> FieldDescriptor:
     return make_field_descriptor(*args, **kwargs)
+
+
+# --------------------------------------------------------------------------------------------
+# in-place receive
+# --------------------------------------------------------------------------------------------
+#: seconds a wait() of an in-place receive exchange waits for the other domains to post theirs
+IPR_WAIT_TIMEOUT = 30.0
+
+_groups_lock = threading.Lock()
+
+
+class _InPlaceRound:
+    __slots__ = ("handle", "error", "lock")
+
+    def __init__(self):
+        self.handle = None
+        self.error: Optional[BaseException] = None
+        self.lock = threading.Lock()
+
+
+class _InPlaceGroup:
+    """The in-place receive communication objects of one pattern container. Every domain lives
+    in this process, so the messages between the domains are the copies of one exchange: it is
+    launched when every domain with a halo or a send has posted its exchange()."""
+
+    def __init__(self, ctx: context, pattern: "Pattern"):
+        self.cond = threading.Condition()
+        self.co = CommunicationObject(ctx, in_place_receive=True)
+        self.required = {pattern._ids[i] for i in range(len(pattern))
+                         if pattern.num_spaces(i) or pattern.num_spaces(i, True)}
+        self.posted: dict = {}
+        self.round = _InPlaceRound()
+
+    @staticmethod
+    def of(ctx: context, pattern: "Pattern") -> "_InPlaceGroup":
+        with _groups_lock:
+            groups = ctx.__dict__.setdefault("_in_place_groups", {})
+            entry = groups.get(id(pattern))
+            if entry is None or entry[0] is not pattern:
+                entry = (pattern, _InPlaceGroup(ctx, pattern))
+                groups[id(pattern)] = entry
+            return entry[1]
+
+    def post(self, bis: list) -> _InPlaceRound:
+        with self.cond:
+            ids = [bi.field.domain_id() for bi in bis]
+            if any(i in self.posted for i in ids):
+                raise RuntimeError("earlier exchange operation was not finished")
+            for i, bi in zip(ids, bis):
+                self.posted[i] = bi
+            rnd = self.round
+            if self.required <= set(self.posted):
+                fields = [self.posted[i] for i in sorted(self.posted)]
+                self.posted = {}
+                self.round = _InPlaceRound()
+                try:
+                    rnd.handle = self.co.exchange(fields)
+                except BaseException as e:
+                    rnd.error = e
+                    raise
+                finally:
+                    self.cond.notify_all()
+            return rnd
+
+    def missing(self) -> list:
+        return sorted(self.required - set(self.posted))
+
+    def wait(self, rnd: _InPlaceRound, timeout: Optional[float]) -> None:
+        with self.cond:
+            done = self.cond.wait_for(lambda: rnd.handle is not None or rnd.error is not None,
+                                      IPR_WAIT_TIMEOUT if timeout is None else timeout)
+            if not done:
+                raise RuntimeError(
+                    f"in-place receive: domain(s) {self.missing()} have not posted their exchange; every "
+                    "domain lives in this process, so each one's exchange() must be called before a wait() "
+                    "can complete")
+        if rnd.error is not None:
+            raise RuntimeError(f"in-place receive exchange failed: {rnd.error}") from rnd.error
+        with rnd.lock:
+            rnd.handle.wait()
+
+
+class InPlaceHandle:
+    """communication_object_ipr::handle (communication_object_ipr.hpp:65-99)."""
+
+    def __init__(self, group: _InPlaceGroup, rnd: _InPlaceRound):
+        self._group, self._round = group, rnd
+
+    def wait(self, timeout: Optional[float] = None) -> None:
+        self._group.wait(self._round, timeout)
+
+    def is_ready(self) -> bool:
+        r = self._round
+        if r.error is not None:
+            return True
+        if r.handle is None:
+            return False
+        with r.lock:
+            return r.handle.is_ready()
+
+    def progress(self) -> None:
+        self.is_ready()
+
+
+class CommunicationObjectIPR:
+    """unstructured::communication_object_ipr (communication_object_ipr.hpp:30-186): the exchange
+    of one field whose halo, per neighbour, is stored on consecutive rows, so that GHEX receives
+    each message straight into it. The k-th value of a neighbour's message lands on row
+    first + k, first being the first local index of that neighbour's receive list (:127-141).
+
+    One process holds every domain here: the exchange of all domains of the pattern runs as one
+    stream-ordered kernel, launched once every domain with a halo has called exchange(); wait()
+    returns when it has completed (and raises if a domain never posts its exchange). Fields whose
+    received rows are not halo rows received once, or whose levels are not contiguous rows, raise
+    when the exchange is launched. ``buffer_info`` may also be a list of buffer_infos of distinct
+    domains of one pattern."""
+
+    def __init__(self, ctx: context, buffer_info):
+        bis = _flatten((buffer_info,))
+        if not bis:
+            raise ValueError("an in-place receive needs a buffer_info")
+        pattern = bis[0].pattern
+        if not isinstance(pattern, Pattern) or any(bi.pattern is not pattern for bi in bis):
+            raise TypeError("an in-place receive needs buffer_infos of one unstructured pattern")
+        ids = [bi.field.domain_id() for bi in bis]
+        if len(set(ids)) != len(ids):
+            raise ValueError("one field per domain")
+        self.context = ctx
+        self._bis = bis
+        self._group = _InPlaceGroup.of(ctx, pattern)
+
+    def exchange(self) -> InPlaceHandle:
+        return InPlaceHandle(self._group, self._group.post(self._bis))
+
+
+def make_communication_object_ipr(ctx: context, buffer_info) -> CommunicationObjectIPR:
+    """make_communication_object_ipr(ctx, buffer_info) (communication_object_ipr.hpp:188-196)."""
+    return CommunicationObjectIPR(ctx, buffer_info)

@@ -267,11 +267,13 @@ class UnstructuredWorkload:
         return a
 
 
-def config2(seed: int = 42, ni: int = 1024, nj: int = 2048, parts: int = 16, levels: int = 64) -> UnstructuredWorkload:
+def config2(seed: int = 42, ni: int = 1024, nj: int = 2048, parts: int = 16, levels: int = 64,
+            halo_by_owner: bool = False) -> UnstructuredWorkload:
     """A periodic ni x nj triangulated lattice, vertex ids permuted by the seed, coordinates
     jittered by uniform +-0.3 cell, partitioned into `parts` domains by recursive coordinate
     bisection; every domain stores its inner vertices (ascending lattice index) followed by its
-    1-ring halo (ascending gid)."""
+    1-ring halo (ascending gid; with halo_by_owner, grouped by owning domain first, as an
+    in-place receive needs)."""
     rng = np.random.default_rng(seed)
     n = ni * nj
     perm = rng.permutation(n).astype(np.int64)
@@ -295,9 +297,13 @@ def config2(seed: int = 42, ni: int = 1024, nj: int = 2048, parts: int = 16, lev
         inner = np.nonzero(part == p)[0]
         halo = np.unique(np.concatenate(halo_of[p]))
         hg = perm[halo]
-        hg = np.sort(hg)
+        if halo_by_owner:
+            hg = hg[np.lexsort((hg, part[halo]))]
+        else:
+            hg = np.sort(hg)
         gids = np.concatenate([perm[inner], hg])
         outer = np.arange(inner.size, gids.size, dtype=np.int64)
         doms.append((p, gids, outer))
+    order = ", halos grouped by owner" if halo_by_owner else ""
     return UnstructuredWorkload(f"cfg2: periodic triangulated lattice {ni}x{nj} ({n} vertices), RCB into {parts} "
-                                f"domains, 1-ring halos, {levels} levels", levels, doms, seed)
+                                f"domains, 1-ring halos{order}, {levels} levels", levels, doms, seed)

@@ -163,6 +163,14 @@ int ghexb_co_create(ghexb_context ctx, ghexb_co* out);
 int ghexb_co_destroy(ghexb_co co);
 int ghexb_co_exchange(
     ghexb_co co, const ghexb_field* fields, int n, void* stream, ghexb_handle* out);
+/* Unstructured in-place receive: replaces make_communication_object_ipr(ctx, buffer_info)
+ * (unstructured/communication_object_ipr.hpp:188-196) and its exchange() (:146-152). GHEX
+ * receives a neighbour's message as raw bytes at the address of the first index of the receive
+ * list (:127-141), so the k-th received value lands on halo row first + k. Here the exchange of
+ * such a communication object places the values the same way, in one stream-ordered kernel for
+ * all given fields; it fails with GHEXB_ERR_INVALID where those rows are not halo rows received
+ * once, or where a field's levels are not contiguous rows (levels first, no padding). */
+int ghexb_co_create_ipr(ghexb_context ctx, ghexb_co* out);
 int ghexb_handle_wait(ghexb_handle h);
 int ghexb_handle_is_ready(ghexb_handle h, int* ready);
 int ghexb_handle_destroy(ghexb_handle h);
@@ -171,6 +179,8 @@ int ghexb_handle_destroy(ghexb_handle h);
  * No reference counterpart: GHEX rebuilds its message layout on every exchange
  * (communication_object.hpp:536-624). */
 int ghexb_plan_create(ghexb_context ctx, const ghexb_field* fields, int n, ghexb_plan* out);
+/* The plan of an in-place receive exchange (see ghexb_co_create_ipr). */
+int ghexb_plan_create_ipr(ghexb_context ctx, const ghexb_field* fields, int n, ghexb_plan* out);
 int ghexb_plan_destroy(ghexb_plan plan);
 /* Host-only validation, no device needed: builds the plan's tables and replays the address
  * computation of every element the forward and adjoint kernels touch, failing with

@@ -14,10 +14,12 @@
 #include <ghex/structured/regular/domain_descriptor.hpp>
 #include <ghex/structured/regular/field_descriptor.hpp>
 #include <ghex/structured/regular/halo_generator.hpp>
+#include <ghex/unstructured/communication_object_ipr.hpp>
 #include <ghex/unstructured/pattern.hpp>
 #include <ghex/unstructured/user_concepts.hpp>
 
 #include <chrono>
+#include <memory>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -227,6 +229,40 @@ int unstructured(int n_dom, const int* ids, const int64_t* gid_off, const int* g
     *seconds = timed(iters, [&] { exchange_all(co, bd, bf); });
     return 0;
 }
+// One in-place receive communication object per domain (communication_object_ipr.hpp), as in
+// GHEX's test_in_place_receive: every object posts its receives into the field's halo and sends
+// its packed values, then every handle is waited on.
+template<typename T>
+int unstructured_ipr(int n_dom, const int* ids, const int64_t* gid_off, const int* gids, const int64_t* outer_off,
+    const int64_t* outer_lids, const int* halo_gids, int n_halo_gids, int levels, void** data, int iters,
+    double* seconds)
+{
+    using dom_t = ghex::unstructured::domain_descriptor<int, int>;
+    using hg_t = ghex::unstructured::halo_generator<int, int>;
+    ghex::context ctxt(MPI_COMM_WORLD, true);
+    std::vector<dom_t> doms;
+    for (int i = 0; i < n_dom; ++i)
+    {
+        std::vector<int> g(gids + gid_off[i], gids + gid_off[i + 1]);
+        std::vector<std::size_t> o(outer_lids + outer_off[i], outer_lids + outer_off[i + 1]);
+        doms.emplace_back(ids[i], g.begin(), g.end(), o.begin(), o.end());
+    }
+    hg_t hg = n_halo_gids < 0 ? hg_t{} : hg_t{std::vector<int>(halo_gids, halo_gids + n_halo_gids)};
+    auto pat = ghex::make_pattern<ghex::unstructured::grid>(ctxt, hg, doms);
+    using dd_t = ghex::unstructured::data_descriptor<ghex::cpu, int, int, T>;
+    std::vector<dd_t> dds;
+    dds.reserve(n_dom);
+    for (int d = 0; d < n_dom; ++d) dds.emplace_back(doms[d], (T*)data[d], (std::size_t)levels, true);
+    using co_t = decltype(ghex::unstructured::make_communication_object_ipr(ctxt, pat(dds[0])));
+    std::vector<std::unique_ptr<co_t>> cos;
+    for (int d = 0; d < n_dom; ++d) cos.emplace_back(new co_t(ctxt, pat(dds[d])));
+    *seconds = timed(iters, [&] {
+        std::vector<typename co_t::handle> hs;
+        for (auto& co : cos) hs.push_back(co->exchange());
+        for (auto& h : hs) h.wait();
+    });
+    return 0;
+}
 } // namespace
 
 extern "C" {
@@ -287,6 +323,33 @@ int ghexref_unstructured_exchange(int n_dom, const int* ids, const int64_t* gid_
     {
         return unstructured(n_dom, ids, gid_off, gids, outer_off, outer_lids, n_fields, dtype, levels, levels_first,
             data, iters, seconds);
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// halo_gids: the gid list of the halo generator, or n_halo_gids < 0 for all outer gids
+int ghexref_unstructured_exchange_ipr(int n_dom, const int* ids, const int64_t* gid_off, const int* gids,
+    const int64_t* outer_off, const int64_t* outer_lids, const int* halo_gids, int n_halo_gids, int dtype, int levels,
+    void** data, int iters, double* seconds)
+{
+    try
+    {
+        switch (dtype)
+        {
+            case F64:
+                return unstructured_ipr<double>(n_dom, ids, gid_off, gids, outer_off, outer_lids, halo_gids,
+                    n_halo_gids, levels, data, iters, seconds);
+            case F32:
+                return unstructured_ipr<float>(n_dom, ids, gid_off, gids, outer_off, outer_lids, halo_gids,
+                    n_halo_gids, levels, data, iters, seconds);
+            case I32:
+                return unstructured_ipr<int>(n_dom, ids, gid_off, gids, outer_off, outer_lids, halo_gids,
+                    n_halo_gids, levels, data, iters, seconds);
+            default: return fail("dtype must be f32, f64 or i32");
+        }
     }
     catch (const std::exception& e)
     {

@@ -35,6 +35,10 @@ class recv_request
 
 class communicator
 {
+  public:
+    struct state;
+
+  private:
     struct posted
     {
         unsigned char* buf;
@@ -48,14 +52,25 @@ class communicator
         tag_type tag;
         std::vector<unsigned char> data;
     };
+  public:
     struct state
     {
         std::vector<posted> recvs;
         std::vector<unexpected> early;
     };
+
+  private:
     std::shared_ptr<state> m_state = std::make_shared<state>();
 
   public:
+    communicator() = default;
+    // communicators of one context share the process's mailbox, as MPI communicators built on
+    // one MPI communicator match each other's messages
+    explicit communicator(std::shared_ptr<state> s)
+    : m_state(std::move(s))
+    {
+    }
+
     rank_type rank() const noexcept { return 0; }
     rank_type size() const noexcept { return 1; }
 
@@ -101,6 +116,15 @@ class communicator
                 return {};
             }
         m_state->early.push_back(unexpected{tag, std::vector<unsigned char>(bytes, bytes + n)});
+        return {};
+    }
+
+    // send with a completion callback (the in-place receive's sends): the copy is done at once
+    template<typename T, typename Callback>
+    send_request send(message_buffer<T>& m, rank_type dst, tag_type tag, Callback&& cb)
+    {
+        send(m, dst, tag);
+        cb(m, dst, tag);
         return {};
     }
 

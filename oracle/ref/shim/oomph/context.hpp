@@ -11,6 +11,7 @@ namespace oomph
 class context
 {
     MPI_Comm m_comm;
+    std::shared_ptr<communicator::state> m_mailbox = std::make_shared<communicator::state>();
 
   public:
     context(MPI_Comm comm, bool /*thread_safe*/ = true)
@@ -18,7 +19,7 @@ class context
     {
     }
     MPI_Comm mpi_comm() const noexcept { return m_comm; }
-    communicator get_communicator() { return communicator{}; }
+    communicator get_communicator() { return communicator{m_mailbox}; }
     template<typename T>
     message_buffer<T> make_buffer(std::size_t n)
     {

@@ -123,6 +123,28 @@ def unstructured_exchange(domains, fields, iterations: int = 0) -> float:
     return sec.value
 
 
+def unstructured_exchange_ipr(domains, levels: int, arrays, iterations: int = 0, halo_gids=None) -> float:
+    """The reference's in-place receive: one communication_object_ipr per domain, every exchange
+    posted, then every handle waited on. arrays: one (n,) or C-ordered (n, levels) array per
+    domain, one dtype (float32, float64 or int32); halo_gids: the halo generator's gid list
+    (None: all outer gids)."""
+    gid_off, gids, outer_off, outer = [0], [], [0], []
+    for _, g, o in domains:
+        gids += list(g)
+        gid_off.append(len(gids))
+        outer += list(o)
+        outer_off.append(len(outer))
+    for a in arrays:
+        assert a.flags["C_CONTIGUOUS"], "levels-first arrays expected"
+    sec = C.c_double()
+    ptrs = (C.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])
+    _check(lib().ghexref_unstructured_exchange_ipr(
+        len(domains), _ints([d[0] for d in domains]), _i64(gid_off), _ints(gids), _i64(outer_off), _i64(outer),
+        _ints(halo_gids or []), -1 if halo_gids is None else len(halo_gids), _CODES[arrays[0].dtype], int(levels), ptrs,
+        iterations, C.byref(sec)))
+    return sec.value
+
+
 def cs_check_field(data: np.ndarray, tile: int, x_first: int, y_first: int, mem_halo: int, n: int, levels: int,
                    ncomp: int, is_vector: bool, halo: int) -> int:
     """check_field of the reference's cubed-sphere test on a float32 field (x, y, z, c), x fastest:

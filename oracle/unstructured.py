@@ -11,7 +11,9 @@ Restates, in plain Python and numpy:
     inner to i (in o's halo order), the receive list its local ids in o; tags
     (i << num_bits(#domains)) | id(o), maps ordered by tag;
   * the exchange (data_descriptor get/set, user_concepts.hpp:383-452, with the message buffer
-    removed) and its adjoint in receive-map order, column by column.
+    removed) and its adjoint in receive-map order, column by column;
+  * the in-place receive (unstructured/communication_object_ipr.hpp:105-186): a neighbour's
+    message lands on consecutive rows from the first index of its receive list.
 
 Fields are numpy arrays of shape (n,) or (n, levels) — either memory order.
 """
@@ -116,3 +118,36 @@ def adjoint(recv, send, grads) -> None:
         else:
             np.add.at(grads[e], (S, slice(None)), h)
         grads[d][R] = 0
+
+
+def in_place_rows(recv, domains):
+    """Rows written by GHEX's in-place receive (unstructured/communication_object_ipr.hpp:127-141):
+    a neighbour's message is received as raw bytes at the address of the first index of its
+    receive list, so its k-th value lands on row first + k. Raises ValueError where those rows
+    are not halo rows of the domain received once (the outcome would depend on copy order)."""
+    out = []
+    for d, entries in enumerate(recv):
+        outer = set(domains[d].outer_lids)
+        claimed = set()
+        rows = []
+        for en in entries:
+            r = list(range(en.lids[0], en.lids[0] + len(en.lids)))
+            for x in r:
+                if x not in outer or x in claimed:
+                    raise ValueError(f"in-place receive: the halo of domain {domains[d].id} received from domain "
+                                     f"{domains[en.neighbor].id} is not stored on consecutive halo rows")
+                claimed.add(x)
+            rows.append(r)
+        out.append(rows)
+    return out
+
+
+def exchange_in_place(recv, send, fields, domains) -> None:
+    """The in-place receive exchange of one field per domain: the sender packs its values in the
+    receiver's order, levels innermost (data_descriptor::get, user_concepts.hpp:415-440), the
+    receiver stores them on in_place_rows."""
+    rows = in_place_rows(recv, domains)
+    for d, entries in enumerate(recv):
+        for en, r in zip(entries, rows[d]):
+            s = next(x for x in send[en.neighbor] if x.neighbor == d and x.tag == en.tag)
+            fields[d][np.asarray(r)] = fields[en.neighbor][np.asarray(s.lids)]

@@ -10,6 +10,14 @@
 * cubed_sphere_test.npz — the cubed-sphere test configuration of
   test/structured/cubed_sphere/test_cubed_sphere_exchange.cpp, scalar and vector, exchanged by
   GHEX's own code;
+* unstructured_ipr.json / unstructured_ipr.npz — the 4-domain case of GHEX's in-place receive
+  test (make_domain_ipr, test/unstructured/unstructured_test_case.hpp, its vector literals read
+  as text), initialised as its initialize_data (domain_id*10000 + gid*100 + level on inner
+  vertices, 0 elsewhere) with 1 level (int32) and 2 levels (float64), exchanged by GHEX's own
+  communication_object_ipr (oracle/_ref); and the same with a halo generator whose gid list
+  (seeded permutation, kept in the json under "permuted_halo_gids") orders some receive lists
+  against the storage order, so that the received values land on rows first + k, not on the
+  receive list's rows;
 * regular_small.npz — small regular cases (periodic 2x2x2 halo 1; uneven 3x3x3 with the five
   fields of the benchmark's batched case) exchanged by GHEX's own code.
 
@@ -37,6 +45,54 @@ def read_domains_literal(reference: Path) -> dict:
         if isinstance(node, ast.Assign) and any(getattr(t, "id", None) == "domains" for t in node.targets):
             return ast.literal_eval(node.value)
     raise RuntimeError("no `domains` literal found")
+
+
+def read_ipr_domains(reference: Path) -> dict:
+    """{id: {"gids": [...], "halo_lids": [...]}} from make_domain_ipr's switch cases."""
+    import re
+    src = (reference / "test" / "unstructured" / "unstructured_test_case.hpp").read_text()
+    body = src[src.index("make_domain_ipr(domain_id_type id)"):]
+    body = body[:body.index("default:")]
+    out = {}
+    for m in re.finditer(r"case\s+(\d+):.*?gids\s*=\s*\{([^}]*)\}.*?halo_lids\s*=\s*\{([^}]*)\}", body, re.S):
+        out[int(m.group(1))] = {"gids": [int(v) for v in m.group(2).split(",")],
+                                "halo_lids": [int(v) for v in m.group(3).split(",")]}
+    if len(out) != 4:
+        raise RuntimeError("make_domain_ipr: expected 4 domains")
+    return out
+
+
+def permuted_ipr_halo(doms: dict) -> list:
+    """A seeded permutation of all gids as a halo generator's list, for which every receive list
+    of the in-place receive still starts at the first row of a block of halo rows received once,
+    and a receive list is out of storage order."""
+    from oracle import unstructured as OU
+    odoms = [OU.Domain(d, doms[d]["gids"], doms[d]["halo_lids"]) for d in sorted(doms)]
+    allg = sorted({g for d in doms.values() for g in d["gids"]})
+    rng = np.random.default_rng(2024)
+    for _ in range(10000):
+        gl = [int(g) for g in rng.permutation(allg)]
+        recv, _, _ = OU.make_pattern(odoms, [gl] * len(odoms))
+        try:
+            OU.in_place_rows(recv, odoms)
+        except ValueError:
+            continue
+        if any(e.lids != sorted(e.lids) for entries in recv for e in entries):
+            return gl
+    raise RuntimeError("no permuted halo order found")
+
+
+def ipr_fields(doms: dict, levels: int, dtype) -> list:
+    """initialize_data of the reference's unstructured test case, levels first."""
+    arrays = []
+    for d in sorted(doms):
+        gids, halo = doms[d]["gids"], set(doms[d]["halo_lids"])
+        a = np.zeros((len(gids), levels), dtype=dtype)
+        for x, g in enumerate(gids):
+            if x not in halo:
+                a[x] = [d * 10000 + g * 100 + l for l in range(levels)]
+        arrays.append(a if levels > 1 else np.ascontiguousarray(a[:, 0]))
+    return arrays
 
 
 def unstructured_fields(dom: dict, rank: int, levels: int, order: str) -> np.ndarray:
@@ -73,6 +129,23 @@ def main() -> None:
         for r, f in zip(sorted(doms), fields):
             out[f"out_{order}_{r}"] = f
     np.savez_compressed(HERE / "unstructured_4domain.npz", **out)
+
+    # ---- in-place receive case
+    idoms = read_ipr_domains(reference)
+    rdoms = [(d, idoms[d]["gids"], idoms[d]["halo_lids"]) for d in sorted(idoms)]
+    perm = permuted_ipr_halo(idoms)
+    (HERE / "unstructured_ipr.json").write_text(json.dumps(
+        {**{str(k): v for k, v in idoms.items()}, "permuted_halo_gids": perm}, indent=1))
+    out = {}
+    for levels, dtype in ((1, np.int32), (2, np.float64)):
+        for tag, gl in (("", None), ("perm_", perm)):
+            arrays = ipr_fields(idoms, levels, dtype)
+            for d, x in zip(sorted(idoms), arrays):
+                out[f"{tag}in_{levels}_{d}"] = x.copy()
+            reflib.unstructured_exchange_ipr(rdoms, levels, arrays, halo_gids=gl)
+            for d, x in zip(sorted(idoms), arrays):
+                out[f"{tag}out_{levels}_{d}"] = x
+    np.savez_compressed(HERE / "unstructured_ipr.npz", **out)
 
     # ---- cubed sphere test configuration
     import cs_cases as cs

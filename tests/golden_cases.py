@@ -43,3 +43,16 @@ def unstructured_check(data: np.ndarray, dom: dict, rank: int, levels: int) -> i
             else:
                 bad += (v - 1000 * int(v / 1000)) != 10 * gid + l
     return int(bad)
+
+
+def ipr_case() -> tuple[dict, list]:
+    """The domains of GHEX's in-place receive test ({id: {"gids", "halo_lids"}}) and the permuted
+    halo generator gid list of the second case."""
+    d = json.loads((GOLDEN / "unstructured_ipr.json").read_text())
+    perm = d.pop("permuted_halo_gids")
+    return {int(k): v for k, v in d.items()}, perm
+
+
+def ipr_arrays() -> dict:
+    with np.load(GOLDEN / "unstructured_ipr.npz") as z:
+        return {k: z[k] for k in z.files}
