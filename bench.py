@@ -56,7 +56,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["cfg0", "cfg1", "cfg2", "cfg2_ipr", "cfg3", "cfg4"], default="cfg1")
+    ap.add_argument("--config", choices=["cfg0", "cfg1", "cfg1_staged", "cfg2", "cfg2_ipr", "cfg3", "cfg4"],
+                    default="cfg1")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-configs", action="store_true", help="skip the other workloads")
@@ -147,6 +148,8 @@ def workload(cfg: str):
     from ghex_b200 import workloads as W
     if cfg == "cfg2_ipr":
         return W.config2(halo_by_owner=True)
+    if cfg == "cfg1_staged":
+        return W.config1()
     return {"cfg0": W.config0, "cfg1": W.config1, "cfg2": W.config2, "cfg3": W.config3, "cfg4": W.config4}[cfg]()
 
 
@@ -161,18 +164,25 @@ class Case:
         self.w = w = workload(cfg)
         self.kind = {"cfg2": "unstructured", "cfg2_ipr": "unstructured", "cfg3": "cubed_sphere"}.get(cfg, "regular")
         self.in_place = cfg == "cfg2_ipr"  # unstructured in-place receive
+        self.staged = cfg == "cfg1_staged"  # one pattern per dimension, exchanged in turn
+        self.stage_bis = []
         self.fields = []
         self.bis = []
         self.wrappers = []  # per field: device tensors of every domain -> their buffer_infos
         if self.kind == "regular":
+            from ghex_b200 import workloads as W
             from ghex_b200.structured import regular as R
             self.api = R
             self.ctx = R.make_context(device=device_index)
+            self.stage_bis = [[] for _ in range(w.dim)] if self.staged else []
             for halos, specs in w.halo_groups().items():
                 hg = R.HaloGenerator(((0,) * w.dim, tuple(n - 1 for n in w.shape)),
                                      [(halos[2 * k], halos[2 * k + 1]) for k in range(w.dim)], w.periodic)
                 doms = [R.DomainDescriptor(i, (f, l)) for i, f, l in w.domains]
                 pat = R.make_pattern(self.ctx, hg, doms)
+                stages = (R.make_staged_pattern(self.ctx, doms, W.cartesian_lookup(w.parts), (0,) * w.dim,
+                                                tuple(n - 1 for n in w.shape), halos, w.periodic)
+                          if self.staged else [])
                 for s in specs:
                     host = [w.domain_array(d, s) for d in w.domains]
                     tens = [torch.from_numpy(a).to(dev) for a in host]
@@ -182,6 +192,8 @@ class Case:
                         for dm, d, t in zip(doms, w.domains, ts)])
                     self.wrappers.append(wrap)
                     self.bis += wrap(tens)
+                    for i, sp in enumerate(stages):
+                        self.stage_bis[i] += [sp(bi.field) for bi in self.bis[-len(tens):]]
             names = sorted({np.dtype(s.dtype).name for s in w.fields}, reverse=True)
             self.dtype = "+".join(n.replace("float", "f") for n in names)
         elif self.kind == "cubed_sphere":
@@ -220,6 +232,7 @@ class Case:
                 assert t.stride() == torch.from_numpy(a).stride()
         self.plan = self.api.make_exchange_plan(self.ctx, self.bis, in_place_receive=self.in_place)
         self.alg = self.plan.info()["algorithmic_bytes"]
+        self.stage_plans = [self.api.make_exchange_plan(self.ctx, b) for b in self.stage_bis]
 
     def reset(self):
         import torch
@@ -500,6 +513,35 @@ def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline
     return out
 
 
+def measure_staged(dev, timer, peak, steps, warmup, autotune=True, baseline=True) -> dict:
+    """The batched workload through staged patterns (one pattern per dimension, exchanged in
+    turn: three dependent launches, no edge or corner boxes) beside the one-launch exchange."""
+    case = Case("cfg1_staged", dev, dev.index)
+    s = timer.stream.cuda_stream
+    if autotune:
+        case.plan.autotune(repeats=5)
+        for pl in case.stage_plans:
+            pl.autotune(repeats=5)
+    ms_staged = timer(lambda: [pl.graph_launch(s) for pl in case.stage_plans], steps, warmup)
+    ms_full = timer(lambda: case.plan.graph_launch(s), steps, warmup)
+    out = {"workload": case.w.name + ", staged pattern", "algorithmic_bytes": case.alg, "dtype": case.dtype,
+           "staged": {"ms": ms_staged, "GB/s": case.alg / ms_staged / 1e6, "launches": len(case.stage_plans),
+                      "roofline_frac": case.alg / ms_staged / 1e6 / peak},
+           "full": {"ms": ms_full, "GB/s": case.alg / ms_full / 1e6},
+           "staged_vs_full": ms_staged / ms_full,
+           "descriptors": {"staged": sum(pl.info()["num_descriptors"] for pl in case.stage_plans),
+                           "full": case.plan.info()["num_descriptors"]}}
+    if baseline:
+        import torch
+        case.reset()
+        for pl in case.stage_plans:
+            pl.launch(pl.BATCHED, s)
+        torch.cuda.synchronize()
+        _, expected, _ = case.reference(1)  # the full pattern's exchange: staged must equal it
+        out["bitexact"] = case.mismatches(expected) == 0
+    return out
+
+
 def calibrate(args):
     """The access-pattern roofline: how fast a library copy kernel (torch's strided copy_) moves
     rows of n float64 elements spaced one x-row of a halo field apart (stride 139 elements, as in
@@ -632,6 +674,8 @@ def main():
             if cfg != args.config:
                 line["configs"][cfg] = measure_config(cfg, dev, timer, peak, min(args.steps, 200), max(3, args.warmup),
                                                       not args.no_autotune, not args.no_baseline)
+        line["configs"]["cfg1_staged"] = measure_staged(dev, timer, peak, min(args.steps, 200), max(3, args.warmup),
+                                                        not args.no_autotune, not args.no_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

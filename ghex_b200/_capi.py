@@ -80,6 +80,7 @@ SIGNATURES = {
     "ghexb_context_create": [_i, C.POINTER(_vp)],
     "ghexb_context_destroy": [_vp],
     "ghexb_pattern_create_regular": [_vp, _i, _pi, _pi, _pi, _pi, _i, _pi64, _pi, _pi, C.POINTER(_vp)],
+    "ghexb_pattern_create_regular_staged": [_vp, _i, _pi, _pi, _pi, _pi, _i, _pi64, _pi, _pi, _pi64, C.POINTER(_vp)],
     "ghexb_pattern_create_cubed_sphere": [_vp, _i, _i, _pi, _i, _pi, _pi, _pi, _pi, _pi, C.POINTER(_vp)],
     "ghexb_pattern_create_unstructured": [_vp, _i, _pi64, _pi64, _pi64, _pi64, _pi64, _pi64, _pi64,
                                           C.POINTER(_vp)],

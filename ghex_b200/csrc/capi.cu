@@ -168,6 +168,29 @@ int ghexb_pattern_create_regular(ghexb_context ctx, int dim, const int* g_first,
     });
 }
 
+int ghexb_pattern_create_regular_staged(ghexb_context ctx, int dim, const int* g_first, const int* g_last,
+    const int* halos, const int* periodic, int n_domains, const int64_t* domain_ids, const int* domain_first,
+    const int* domain_last, const int64_t* neighbor_ids, ghexb_pattern* out)
+{
+    return guarded([&] {
+        require(ctx && g_first && g_last && halos && periodic && domain_ids && domain_first && domain_last &&
+                    neighbor_ids && out,
+            "null argument");
+        require(dim >= 1 && dim <= 3, "regular patterns support 1 to 3 dimensions");
+        std::vector<std::unique_ptr<ghexb_pattern_s>> ps;
+        std::vector<ghexb_pattern_s*> raw;
+        for (int i = 0; i < dim; ++i)
+        {
+            ps.push_back(std::make_unique<ghexb_pattern_s>());
+            ps.back()->ctx = ctx;
+            raw.push_back(ps.back().get());
+        }
+        ghexb::build_regular_staged(raw.data(), dim, g_first, g_last, halos, periodic, n_domains, domain_ids,
+            domain_first, domain_last, neighbor_ids);
+        for (int i = 0; i < dim; ++i) out[i] = ps[i].release();
+    });
+}
+
 int ghexb_pattern_create_cubed_sphere(ghexb_context ctx, int edge_size, int levels, const int* halos,
     int n_domains, const int* tiles, const int* x_first, const int* x_last, const int* y_first,
     const int* y_last, ghexb_pattern* out)

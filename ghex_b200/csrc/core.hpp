@@ -51,6 +51,11 @@ using coord4 = std::array<int, 4>;
 struct space_pair
 {
     coord4 lfirst{}, llast{}, gfirst{}, glast{};
+    // staged patterns: the receive space's data comes from the matching send space of the
+    // neighbour, whose first cell is sfirst in the neighbour's local coordinates (the global
+    // coordinates of a staged receive space are not wrapped and do not locate the source)
+    bool has_src = false;
+    coord4 sfirst{};
 };
 
 // The iteration spaces one domain receives from (or sends to) one neighbour domain: one entry
@@ -144,6 +149,9 @@ struct ghexb_field_s
 namespace ghexb
 {
 // pattern builders (pattern_regular.cpp, pattern_cubed_sphere.cpp, pattern_unstructured.cpp)
+void build_regular_staged(ghexb_pattern_s* const* stages, int dim, const int* g_first, const int* g_last,
+    const int* halos, const int* periodic, int n, const int64_t* ids, const int* first, const int* last,
+    const int64_t* neighbor_ids);
 void build_regular(ghexb_pattern_s& p, int dim, const int* g_first, const int* g_last,
     const int* halos, const int* periodic, int n, const int64_t* ids, const int* first,
     const int* last);

@@ -140,8 +140,8 @@ struct builder
         for (int a = 0; a < D; ++a)
         {
             const int64_t dl = sp.lfirst[a] + dst.offsets[a], dh = sp.llast[a] + dst.offsets[a];
-            const int64_t sl = sp.gfirst[a] - sdom.first[a] + src.offsets[a];
-            const int64_t sh = sp.glast[a] - sdom.first[a] + src.offsets[a];
+            const int64_t sl = (sp.has_src ? sp.sfirst[a] : sp.gfirst[a] - sdom.first[a]) + src.offsets[a];
+            const int64_t sh = sl + (sp.llast[a] - sp.lfirst[a]);
             check_range(dst, a, dl, dh, "destination");
             check_range(src, a, sl, sh, "source");
             dof += dl * estride(dst, a);

@@ -23,7 +23,8 @@ from .._core import (Architecture, BufferInfo, CommunicationObject, ExchangePlan
                      PatternContainer, array_info, context, make_communication_object, make_context,
                      make_exchange_plan)
 
-__all__ = ["Architecture", "DomainDescriptor", "HaloGenerator", "make_pattern", "make_field_descriptor",
+__all__ = ["Architecture", "DomainDescriptor", "HaloGenerator", "make_pattern", "make_staged_pattern",
+           "make_field_descriptor",
            "wrap_field", "make_communication_object", "make_context", "make_exchange_plan", "ExchangePlan",
            "CommunicationObject", "BufferInfo"]
 
@@ -143,6 +144,59 @@ def make_pattern(context: context, halo_gen: HaloGenerator, domain_range: Sequen
          int64_array([d.domain_id() for d in domains]), int_array([v for d in domains for v in d.first()]),
          int_array([v for d in domains for v in d.last()]), C.byref(h))
     return Pattern(context, h, domains, halo_gen)
+
+
+def _lookup_id(found: Any) -> int:
+    """The domain id in what a domain lookup returned: an int, or an object with an ``id``
+    attribute or method (as the reference's neighbor type, which also carries a rank)."""
+    if isinstance(found, int):
+        return found
+    v = getattr(found, "id", None)
+    if v is None:
+        raise TypeError("a domain lookup must return a domain id or an object with id()")
+    return int(v() if callable(v) else v)
+
+
+def make_staged_pattern(context: context, domain_range: Sequence[DomainDescriptor], domain_lookup,
+                        g_first: Sequence[int], g_last: Sequence[int], halos: Sequence,
+                        periodic: Sequence[bool]) -> list:
+    """structured::regular::make_staged_pattern(ctx, domains, domain_lookup, g_first, g_last,
+    halos, periodic) (structured/regular/make_pattern.hpp:47-256): one pattern container per
+    dimension; exchanging them one after the other (waiting in between) fills the halos, edges and
+    corners included, through the faces. ``domain_lookup(id, offset)`` returns the neighbour of
+    domain ``id`` at ``offset`` (a tuple with one entry of -1 or +1) as an id or an object with
+    ``id()``; it is called only where the domain has a halo on that side. ``halos`` is the
+    reference's flat array (dim0-, dim0+, dim1-, ...) or one (minus, plus) pair per dimension."""
+    domains = list(domain_range)
+    if not domains:
+        raise ValueError("make_staged_pattern needs at least one domain")
+    dim = len(g_first)
+    flat = [v for h in halos for v in ((h, h) if isinstance(h, int) else h)] if len(halos) == dim else list(halos)
+    if len(flat) != 2 * dim or len(periodic) != dim or len(g_last) != dim:
+        raise ValueError("halos, periodicity and global corners need one entry per dimension")
+    for d in domains:
+        if d.dim != dim:
+            raise ValueError("domain and global corners differ in dimension")
+    nbr = []
+    for d in domains:
+        for i in range(dim):
+            for side, step in ((0, -1), (1, 1)):
+                h = flat[2 * i + side]
+                edge = d.first()[i] - h >= g_first[i] if step < 0 else d.last()[i] + h <= g_last[i]
+                if h > 0 and (periodic[i] or edge):
+                    off = [0] * dim
+                    off[i] = step
+                    nbr.append(_lookup_id(domain_lookup(d.domain_id(), tuple(off))))
+                else:
+                    nbr.append(-1)
+    out = (C.c_void_p * dim)()
+    call("ghexb_pattern_create_regular_staged", context._h, dim, int_array(g_first), int_array(g_last),
+         int_array(flat), int_array([int(bool(p)) for p in periodic]), len(domains),
+         int64_array([d.domain_id() for d in domains]), int_array([v for d in domains for v in d.first()]),
+         int_array([v for d in domains for v in d.last()]), int64_array(nbr), out)
+    gen = HaloGenerator((tuple(g_first), tuple(g_last)), [(flat[2 * k], flat[2 * k + 1]) for k in range(dim)],
+                        periodic)
+    return [Pattern(context, C.c_void_p(out[i]), domains, gen) for i in range(dim)]
 
 
 def _layout_order(strides: Sequence[int]) -> tuple[int, ...]:

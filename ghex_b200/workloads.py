@@ -86,6 +86,11 @@ class RegularWorkload:
     def dim(self) -> int:
         return len(self.shape)
 
+    @property
+    def parts(self) -> tuple:
+        """Blocks per dimension of the tensor-product split."""
+        return tuple(len({d[1][k] for d in self.domains}) for k in range(self.dim))
+
     def halo_groups(self) -> dict:
         """Fields grouped by halo widths (one pattern per group)."""
         groups: dict = {}
@@ -128,6 +133,25 @@ def regular_decomposition(shape: Sequence[int], parts: Sequence[int], seed: int 
         last = tuple(splits[k][c[k]][1] for k in range(len(shape)))
         doms.append((idx, first, last))
     return doms
+
+
+def cartesian_lookup(parts: Sequence[int]):
+    """Domain lookup of a regular_decomposition (ids in x-fastest order), periodic in every
+    dimension: lookup(id, offset) is the id of the domain `offset` blocks away."""
+    dim = len(parts)
+
+    def lookup(i: int, offset) -> int:
+        c, r = [], i
+        for k in range(dim):
+            c.append(r % parts[k])
+            r //= parts[k]
+        n, stride = 0, 1
+        for k in range(dim):
+            n += ((c[k] + offset[k]) % parts[k]) * stride
+            stride *= parts[k]
+        return n
+
+    return lookup
 
 
 def config0(seed: int = 42) -> RegularWorkload:

@@ -93,6 +93,18 @@ int ghexb_pattern_create_regular(ghexb_context ctx, int dim, const int* g_first,
     const int* halos, const int* periodic, int n_domains, const int64_t* domain_ids,
     const int* domain_first, const int* domain_last, ghexb_pattern* out);
 
+/* Staged regular pattern: replaces structured::regular::make_staged_pattern(ctx, domains,
+ * domain_lookup, g_first, g_last, halos, periodic) (structured/regular/make_pattern.hpp:47-256).
+ * Writes dim patterns to out[0..dim): pattern i exchanges the halos of dimension i over the
+ * domain grown by the halos of dimensions 0..i-1, so that exchanging the patterns one after the
+ * other fills edges and corners through the faces. neighbor_ids[(d*dim + i)*2 + s] is the id
+ * that domain_lookup(id of domain d, offset -1 (s = 0) or +1 (s = 1) along dimension i) returns;
+ * it is read only where domain d has a halo on that side. Fails with GHEXB_ERR_INVALID where a
+ * receive space has no send space of the same shape feeding it. */
+int ghexb_pattern_create_regular_staged(ghexb_context ctx, int dim, const int* g_first, const int* g_last,
+    const int* halos, const int* periodic, int n_domains, const int64_t* domain_ids,
+    const int* domain_first, const int* domain_last, const int64_t* neighbor_ids, ghexb_pattern* out);
+
 /* Cubed sphere: cubed_sphere::halo_generator(halos) (structured/cubed_sphere/halo_generator.hpp:59-71)
  * and domain_descriptor(cube{edge_size, levels}, tile, x_first, x_last, y_first, y_last)
  * (structured/cubed_sphere/domain_descriptor.hpp:92-104). halos holds 4 values in the order of

@@ -14,10 +14,12 @@
 #include <ghex/structured/regular/domain_descriptor.hpp>
 #include <ghex/structured/regular/field_descriptor.hpp>
 #include <ghex/structured/regular/halo_generator.hpp>
+#include <ghex/structured/regular/make_pattern.hpp>
 #include <ghex/unstructured/communication_object_ipr.hpp>
 #include <ghex/unstructured/pattern.hpp>
 #include <ghex/unstructured/user_concepts.hpp>
 
+#include <algorithm>
 #include <chrono>
 #include <memory>
 #include <cstdint>
@@ -155,6 +157,100 @@ int regular(const int* g_first, const int* g_last, int n_dom, const int* ids, co
     return 0;
 }
 
+// ---- staged regular pattern ----------------------------------------------------------------
+// make_staged_pattern with a domain lookup read from a table: nbr[(d*D + i)*2 + s] is the
+// neighbour of domain d along dimension i at offset -1 (s = 0) or +1 (s = 1).
+template<int D>
+struct table_lookup
+{
+    struct neighbor
+    {
+        int m_id;
+        int rank() const noexcept { return 0; }
+        int id() const noexcept { return m_id; }
+    };
+    std::vector<int> ids;
+    const int64_t* nbr;
+    neighbor operator()(int id, std::array<int, D> const& offset) const
+    {
+        const int d = (int)(std::find(ids.begin(), ids.end(), id) - ids.begin());
+        for (int i = 0; i < D; ++i)
+            if (offset[i] != 0) return {(int)nbr[((int64_t)d * D + i) * 2 + (offset[i] > 0 ? 1 : 0)]};
+        return {id};
+    }
+};
+
+// One field (one dtype) exchanged stage after stage with one communication object, as GHEX's
+// test_simple_regular_domain does.
+template<int D, typename T>
+int regular_staged(const int* g_first, const int* g_last, int n_dom, const int* ids, const int* firsts,
+    const int* lasts, const int* halos, const int* periodic, const int64_t* nbr, void** data, const int* offsets,
+    const int* extents, int iters, double* seconds)
+{
+    using dom_t = ghex::structured::regular::domain_descriptor<int, std::integral_constant<int, D>>;
+    using layout = std::conditional_t<D == 3, gridtools::layout_map<2, 1, 0>,
+        std::conditional_t<D == 2, gridtools::layout_map<1, 0>, gridtools::layout_map<0>>>;
+    using arr = std::array<int, D>;
+    ghex::context ctxt(MPI_COMM_WORLD, true);
+    std::vector<dom_t> doms;
+    for (int i = 0; i < n_dom; ++i)
+    {
+        arr f, l;
+        for (int k = 0; k < D; ++k) f[k] = firsts[i * D + k], l[k] = lasts[i * D + k];
+        doms.emplace_back(ids[i], f, l);
+    }
+    arr gf, gl;
+    std::array<int, 2 * D> h;
+    std::array<bool, D> p;
+    for (int k = 0; k < D; ++k) gf[k] = g_first[k], gl[k] = g_last[k], p[k] = periodic[k] != 0;
+    for (int k = 0; k < 2 * D; ++k) h[k] = halos[k];
+    table_lookup<D> lu{std::vector<int>(ids, ids + n_dom), nbr};
+    auto stages = ghex::structured::regular::make_staged_pattern(ctxt, doms, lu, gf, gl, h, p);
+    using fd_t = ghex::structured::regular::field_descriptor<T, ghex::cpu, dom_t, layout>;
+    std::vector<fd_t> fds;
+    fds.reserve(n_dom);
+    for (int d = 0; d < n_dom; ++d)
+    {
+        arr off, ext;
+        for (int k = 0; k < D; ++k) off[k] = offsets[k], ext[k] = extents[d * D + k];
+        fds.push_back(ghex::wrap_field<ghex::cpu, layout>(doms[d], (T*)data[d], off, ext));
+    }
+    using pattern_t = std::remove_reference_t<decltype(*stages[0])>;
+    using bi_t = decltype((*stages[0])(fds[0]));
+    auto co = ghex::make_communication_object<pattern_t>(ctxt);
+    *seconds = timed(iters, [&] {
+        for (int i = 0; i < D; ++i)
+        {
+            std::vector<bi_t> bis;
+            for (auto& f : fds) bis.push_back((*stages[i])(f));
+            co.exchange(bis.begin(), bis.end()).wait();
+        }
+    });
+    return 0;
+}
+
+template<int D>
+int regular_staged_dispatch(int dtype, const int* g_first, const int* g_last, int n_dom, const int* ids,
+    const int* firsts, const int* lasts, const int* halos, const int* periodic, const int64_t* nbr, void** data,
+    const int* offsets, const int* extents, int iters, double* seconds)
+{
+    switch (dtype)
+    {
+        case F64:
+            return regular_staged<D, double>(g_first, g_last, n_dom, ids, firsts, lasts, halos, periodic, nbr, data,
+                offsets, extents, iters, seconds);
+        case F32:
+            return regular_staged<D, float>(g_first, g_last, n_dom, ids, firsts, lasts, halos, periodic, nbr, data,
+                offsets, extents, iters, seconds);
+        case I32:
+            return regular_staged<D, int32_t>(g_first, g_last, n_dom, ids, firsts, lasts, halos, periodic, nbr, data,
+                offsets, extents, iters, seconds);
+        default:
+            return regular_staged<D, int64_t>(g_first, g_last, n_dom, ids, firsts, lasts, halos, periodic, nbr, data,
+                offsets, extents, iters, seconds);
+    }
+}
+
 // ---- cubed sphere -------------------------------------------------------------------------
 template<typename T>
 int cubed(int edge, int levels, const int* halos, int n_dom, const int* tiles, const int* xf, const int* xl,
@@ -271,6 +367,29 @@ int ghexref_last_error(char* buf, size_t len)
 {
     std::snprintf(buf, len, "%s", g_err.c_str());
     return 0;
+}
+
+int ghexref_regular_staged_exchange(int dim, const int* g_first, const int* g_last, int n_dom, const int* ids,
+    const int* firsts, const int* lasts, const int* halos, const int* periodic, const int64_t* neighbor_ids,
+    int dtype, void** data, const int* offsets, const int* extents, int iters, double* seconds)
+{
+    try
+    {
+        switch (dim)
+        {
+            case 2:
+                return regular_staged_dispatch<2>(dtype, g_first, g_last, n_dom, ids, firsts, lasts, halos, periodic,
+                    neighbor_ids, data, offsets, extents, iters, seconds);
+            case 3:
+                return regular_staged_dispatch<3>(dtype, g_first, g_last, n_dom, ids, firsts, lasts, halos, periodic,
+                    neighbor_ids, data, offsets, extents, iters, seconds);
+            default: return fail("dim must be 2 or 3");
+        }
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
 }
 
 int ghexref_regular_exchange(int dim, const int* g_first, const int* g_last, int n_dom, const int* ids,

@@ -80,6 +80,29 @@ def regular_exchange(shape, periodic_groups, domains, fields, iterations: int = 
     return sec.value
 
 
+def regular_staged_exchange(shape, halos, periodic, domains, lookup, arrays, offsets, iterations: int = 0) -> float:
+    """The reference's staged pattern (make_staged_pattern) with one field, x-fastest arrays of
+    one dtype, exchanged stage after stage by one communication object. lookup(id, offset) is the
+    domain lookup; it is tabulated for offsets -1 and +1 along every dimension."""
+    dim = len(shape)
+    nbr = []
+    for i_d, first, last in domains:
+        for i in range(dim):
+            for step in (-1, 1):
+                off = [0] * dim
+                off[i] = step
+                h = halos[2 * i + (0 if step < 0 else 1)]
+                nbr.append(int(lookup(i_d, tuple(off))) if h > 0 else -1)
+    exts = [v for a in arrays for v in a.shape[:dim]]
+    sec = C.c_double()
+    _check(lib().ghexref_regular_staged_exchange(
+        dim, _ints([0] * dim), _ints([n - 1 for n in shape]), len(domains), _ints([d[0] for d in domains]),
+        _ints([v for d in domains for v in d[1]]), _ints([v for d in domains for v in d[2]]), _ints(halos),
+        _ints([int(p) for p in periodic]), _i64(nbr), _CODES[arrays[0].dtype], _ptrs(arrays), _ints(offsets),
+        _ints(exts), iterations, C.byref(sec)))
+    return sec.value
+
+
 def cubed_exchange(edge, levels, halos, domains, fields, iterations: int = 0) -> float:
     """domains: (tile, x_first, x_last, y_first, y_last); fields: list of
     (ncomp, is_vector, offsets (x, y, z), [array (x, y, z, c) per domain]), one dtype for all."""

@@ -7,6 +7,9 @@ Restates, in plain Python and numpy:
   * the exchange: pack (structured/regular/field_descriptor.hpp:72-83, pack_kernels.hpp:66-101)
     followed by unpack (field_descriptor.hpp:85-96, pack_kernels.hpp:103-138) with the buffer
     removed — the value that lands in a halo cell is the value of the cell it was packed from.
+  * make_staged_pattern (structured/regular/make_pattern.hpp:47-256) and the exchange of its
+    stages one after the other, each as GHEX's message passing: all send spaces packed, then
+    the k-th receive space of an entry filled from the k-th send space of the sender's entry;
   * the adjoint: the explicit transpose of that copy, visited in receive-map order
     (pattern order, then neighbour id, then iteration space, then for_loop order of
     util/for_each.hpp:84-112): owner += halo; halo = 0.
@@ -106,6 +109,107 @@ def make_pattern(g_first, g_last, halos, periodic, domains: Sequence[Domain]) ->
             entries.append(Entry(idx[sid], tag, by_src[sid]))
         out.append(entries)
     return out
+
+
+def make_staged_pattern(g_first, g_last, halos, periodic, domains: Sequence[Domain], lookup) -> list:
+    """One (receive entries, send entries) pair per dimension (make_pattern.hpp:47-256), single
+    process: per domain the entries in neighbour-id order, tags a running counter over the
+    stage's receive entries, a send entry tagged as the receive entry it feeds. lookup(id,
+    offset) -> neighbour id, called only where the domain has a halo on that side."""
+    dim = len(g_first)
+    idx = {d.id: i for i, d in enumerate(domains)}
+    recv = [[{} for _ in domains] for _ in range(dim)]
+    send = [[{} for _ in domains] for _ in range(dim)]
+    for di, d in enumerate(domains):
+        lf, ll = [0] * dim, [d.last[k] - d.first[k] for k in range(dim)]
+        gf, gl = list(d.first), list(d.last)
+        for i in range(dim):
+            hm, hp = halos[2 * i], halos[2 * i + 1]
+            has_left = hm > 0 and (periodic[i] or gf[i] - hm >= g_first[i])
+            has_right = hp > 0 and (periodic[i] or gl[i] + hp <= g_last[i])
+
+            def space(lo, hi):
+                a_lf, a_ll, a_gf, a_gl = list(lf), list(ll), list(gf), list(gl)
+                a_lf[i], a_ll[i] = lo, hi
+                a_gf[i], a_gl[i] = gf[i] + lo - lf[i], gf[i] + hi - lf[i]
+                return Space(tuple(a_lf), tuple(a_ll), tuple(a_gf), tuple(a_gl))
+
+            def neighbour(step):
+                off = [0] * dim
+                off[i] = step
+                return lookup(d.id, tuple(off))
+
+            if has_left:
+                recv[i][di].setdefault(neighbour(-1), []).append(space(lf[i] - hm, lf[i] - 1))
+            if has_right:
+                send[i][di].setdefault(neighbour(1), []).append(space(ll[i] + 1 - hm, ll[i]))
+                recv[i][di].setdefault(neighbour(1), []).append(space(ll[i] + 1, ll[i] + hp))
+            if has_left:
+                send[i][di].setdefault(neighbour(-1), []).append(space(lf[i], lf[i] - 1 + hp))
+                lf[i] -= hm
+                gf[i] -= hm
+            if has_right:
+                ll[i] += hp
+                gl[i] += hp
+    stages = []
+    for i in range(dim):
+        tag = -1
+        r_out = []
+        for di in range(len(domains)):
+            entries = []
+            for nid in sorted(recv[i][di]):
+                tag += 1
+                entries.append(Entry(idx[nid], tag, recv[i][di][nid]))
+            r_out.append(entries)
+        s_out = []
+        for di in range(len(domains)):
+            entries = []
+            for nid in sorted(send[i][di]):
+                # an entry holding only empty spaces (zero halo width on that side) may feed no
+                # receive entry; it carries nothing and keeps tag 0
+                rtag = next((e.tag for e in r_out[idx[nid]] if e.neighbor == di), 0)
+                entries.append(Entry(idx[nid], rtag, send[i][di][nid]))
+            s_out.append(entries)
+        # every receive space needs a non-empty send space of the same shape feeding it; with a
+        # zero halo width on one side only, the reference's messages do not match (the receive
+        # expects data the sender never packs), which is refused here
+        for d, entries in enumerate(r_out):
+            for en in entries:
+                sent = [x for x in s_out[en.neighbor] if x.neighbor == d]
+                full = [sp for x in sent for sp in x.spaces if _nonempty(sp)]
+                if len(full) != len(en.spaces) or any(
+                        tuple(a - b for a, b in zip(r.llast, r.lfirst)) != tuple(a - b for a, b in zip(f.llast, f.lfirst))
+                        for r, f in zip(en.spaces, full)):
+                    raise ValueError(f"staged pattern: what domain {domains[d].id} receives from domain "
+                                     f"{domains[en.neighbor].id} does not match what that domain sends")
+        stages.append((r_out, s_out))
+    return stages
+
+
+def _nonempty(sp: Space) -> bool:
+    return all(b >= a for a, b in zip(sp.lfirst, sp.llast))
+
+
+def exchange_staged(stages, domains: Sequence[Domain], fields: Sequence[np.ndarray], offsets: Sequence[tuple]) -> None:
+    """The stages in order; within one, every send space is read before any receive space is
+    written (pack, then unpack)."""
+    dim = len(domains[0].first)
+    for recv, send in stages:
+        moves = []
+        for d, entries in enumerate(recv):
+            for en in entries:
+                e = en.neighbor
+                sent = next(x for x in send[e] if x.neighbor == d and x.tag == en.tag)
+                # a side with a zero halo width sends an empty space, which carries nothing
+                spaces = [x for x in sent.spaces if _nonempty(x)]
+                for rs, ss in zip(en.spaces, spaces):
+                    dlo = tuple(rs.lfirst[k] + offsets[d][k] for k in range(dim))
+                    dhi = tuple(rs.llast[k] + offsets[d][k] for k in range(dim))
+                    slo = tuple(ss.lfirst[k] + offsets[e][k] for k in range(dim))
+                    shi = tuple(ss.llast[k] + offsets[e][k] for k in range(dim))
+                    moves.append((d, _slices(dlo, dhi), fields[e][_slices(slo, shi)].copy()))
+        for d, dst, vals in moves:
+            fields[d][dst] = vals
 
 
 def _slices(lo, hi):

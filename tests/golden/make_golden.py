@@ -18,6 +18,10 @@
   (seeded permutation, kept in the json under "permuted_halo_gids") orders some receive lists
   against the storage order, so that the received values land on rows first + k, not on the
   receive list's rows;
+* regular_staged.npz — the staged pattern (make_staged_pattern): the 2-D case of
+  test/structured/regular/test_simple_regular_domain.cpp (one process: two 8x4 domains stacked
+  in y, halo 3, periodic, cells holding their (x, y) coordinates, the test's domain lookup) and a
+  3-D uneven 3x2x3 split with asymmetric halos, exchanged stage by stage by GHEX's own code;
 * regular_small.npz — small regular cases (periodic 2x2x2 halo 1; uneven 3x3x3 with the five
   fields of the benchmark's batched case) exchanged by GHEX's own code.
 
@@ -146,6 +150,19 @@ def main() -> None:
             for d, x in zip(sorted(idoms), arrays):
                 out[f"{tag}out_{levels}_{d}"] = x
     np.savez_compressed(HERE / "unstructured_ipr.npz", **out)
+
+    # ---- staged regular pattern
+    import regular_cases as rc
+    out = {}
+    for name, case in rc.staged_cases().items():
+        arrays = case["arrays"]()
+        for i, x in enumerate(arrays):
+            out[f"{name}_in_{i}"] = x.copy(order="K")
+        reflib.regular_staged_exchange(case["shape"], case["halos"], case["periodic"], case["domains"],
+                                       case["lookup"], arrays, case["offsets"])
+        for i, x in enumerate(arrays):
+            out[f"{name}_out_{i}"] = x
+    np.savez_compressed(HERE / "regular_staged.npz", **out)
 
     # ---- cubed sphere test configuration
     import cs_cases as cs

@@ -56,3 +56,8 @@ def ipr_case() -> tuple[dict, list]:
 def ipr_arrays() -> dict:
     with np.load(GOLDEN / "unstructured_ipr.npz") as z:
         return {k: z[k] for k in z.files}
+
+
+def staged_arrays() -> dict:
+    with np.load(GOLDEN / "regular_staged.npz") as z:
+        return {k: z[k] for k in z.files}

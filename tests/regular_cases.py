@@ -16,12 +16,12 @@ import numpy as np
 DIM, HALO = 8, 3
 
 
-def simple_2d_domains():
-    """(id, first, last) of the 8 domains: ranks on a 2x2 grid, 2 domains each (:162-168)."""
+def simple_2d_domains(dims=(2, 2)):
+    """(id, first, last) of the domains: ranks on a dims grid with x fastest (sim(), :470-474),
+    2 domains each (make_domain, :162-168)."""
     doms = []
-    dims = (2, 2)
-    for rank in range(4):
-        cx, cy = divmod(rank, dims[1])  # MPI cartesian coordinates: the last one varies fastest
+    for rank in range(dims[0] * dims[1]):
+        cy, cx = divmod(rank, dims[0])
         for i in range(2):
             x = cx * DIM
             y = (cy * 2 + i) * (DIM // 2)
@@ -101,3 +101,61 @@ def owner_check(w, arrays, spec):
         u = np.dtype(f"u{a.itemsize}")
         bad += int(np.count_nonzero(owner_vals.view(u) != np.ascontiguousarray(a).view(u)))
     return bad
+
+
+# ---- staged pattern (make_staged_pattern, structured/regular/make_pattern.hpp) ------------------
+def simple_2d_lookup(dims):
+    """domain_lu of the reference test (:170-191): the neighbour of domain `id` at `offset`."""
+    def lookup(id_, offset):
+        rank = id_ // 2
+        y_ = id_ - 2 * rank
+        y = rank // dims[0]
+        x = rank - y * dims[0]
+        y = ((2 * y + y_ + offset[1]) + dims[1] * 2) % (dims[1] * 2)
+        x = (x + offset[0] + dims[0]) % dims[0]
+        n_rank = (y // 2) * dims[0] + x
+        return 2 * n_rank + (y % 2)
+    return lookup
+
+
+def simple_2d_packed(doms):
+    """The (x, y) int32 pairs of simple_2d_fields as one int64 per cell (x in the low half), in
+    the test's layout: x fastest (layout_map<1, 0>)."""
+    out = []
+    for a in simple_2d_fields(doms):
+        p = (a[..., 1].astype(np.int64) << 32) | (a[..., 0].astype(np.int64) & 0xFFFFFFFF)
+        out.append(np.asfortranarray(p))
+    return out
+
+
+def pairs_view(packed: np.ndarray) -> np.ndarray:
+    """The int64 cells of simple_2d_packed as an (x, y, 2) int32 array over the same memory:
+    component innermost, then x, then y."""
+    nx, ny = packed.shape
+    buf = np.asfortranarray(packed).ravel(order="F").view(np.int32)
+    return np.lib.stride_tricks.as_strided(buf, shape=(nx, ny, 2), strides=(8, 8 * nx, 4))
+
+
+def staged_cases() -> dict:
+    """Workloads of the staged pattern: the 2-D test case for one process (dims 1x1) and for a
+    2x2 process grid, and an uneven 3-D split with asymmetric halos."""
+    from ghex_b200 import workloads as W
+    out = {}
+    for dims in ((1, 1), (2, 2)):
+        doms = simple_2d_domains(dims)
+        out[f"simple_2d_{dims[0]}x{dims[1]}"] = {
+            "shape": (dims[0] * DIM, dims[1] * DIM), "halos": (HALO,) * 4, "periodic": (True, True),
+            "domains": doms, "lookup": simple_2d_lookup(dims), "offsets": (HALO, HALO), "dims": dims,
+            "arrays": (lambda doms=doms: simple_2d_packed(doms))}
+    shape, parts, halos = (20, 16, 12), (3, 2, 3), (2, 1, 1, 2, 1, 2)
+    doms3 = W.regular_decomposition(shape, parts, 3)
+
+    def arrays3():
+        rng = np.random.default_rng(23)
+        return [np.asfortranarray(rng.standard_normal(
+            tuple(l[k] - f[k] + 1 + halos[2 * k] + halos[2 * k + 1] for k in range(3)))) for _, f, l in doms3]
+    out["uneven_3d"] = {"shape": shape, "halos": halos, "periodic": (True, False, True), "domains": doms3,
+                        "lookup": W.cartesian_lookup(parts), "offsets": (halos[0], halos[2], halos[4]),
+                        "arrays": arrays3}
+    return out
+

@@ -160,3 +160,38 @@ def test_unstructured_plan_accesses_in_bounds(case):
     n = C.c_int64()
     _capi.call("ghexb_plan_check", ctx._h, arr, len(handles), C.byref(n))
     assert n.value > 0
+
+
+@pytest.mark.parametrize("name", ["simple_2d_2x2", "uneven_3d"])
+def test_staged_plan_accesses_in_bounds(name):
+    """Every stage of a staged pattern: accesses stay inside the fields, and the forward writes
+    each receive cell of the stage once."""
+    import regular_cases as RC
+    case = RC.staged_cases()[name]
+    dim = len(case["shape"])
+    ctx = R.make_context(device=0)
+    doms = [R.DomainDescriptor(i, (f, l)) for i, f, l in case["domains"]]
+    pats = R.make_staged_pattern(ctx, doms, case["lookup"], (0,) * dim, tuple(n - 1 for n in case["shape"]),
+                                 case["halos"], case["periodic"])
+    keep, base = [], 1 << 40
+    fields = []
+    for d, (_, f, l) in zip(doms, case["domains"]):
+        ext = tuple(l[k] - f[k] + 1 + case["halos"][2 * k] + case["halos"][2 * k + 1] for k in range(dim))
+        fields.append(FakeField(d, base, _capi.F64, 8, case["offsets"], ext))
+        n = 1
+        for e in ext:
+            n *= e
+        base += ((n * 8 + 255) // 256) * 256
+    for p in pats:
+        handles = [p(f).handle() for f in fields]
+        arr = (C.c_void_p * len(handles))(*handles)
+        n = C.c_int64()
+        _capi.call("ghexb_plan_check", ctx._h, arr, len(handles), C.byref(n))
+        cells = 0
+        for i in range(len(doms)):
+            for _, lf, ll, _, _ in p.spaces(i):
+                c = 1
+                for k in range(dim):
+                    c *= ll[k] - lf[k] + 1
+                cells += c
+        assert n.value == 2 * cells
