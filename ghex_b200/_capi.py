@@ -84,6 +84,8 @@ SIGNATURES = {
     "ghexb_pattern_create_cubed_sphere": [_vp, _i, _i, _pi, _i, _pi, _pi, _pi, _pi, _pi, C.POINTER(_vp)],
     "ghexb_pattern_create_unstructured": [_vp, _i, _pi64, _pi64, _pi64, _pi64, _pi64, _pi64, _pi64,
                                           C.POINTER(_vp)],
+    "ghexb_pattern_create_unstructured_hinted": [_vp, _i, _pi64, _pi64, _pi64, _pi64, _pi64, _pi64, _pi64, _pi64,
+                                                 _pi64, _pi64, C.POINTER(_vp)],
     "ghexb_pattern_destroy": [_vp],
     "ghexb_pattern_num_domains": [_vp, _pi],
     "ghexb_pattern_domain_id": [_vp, _i, _pi64],

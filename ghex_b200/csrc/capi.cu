@@ -223,6 +223,26 @@ int ghexb_pattern_create_unstructured(ghexb_context ctx, int n_domains, const in
     });
 }
 
+int ghexb_pattern_create_unstructured_hinted(ghexb_context ctx, int n_domains, const int64_t* domain_ids,
+    const int64_t* gid_offsets, const int64_t* gids, const int64_t* outer_offsets, const int64_t* outer_lids,
+    const int64_t* halo_gid_offsets, const int64_t* halo_gids, const int64_t* hint_offsets,
+    const int64_t* hint_domain_ids, const int64_t* hint_remote_indices, ghexb_pattern* out)
+{
+    return guarded([&] {
+        require(ctx && out && domain_ids && gid_offsets && outer_offsets && hint_offsets, "null argument");
+        require(n_domains > 0, "a pattern needs at least one domain");
+        require(gid_offsets[n_domains] == 0 || gids, "null gids");
+        require(outer_offsets[n_domains] == 0 || outer_lids, "null outer lids");
+        require(!halo_gid_offsets || halo_gid_offsets[n_domains] == 0 || halo_gids, "null halo gids");
+        require(hint_offsets[n_domains] == 0 || (hint_domain_ids && hint_remote_indices), "null hints");
+        auto p = std::make_unique<ghexb_pattern_s>();
+        p->ctx = ctx;
+        ghexb::build_unstructured(*p, n_domains, domain_ids, gid_offsets, gids, outer_offsets, outer_lids,
+            halo_gid_offsets, halo_gids, hint_offsets, hint_domain_ids, hint_remote_indices);
+        *out = p.release();
+    });
+}
+
 int ghexb_pattern_destroy(ghexb_pattern p)
 {
     delete p;

@@ -158,9 +158,11 @@ void build_regular(ghexb_pattern_s& p, int dim, const int* g_first, const int* g
 void build_cubed_sphere(ghexb_pattern_s& p, int edge, int levels, const int* halos, int n,
     const int* tiles, const int* x_first, const int* x_last, const int* y_first,
     const int* y_last);
+// hint_off == nullptr: no receive domain ids generator
 void build_unstructured(ghexb_pattern_s& p, int n, const int64_t* ids, const int64_t* gid_off,
     const int64_t* gids, const int64_t* outer_off, const int64_t* outer_lids,
-    const int64_t* halo_off, const int64_t* halo_gids);
+    const int64_t* halo_off, const int64_t* halo_gids, const int64_t* hint_off = nullptr,
+    const int64_t* hint_ids = nullptr, const int64_t* hint_remote = nullptr);
 
 // cubed-sphere coordinate transforms (pattern_cubed_sphere.cpp)
 struct cs_transform

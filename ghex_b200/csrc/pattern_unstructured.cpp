@@ -13,7 +13,14 @@
 //    (unstructured/pattern.hpp:187-370): for every domain and every neighbour domain, the
 //    neighbour's halo gids that are inner to the domain become the send list (in the neighbour's
 //    halo order) and, mapped through the neighbour's make_outer_lids, its receive list. Tags are
-//    (sender index << num_bits(#domains)) | receiver id; maps are ordered by (rank, tag).
+//    (sender index << num_bits(#domains)) | receiver id; maps are ordered by (rank, tag);
+//  * make_pattern_impl<unstructured grid>::apply with a receive domain ids generator
+//    (unstructured/pattern.hpp:371-588): the generator names, for every halo element in the halo
+//    generator's order, its owner domain and its local index there; receive lists group the halo
+//    elements by owner (ascending owner id), the owner's send list holds the named local indices in
+//    the receiver's order, tags are (owner id << 7) + receiver id and the maximum tag is
+//    (max id << 7) + max id. Unlike the reference, a named index must be an inner element of the
+//    owner (a halo element would be read while it is being written).
 #include <algorithm>
 #include <map>
 #include <unordered_map>
@@ -60,7 +67,8 @@ unsigned num_bits(unsigned n) { return n ? 1u + num_bits(n >> 1) : 1u; }
 
 void build_unstructured(ghexb_pattern_s& p, int n, const int64_t* ids, const int64_t* gid_off,
     const int64_t* gids, const int64_t* outer_off, const int64_t* outer_lids,
-    const int64_t* halo_off, const int64_t* halo_gids)
+    const int64_t* halo_off, const int64_t* halo_gids, const int64_t* hint_off, const int64_t* hint_ids,
+    const int64_t* hint_remote)
 {
     if (n < 1) throw error(GHEXB_ERR_INVALID, "a pattern needs at least one domain");
     p.kind = pattern_kind::unstructured;
@@ -106,7 +114,7 @@ void build_unstructured(ghexb_pattern_s& p, int n, const int64_t* ids, const int
     if (max_id > (int64_t)0x7fffffff) throw error(GHEXB_ERR_INVALID, "domain ids must fit into int");
 
     // halos of every domain: local ids and their gids
-    std::vector<std::vector<int64_t>> halo_gid_lists(n);
+    std::vector<std::vector<int64_t>> halo_gid_lists(n), halo_lid_lists(n);
     for (int i = 0; i < n; ++i)
     {
         std::vector<int64_t> lids;
@@ -114,6 +122,53 @@ void build_unstructured(ghexb_pattern_s& p, int n, const int64_t* ids, const int
         else
             lids = dom[i].make_outer_lids(dom[i].outer_gids);
         for (auto lid : lids) halo_gid_lists[i].push_back(dom[i].gids[lid]);
+        halo_lid_lists[i] = std::move(lids);
+    }
+
+    if (hint_off)
+    {
+        auto hint_tag = [](int64_t sender, int64_t receiver) {
+            return (int)(((uint32_t)sender << 7) + (uint32_t)receiver);
+        };
+        p.max_tag = hint_tag(max_id, max_id);
+        std::vector<std::map<int64_t, list_entry>> recv(n), send(n); // keyed by neighbour id
+        for (int i = 0; i < n; ++i)
+        {
+            const auto& lids = halo_lid_lists[i];
+            if (hint_off[i + 1] - hint_off[i] != (int64_t)lids.size())
+                throw error(GHEXB_ERR_INVALID, "the receive domain ids generator gives " +
+                                                   std::to_string(hint_off[i + 1] - hint_off[i]) + " entries for the " +
+                                                   std::to_string(lids.size()) + " halo elements of domain " +
+                                                   std::to_string(dom[i].id));
+            for (size_t k = 0; k < lids.size(); ++k)
+            {
+                const int64_t owner = hint_ids[hint_off[i] + (int64_t)k];
+                const int64_t rem = hint_remote[hint_off[i] + (int64_t)k];
+                const int o = p.find_domain(owner);
+                if (o < 0)
+                    throw error(GHEXB_ERR_INVALID, "the receive domain ids generator names unknown domain " +
+                                                       std::to_string(owner));
+                if (rem < 0 || rem >= (int64_t)dom[o].gids.size() ||
+                    std::binary_search(p.domains[o].outer.begin(), p.domains[o].outer.end(), rem))
+                    throw error(GHEXB_ERR_INVALID, "the receive domain ids generator names local index " +
+                                                       std::to_string(rem) + " of domain " + std::to_string(owner) +
+                                                       ", which is not an inner element");
+                auto& r = recv[i][owner];
+                r.neighbor = o;
+                r.tag = hint_tag(owner, dom[i].id);
+                r.lids.push_back(lids[k]);
+                auto& sd = send[o][dom[i].id];
+                sd.neighbor = i;
+                sd.tag = r.tag;
+                sd.lids.push_back(rem);
+            }
+        }
+        for (int i = 0; i < n; ++i)
+        {
+            for (auto& kv : send[i]) p.domains[i].usend.push_back(std::move(kv.second));
+            for (auto& kv : recv[i]) p.domains[i].urecv.push_back(std::move(kv.second));
+        }
+        return;
     }
 
     const unsigned shift = num_bits((unsigned)n);

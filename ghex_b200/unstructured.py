@@ -76,8 +76,27 @@ class Pattern(PatternContainer):
         self.domains = list(domains)
 
 
-def make_pattern(context: context, halo_gen: Union[HaloGenerator, Sequence[HaloGenerator]],
-                 domain_range: Sequence[DomainDescriptor]) -> Pattern:
+def _hints_of(found) -> tuple:
+    """(owner ids, remote indices) from what a receive domain ids generator returned: an object
+    with domain_ids() and remote_indices() (attributes or methods, as the reference's halo type),
+    or a tuple (domain_ids, remote_indices[, ranks])."""
+    if isinstance(found, (tuple, list)):
+        return list(found[0]), list(found[1])
+    get = lambda name: (lambda v: v() if callable(v) else v)(getattr(found, name))
+    return list(get("domain_ids")), list(get("remote_indices"))
+
+
+def make_pattern(context: context, halo_gen: Union[HaloGenerator, Sequence[HaloGenerator]], *args) -> Pattern:
+    """make_pattern<unstructured::grid>(ctx, halo_gen, domains), or with a receive domain ids
+    generator make_pattern(ctx, halo_gen, recv_domain_ids_gen, domains) (pattern_container.hpp:
+    112-146): ``recv_domain_ids_gen(domain)`` returns, for each halo element in the halo
+    generator's order, its owner domain id and its local index in the owner."""
+    if len(args) == 1:
+        rdig, domain_range = None, args[0]
+    elif len(args) == 2:
+        rdig, domain_range = args
+    else:
+        raise TypeError("make_pattern(ctx, halo_gen, [recv_domain_ids_gen,] domains)")
     domains = list(domain_range)
     if not domains:
         raise ValueError("make_pattern needs at least one domain")
@@ -96,9 +115,18 @@ def make_pattern(context: context, halo_gen: Union[HaloGenerator, Sequence[HaloG
         halo_off_arr = int64_array(np.cumsum([0] + [h.size for h in halo_lists]))
         halo_arr = int64_array(np.concatenate(halo_lists) if halo_lists else np.zeros(0, dtype=np.int64))
     h = C.c_void_p()
-    call("ghexb_pattern_create_unstructured", context._h, len(domains), int64_array([d.domain_id() for d in domains]),
-         int64_array(gid_off), int64_array(gids), int64_array(outer_off), int64_array(outer), halo_off_arr, halo_arr,
-         C.byref(h))
+    common = (context._h, len(domains), int64_array([d.domain_id() for d in domains]), int64_array(gid_off),
+              int64_array(gids), int64_array(outer_off), int64_array(outer), halo_off_arr, halo_arr)
+    if rdig is None:
+        call("ghexb_pattern_create_unstructured", *common, C.byref(h))
+    else:
+        hints = [_hints_of(rdig(d)) for d in domains]
+        for ids_, rem in hints:
+            if len(ids_) != len(rem):
+                raise ValueError("the receive domain ids generator gives domain ids and remote indices of different lengths")
+        hoff = np.cumsum([0] + [len(a) for a, _ in hints])
+        call("ghexb_pattern_create_unstructured_hinted", *common, int64_array(hoff),
+             int64_array([v for a, _ in hints for v in a]), int64_array([v for _, b in hints for v in b]), C.byref(h))
     return Pattern(context, h, domains)
 
 

@@ -126,6 +126,20 @@ int ghexb_pattern_create_unstructured(ghexb_context ctx, int n_domains, const in
     const int64_t* outer_lids, const int64_t* halo_gid_offsets, const int64_t* halo_gids,
     ghexb_pattern* out);
 
+/* Unstructured with a receive domain ids generator: replaces make_pattern<unstructured::grid>(ctx,
+ * halo_gen, recv_domain_ids_gen, domains) (pattern_container.hpp:137-146, unstructured/pattern.hpp:
+ * 371-588). Domains and halo generator as above; for domain k, hint_domain_ids and
+ * hint_remote_indices [hint_offsets[k] .. hint_offsets[k+1]) give, for each halo element in the
+ * halo generator's order, the id of its owner domain and its local index there (the generator's
+ * domain_ids() and remote_indices(); ranks are not needed in one process). Receive lists group
+ * the halo by owner, send lists hold the remote indices in the receiver's order, tags are
+ * (owner id << 7) + receiver id. A remote index must name an inner element of its owner. */
+int ghexb_pattern_create_unstructured_hinted(ghexb_context ctx, int n_domains, const int64_t* domain_ids,
+    const int64_t* gid_offsets, const int64_t* gids, const int64_t* outer_offsets,
+    const int64_t* outer_lids, const int64_t* halo_gid_offsets, const int64_t* halo_gids,
+    const int64_t* hint_offsets, const int64_t* hint_domain_ids, const int64_t* hint_remote_indices,
+    ghexb_pattern* out);
+
 int ghexb_pattern_destroy(ghexb_pattern p);
 
 /* Introspection, mirroring pattern::recv_halos()/send_halos() (structured/pattern.hpp:184-187). */

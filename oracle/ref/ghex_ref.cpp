@@ -325,6 +325,62 @@ int unstructured(int n_dom, const int* ids, const int64_t* gid_off, const int* g
     *seconds = timed(iters, [&] { exchange_all(co, bd, bf); });
     return 0;
 }
+// make_pattern(ctx, halo_gen, recv_domain_ids_gen, domains) (unstructured/pattern.hpp:371-588):
+// the receive domain ids generator is read from tables, one (owner id, remote index) per halo
+// element of every domain in the halo generator's order; the halo generator takes the gid list.
+template<typename T>
+int unstructured_hinted(int n_dom, const int* ids, const int64_t* gid_off, const int* gids, const int64_t* outer_off,
+    const int64_t* outer_lids, const int* halo_gids, int n_halo_gids, const int64_t* hint_off, const int* hint_ids,
+    const int* hint_remote, int levels, void** data, int iters, double* seconds)
+{
+    using dom_t = ghex::unstructured::domain_descriptor<int, int>;
+    using hg_t = ghex::unstructured::halo_generator<int, int>;
+    struct hints
+    {
+        struct halo
+        {
+            std::vector<int> m_ids, m_ranks;
+            std::vector<int> m_remote;
+            const std::vector<int>& domain_ids() const noexcept { return m_ids; }
+            const std::vector<int>& remote_indices() const noexcept { return m_remote; }
+            const std::vector<int>& ranks() const noexcept { return m_ranks; }
+        };
+        std::vector<int> ids;
+        const int64_t* off;
+        const int* hid;
+        const int* hrem;
+        halo operator()(const dom_t& d) const
+        {
+            const int k = (int)(std::find(ids.begin(), ids.end(), d.domain_id()) - ids.begin());
+            halo h;
+            h.m_ids.assign(hid + off[k], hid + off[k + 1]);
+            h.m_remote.assign(hrem + off[k], hrem + off[k + 1]);
+            h.m_ranks.assign(h.m_ids.size(), 0);
+            return h;
+        }
+    };
+    ghex::context ctxt(MPI_COMM_WORLD, true);
+    std::vector<dom_t> doms;
+    for (int i = 0; i < n_dom; ++i)
+    {
+        std::vector<int> g(gids + gid_off[i], gids + gid_off[i + 1]);
+        std::vector<std::size_t> o(outer_lids + outer_off[i], outer_lids + outer_off[i + 1]);
+        doms.emplace_back(ids[i], g.begin(), g.end(), o.begin(), o.end());
+    }
+    hg_t hg = n_halo_gids < 0 ? hg_t{} : hg_t{std::vector<int>(halo_gids, halo_gids + n_halo_gids)};
+    hints rdig{std::vector<int>(ids, ids + n_dom), hint_off, hint_ids, hint_remote};
+    auto pat = ghex::make_pattern<ghex::unstructured::grid>(ctxt, hg, rdig, doms);
+    using dd_t = ghex::unstructured::data_descriptor<ghex::cpu, int, int, T>;
+    std::vector<dd_t> dds;
+    dds.reserve(n_dom);
+    for (int d = 0; d < n_dom; ++d) dds.emplace_back(doms[d], (T*)data[d], (std::size_t)levels, true);
+    std::vector<decltype(pat(dds[0]))> bis;
+    for (auto& dd : dds) bis.push_back(pat(dd));
+    auto co = ghex::make_communication_object<decltype(pat)>(ctxt);
+    *seconds = timed(iters, [&] { co.exchange(bis.begin(), bis.end()).wait(); });
+    return 0;
+}
+
 // One in-place receive communication object per domain (communication_object_ipr.hpp), as in
 // GHEX's test_in_place_receive: every object posts its receives into the field's halo and sends
 // its packed values, then every handle is waited on.
@@ -442,6 +498,28 @@ int ghexref_unstructured_exchange(int n_dom, const int* ids, const int64_t* gid_
     {
         return unstructured(n_dom, ids, gid_off, gids, outer_off, outer_lids, n_fields, dtype, levels, levels_first,
             data, iters, seconds);
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// hint_off[k] .. hint_off[k+1]: domain k's (owner id, remote index) per halo element
+int ghexref_unstructured_exchange_hinted(int n_dom, const int* ids, const int64_t* gid_off, const int* gids,
+    const int64_t* outer_off, const int64_t* outer_lids, const int* halo_gids, int n_halo_gids,
+    const int64_t* hint_off, const int* hint_ids, const int* hint_remote, int dtype, int levels, void** data,
+    int iters, double* seconds)
+{
+    try
+    {
+        if (dtype == F64)
+            return unstructured_hinted<double>(n_dom, ids, gid_off, gids, outer_off, outer_lids, halo_gids,
+                n_halo_gids, hint_off, hint_ids, hint_remote, levels, data, iters, seconds);
+        if (dtype == I32)
+            return unstructured_hinted<int>(n_dom, ids, gid_off, gids, outer_off, outer_lids, halo_gids,
+                n_halo_gids, hint_off, hint_ids, hint_remote, levels, data, iters, seconds);
+        return fail("dtype must be f64 or i32");
     }
     catch (const std::exception& e)
     {

@@ -146,6 +146,31 @@ def unstructured_exchange(domains, fields, iterations: int = 0) -> float:
     return sec.value
 
 
+def unstructured_exchange_hinted(domains, halo_gids, hints, levels: int, arrays, iterations: int = 0) -> float:
+    """The reference's make_pattern with a receive domain ids generator (one communication object,
+    all domains): hints[k] = (owner ids, remote indices) of domain k's halo elements in the halo
+    generator's order; halo_gids: the halo generator's gid list (None: all outer gids); arrays
+    one (n,) or C-ordered (n, levels) array per domain, float64 or int32."""
+    gid_off, gids, outer_off, outer = [0], [], [0], []
+    for _, g, o in domains:
+        gids += list(g)
+        gid_off.append(len(gids))
+        outer += list(o)
+        outer_off.append(len(outer))
+    hoff, hid, hrem = [0], [], []
+    for ids_, rem in hints:
+        hid += list(ids_)
+        hrem += list(rem)
+        hoff.append(len(hid))
+    sec = C.c_double()
+    ptrs = (C.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])
+    _check(lib().ghexref_unstructured_exchange_hinted(
+        len(domains), _ints([d[0] for d in domains]), _i64(gid_off), _ints(gids), _i64(outer_off), _i64(outer),
+        _ints(halo_gids or []), -1 if halo_gids is None else len(halo_gids), _i64(hoff), _ints(hid), _ints(hrem),
+        _CODES[arrays[0].dtype], int(levels), ptrs, iterations, C.byref(sec)))
+    return sec.value
+
+
 def unstructured_exchange_ipr(domains, levels: int, arrays, iterations: int = 0, halo_gids=None) -> float:
     """The reference's in-place receive: one communication_object_ipr per domain, every exchange
     posted, then every handle waited on. arrays: one (n,) or C-ordered (n, levels) array per

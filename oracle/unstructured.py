@@ -12,6 +12,7 @@ Restates, in plain Python and numpy:
     (i << num_bits(#domains)) | id(o), maps ordered by tag;
   * the exchange (data_descriptor get/set, user_concepts.hpp:383-452, with the message buffer
     removed) and its adjoint in receive-map order, column by column;
+  * make_pattern with a receive domain ids generator (unstructured/pattern.hpp:371-588);
   * the in-place receive (unstructured/communication_object_ipr.hpp:105-186): a neighbour's
     message lands on consecutive rows from the first index of its receive list.
 
@@ -94,6 +95,33 @@ def make_pattern(domains: list[Domain], halo_gids=None):
     max_tag = (n << shift) | max(d.id for d in domains)
     return ([[recv[d][t] for t in sorted(recv[d])] for d in range(n)],
             [[send[d][t] for t in sorted(send[d])] for d in range(n)], max_tag)
+
+
+def make_pattern_hinted(domains: list[Domain], hints, halo_gids=None):
+    """make_pattern with a receive domain ids generator (unstructured/pattern.hpp:371-588), one
+    process. hints[i] = (owner ids, remote indices) per halo element of domain i in the halo
+    generator's order. Receive entries group the halo elements by owner (ascending owner id),
+    the owner's send entry lists the remote indices in the receiver's order; tag (owner id << 7) +
+    receiver id; maximum tag (max id << 7) + max id. A remote index must be an inner element."""
+    n = len(domains)
+    idx = {d.id: i for i, d in enumerate(domains)}
+    recv = [dict() for _ in range(n)]
+    send = [dict() for _ in range(n)]
+    for i, d in enumerate(domains):
+        lids = d.make_outer_lids(d.outer_gids if halo_gids is None else halo_gids[i])
+        owners, remote = hints[i]
+        if len(owners) != len(lids) or len(remote) != len(lids):
+            raise ValueError("one receive domain id and remote index per halo element")
+        for lid, o, r in zip(lids, owners, remote):
+            od = domains[idx[o]]
+            if not (0 <= r < len(od.gids)) or r in set(od.outer_lids):
+                raise ValueError(f"remote index {r} of domain {o} is not an inner element")
+            tag = ((o << 7) + d.id) & 0xFFFFFFFF
+            recv[i].setdefault(o, Entry(idx[o], tag)).lids.append(lid)
+            send[idx[o]].setdefault(d.id, Entry(i, tag)).lids.append(r)
+    m = max(d.id for d in domains)
+    return ([[recv[i][k] for k in sorted(recv[i])] for i in range(n)],
+            [[send[i][k] for k in sorted(send[i])] for i in range(n)], (m << 7) + m)
 
 
 def _pairs(recv, send):

@@ -18,6 +18,13 @@
   (seeded permutation, kept in the json under "permuted_halo_gids") orders some receive lists
   against the storage order, so that the received values land on rows first + k, not on the
   receive list's rows;
+* unstructured_hinted.json / unstructured_hinted.npz — the 4-domain case of GHEX's C++
+  unstructured tests with its receive domain ids generator (make_domain, make_halo_gen,
+  recv_domain_ids_gen and the send / receive maps of check_send_halos_indices and
+  check_recv_halos_indices in test/unstructured/unstructured_test_case.hpp and
+  test_user_concepts.cpp, read as text), its fields initialised as initialize_data with 1 level
+  (int32) and 2 levels (float64), exchanged through make_pattern(ctx, hg, rdig, domains) by
+  GHEX's own code;
 * regular_staged.npz — the staged pattern (make_staged_pattern): the 2-D case of
   test/structured/regular/test_simple_regular_domain.cpp (one process: two 8x4 domains stacked
   in y, halo 3, periodic, cells holding their (x, y) coordinates, the test's domain lookup) and a
@@ -86,6 +93,37 @@ def permuted_ipr_halo(doms: dict) -> list:
     raise RuntimeError("no permuted halo order found")
 
 
+def read_hinted_case(reference: Path) -> dict:
+    """Domains, receive domain ids generator tables and expected send / receive maps of the C++
+    unstructured test case."""
+    import re
+    src = (reference / "test" / "unstructured" / "unstructured_test_case.hpp").read_text()
+
+    def block(start, end):
+        b = src[src.index(start):]
+        return b[:b.index(end)]
+
+    md = block("make_domain(domain_id_type id)", "default:")
+    doms = {int(m.group(1)): {"gids": [int(v) for v in m.group(2).split(",")],
+                              "halo_lids": [int(v) for v in m.group(3).split(",")]}
+            for m in re.finditer(r"case\s+(\d+):.*?gids\s*=\s*\{([^}]*)\}.*?halo_lids\s*=\s*\{([^}]*)\}", md, re.S)}
+    rd = block("halo operator()(const domain_descriptor_type& domain) const", "std::vector<int> ranks")
+    hints = {int(m.group(1)): [[int(v) for v in m.group(2).split(",")], [int(v) for v in m.group(3).split(",")]]
+             for m in re.finditer(r"case\s+(\d+):.*?domain_ids\.insert\(domain_ids\.end\(\),\s*\{([^}]*)\}\)"
+                                  r".*?remote_indices\.insert\(remote_indices\.end\(\),\s*\{([^}]*)\}\)", rd, re.S)}
+
+    def ref_maps(fn):
+        b = block(f"void\n{fn}(const pattern_type& p)", "EXPECT")
+        return {int(m.group(1)): {int(a): [int(v) for v in c.split(",")] for a, c in
+                                  re.findall(r"domain_id_type\{(\d+)\},\s*local_indices_type\{([^}]*)\}", m.group(2))}
+                for m in re.finditer(r"case\s+(\d+):(.*?)break;", b, re.S)}
+    if len(doms) != 4 or len(hints) != 4:
+        raise RuntimeError("unexpected test case layout")
+    halo = sorted({v["gids"][l] for v in doms.values() for l in v["halo_lids"]})  # make_halo_gen
+    return {"domains": doms, "hints": hints, "halo_gids": halo, "send": ref_maps("check_send_halos_indices"),
+            "recv": ref_maps("check_recv_halos_indices")}
+
+
 def ipr_fields(doms: dict, levels: int, dtype) -> list:
     """initialize_data of the reference's unstructured test case, levels first."""
     arrays = []
@@ -150,6 +188,23 @@ def main() -> None:
             for d, x in zip(sorted(idoms), arrays):
                 out[f"{tag}out_{levels}_{d}"] = x
     np.savez_compressed(HERE / "unstructured_ipr.npz", **out)
+
+    # ---- receive domain ids generator
+    hc = read_hinted_case(reference)
+    (HERE / "unstructured_hinted.json").write_text(json.dumps(
+        {k: ({str(a): b for a, b in v.items()} if isinstance(v, dict) else v) for k, v in hc.items()}, indent=1))
+    hdoms = hc["domains"]
+    rdoms = [(d, hdoms[d]["gids"], hdoms[d]["halo_lids"]) for d in sorted(hdoms)]
+    out = {}
+    for levels, dtype in ((1, np.int32), (2, np.float64)):
+        arrays = ipr_fields(hdoms, levels, dtype)
+        for d, x in zip(sorted(hdoms), arrays):
+            out[f"in_{levels}_{d}"] = x.copy()
+        reflib.unstructured_exchange_hinted(rdoms, hc["halo_gids"], [hc["hints"][d] for d in sorted(hdoms)], levels,
+                                            arrays)
+        for d, x in zip(sorted(hdoms), arrays):
+            out[f"out_{levels}_{d}"] = x
+    np.savez_compressed(HERE / "unstructured_hinted.npz", **out)
 
     # ---- staged regular pattern
     import regular_cases as rc

@@ -61,3 +61,19 @@ def ipr_arrays() -> dict:
 def staged_arrays() -> dict:
     with np.load(GOLDEN / "regular_staged.npz") as z:
         return {k: z[k] for k in z.files}
+
+
+def hinted_case() -> dict:
+    """The C++ unstructured test case with its receive domain ids generator: domains, hints
+    (owner ids, remote indices), the halo generator's gid list and the expected send / receive
+    maps, all keyed by domain id."""
+    d = json.loads((GOLDEN / "unstructured_hinted.json").read_text())
+    conv = lambda m: {int(k): v for k, v in m.items()}
+    return {"domains": conv(d["domains"]), "hints": conv(d["hints"]), "halo_gids": d["halo_gids"],
+            "send": {int(k): conv(v) for k, v in d["send"].items()},
+            "recv": {int(k): conv(v) for k, v in d["recv"].items()}}
+
+
+def hinted_arrays() -> dict:
+    with np.load(GOLDEN / "unstructured_hinted.npz") as z:
+        return {k: z[k] for k in z.files}

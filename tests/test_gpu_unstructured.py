@@ -121,3 +121,39 @@ def test_cfg2_adjoint_one_launch_bitexact(cuda, levels_first):
     OU.adjoint(recv, send, g32)
     assert sum(bits_equal(t.cpu().numpy(), e) for t, e in zip(t64, g64)) == 0
     assert sum(bits_equal(t.cpu().numpy(), e) for t, e in zip(t32, g32)) == 0
+
+
+@pytest.mark.parametrize("levels", [1, 2])
+def test_receive_domain_ids_generator(levels):
+    """make_pattern(ctx, hg, recv_domain_ids_gen, domains) of GHEX's C++ test case: GHEX's own
+    outputs, through the communication object and an explicit plan in every form; the adjoint
+    (float64) against the oracle's transpose."""
+    hc = G.hinted_case()
+    arrs = G.hinted_arrays()
+    ids = sorted(hc["domains"])
+    ctx = U.make_context()
+    ud = [U.DomainDescriptor(d, hc["domains"][d]["gids"], hc["domains"][d]["halo_lids"]) for d in ids]
+    pat = U.make_pattern(ctx, U.HaloGenerator(hc["halo_gids"]), lambda dom: hc["hints"][dom.domain_id()], ud)
+    host = [arrs[f"in_{levels}_{d}"] for d in ids]
+    tens = [torch.from_numpy(a).to("cuda") for a in host]
+    bis = [pat(U.make_field_descriptor(d, t)) for d, t in zip(ud, tens)]
+    U.make_communication_object(ctx).exchange(bis).wait()
+    expected = [arrs[f"out_{levels}_{d}"] for d in ids]
+    assert sum(bits_equal(t.cpu().numpy(), e) for t, e in zip(tens, expected)) == 0
+    plan = U.make_exchange_plan(ctx, bis)
+    for form in (plan.BATCHED, plan.PER_FIELD, plan.PER_BOX):
+        for t, a in zip(tens, host):
+            t.copy_(torch.from_numpy(a))
+        plan.launch(form)
+        torch.cuda.synchronize()
+        assert sum(bits_equal(t.cpu().numpy(), e) for t, e in zip(tens, expected)) == 0
+    if host[0].dtype == np.float64:
+        odoms = [OU.Domain(d, hc["domains"][d]["gids"], hc["domains"][d]["halo_lids"]) for d in ids]
+        recv, send, _ = OU.make_pattern_hinted(odoms, [hc["hints"][d] for d in ids], [hc["halo_gids"]] * len(ids))
+        adj = [a.copy() for a in host]
+        OU.adjoint(recv, send, adj)
+        for t, a in zip(tens, host):
+            t.copy_(torch.from_numpy(a))
+        plan.adjoint()
+        torch.cuda.synchronize()
+        assert sum(bits_equal(t.cpu().numpy(), e) for t, e in zip(tens, adj)) == 0
