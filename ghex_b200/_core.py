@@ -37,16 +37,25 @@ def _torch():
         return None
 
 
+def check_arch(field: Any, arch) -> None:
+    """arch=Architecture.CPU names a host field: it must be pinned host memory, which the device
+    kernels read and write in place; arch=Architecture.GPU accepts device or pinned host memory."""
+    if arch == Architecture.CPU and array_info(field)["device"] != "host":
+        raise TypeError("arch=Architecture.CPU needs a pinned host array")
+
+
 def array_info(field: Any) -> dict:
     """Pointer, shape, byte strides, dtype code and device of a CUDA array.
 
-    Accepts torch tensors and any object exposing ``__cuda_array_interface__``. Host arrays are
-    rejected: ghex_b200 exchanges device memory only.
+    Accepts torch tensors on a CUDA device, pinned (page-locked) host tensors — the exchange
+    kernels then read and write them in host memory over the host interconnect — and any object
+    exposing ``__cuda_array_interface__``. Pageable host arrays are rejected.
     """
     torch = _torch()
     if torch is not None and isinstance(field, torch.Tensor):
-        if not field.is_cuda:
-            raise TypeError("ghex_b200 exchanges device memory only: the tensor is not on a CUDA device")
+        if not field.is_cuda and not (field.device.type == "cpu" and field.is_pinned()):
+            raise TypeError("ghex_b200 exchanges device memory or pinned host memory: the tensor is a pageable "
+                            "host tensor (use tensor.pin_memory())")
         codes = {torch.float32: _capi.F32, torch.float64: _capi.F64, torch.int32: _capi.I32,
                  torch.int64: _capi.I64, torch.uint8: _capi.U8, torch.uint16: _capi.U16}
         if field.dtype not in codes:
@@ -54,7 +63,7 @@ def array_info(field: Any) -> dict:
         es = field.element_size()
         return {"ptr": field.data_ptr(), "shape": tuple(field.shape),
                 "strides": tuple(s * es for s in field.stride()), "dtype": codes[field.dtype],
-                "itemsize": es, "device": field.device.index or 0}
+                "itemsize": es, "device": (field.device.index or 0) if field.is_cuda else "host"}
     cai = getattr(field, "__cuda_array_interface__", None)
     if cai is None:
         raise TypeError("ghex_b200 exchanges device memory only: expected a CUDA tensor or an object "
@@ -84,7 +93,8 @@ def stream_of(fields: Iterable[Any]):
     torch = _torch()
     for f in fields:
         if torch is not None and isinstance(f, torch.Tensor):
-            return C.c_void_p(torch.cuda.current_stream(f.device).cuda_stream)
+            dev = f.device if f.is_cuda else None  # pinned host tensors: the current device's stream
+            return C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
     return C.c_void_p(0)
 
 

@@ -808,8 +808,32 @@ void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* f
     find_pairs(plan);
 }
 
+void check_accessible(const void* p)
+{
+    cudaPointerAttributes a{};
+    const cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess)
+    {
+        (void)cudaGetLastError();
+        throw error(GHEXB_ERR_INVALID, std::string("field memory: cudaPointerGetAttributes failed: ") +
+                                           cudaGetErrorString(e));
+    }
+    switch (a.type)
+    {
+        case cudaMemoryTypeDevice:
+        case cudaMemoryTypeManaged: return;
+        case cudaMemoryTypeHost:
+            if (a.devicePointer == p) return;
+            throw error(GHEXB_ERR_INVALID, "pinned host memory of a field is not mapped at the same address on the device");
+        default:
+            throw error(GHEXB_ERR_INVALID,
+                "field memory is neither device memory nor pinned (page-locked) host memory");
+    }
+}
+
 void upload_plan(ghexb_plan_s& plan)
 {
+    for (const auto& f : plan.fields) check_accessible(f.data);
     // upload index lists, patch device pointers, upload descriptor tables
     upload(plan.d_idx, plan.idx);
     for (size_t i = 0; i < plan.lists.size(); ++i)
@@ -1569,6 +1593,7 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
         if (plan.lists[i].unit == 16 && (reinterpret_cast<uintptr_t>(data[plan.list_src_slot[i]]) % 16 ||
                                            reinterpret_cast<uintptr_t>(data[plan.list_dst_slot[i]]) % 16))
             throw error(GHEXB_ERR_INVALID, "rebind: 16-byte column alignment of the plan is not met by the new memory");
+    for (int i = 0; i < n; ++i) check_accessible(data[i]);
     for (int i = 0; i < n; ++i) plan.fields[i].data = static_cast<char*>(data[i]);
     for (size_t i = 0; i < plan.boxes.size(); ++i)
     {

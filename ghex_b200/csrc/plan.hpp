@@ -116,6 +116,10 @@ namespace ghexb
 {
 // Builds the host tables of a plan from the fields (plan.cu). Throws ghexb::error.
 void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* fields, int n);
+// Kernels address a field's memory directly: device or managed memory, or pinned host memory
+// mapped at the same address (unified addressing; the kernels then move its bytes over the host
+// interconnect). Anything else is refused before a launch could touch it.
+void check_accessible(const void* p);
 // Uploads the tables and tiles to the device.
 void upload_plan(ghexb_plan_s& plan);
 // build_tables + upload_plan

@@ -13,7 +13,7 @@ from dataclasses import dataclass
 from typing import Any, Sequence, Union
 
 from .._capi import call, int_array, int64_array
-from .._core import (Architecture, FieldDescriptorBase, PatternContainer, array_info, context,
+from .._core import (Architecture, FieldDescriptorBase, PatternContainer, array_info, check_arch, context,
                      make_communication_object, make_context, make_exchange_plan)
 from .regular import _layout_order
 
@@ -121,6 +121,5 @@ class FieldDescriptor(FieldDescriptorBase):
 def make_field_descriptor(domain: DomainDescriptor, field: Any, offsets: Sequence[int], extents: Sequence[int],
                           num_components: int = 1, is_vector: bool = False, *,
                           arch: Architecture = Architecture.GPU) -> FieldDescriptor:
-    if arch == Architecture.CPU:
-        raise TypeError("ghex_b200 exchanges device memory only (arch=Architecture.GPU)")
+    check_arch(field, arch)
     return FieldDescriptor(domain, field, offsets, extents, num_components, is_vector)

@@ -20,7 +20,7 @@ from typing import Any, Sequence, Union
 from .. import _capi
 from .._capi import call, int_array, int64_array
 from .._core import (Architecture, BufferInfo, CommunicationObject, ExchangePlan, FieldDescriptorBase,
-                     PatternContainer, array_info, context, make_communication_object, make_context,
+                     PatternContainer, array_info, check_arch, context, make_communication_object, make_context,
                      make_exchange_plan)
 
 __all__ = ["Architecture", "DomainDescriptor", "HaloGenerator", "make_pattern", "make_staged_pattern",
@@ -253,8 +253,7 @@ def make_field_descriptor(domain_desc: DomainDescriptor, field: Any, offsets: Se
                           extents: Sequence[int], *, arch: Architecture = Architecture.GPU,
                           num_components: int = 1) -> FieldDescriptor:
     """(bindings/python/src/ghex/structured/regular.py:65-97). Only GPU arrays are accepted."""
-    if arch == Architecture.CPU:
-        raise TypeError("ghex_b200 exchanges device memory only (arch=Architecture.GPU)")
+    check_arch(field, arch)
     return FieldDescriptor(domain_desc, field, offsets, extents, num_components)
 
 

@@ -17,7 +17,7 @@ import threading
 from typing import Any, Optional, Sequence, Union
 
 from ._capi import call, int64_array
-from ._core import (Architecture, BufferInfo, CommunicationObject, FieldDescriptorBase, PatternContainer,
+from ._core import (Architecture, BufferInfo, CommunicationObject, FieldDescriptorBase, PatternContainer, check_arch,
                     _flatten, array_info, context, make_communication_object, make_context,
                     make_exchange_plan)
 
@@ -176,8 +176,7 @@ class FieldDescriptor(FieldDescriptorBase):
 
 def make_field_descriptor(domain_desc: DomainDescriptor, field: Any, *,
                           arch: Optional[Architecture] = Architecture.GPU) -> FieldDescriptor:
-    if arch == Architecture.CPU:
-        raise TypeError("ghex_b200 exchanges device memory only (arch=Architecture.GPU)")
+    check_arch(field, arch)
     return FieldDescriptor(domain_desc, field)
 
 

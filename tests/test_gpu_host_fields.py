@@ -1,0 +1,99 @@
+"""Fields in pinned host memory: the device kernels read the source cells from host memory and
+write the halo cells into it, bit-exact against the oracle, for the three grids, through the
+communication object and explicit plans; pageable host memory is refused before any launch."""
+import numpy as np
+import pytest
+import torch
+
+from ghex_b200 import Architecture
+from ghex_b200 import unstructured as U
+from ghex_b200 import workloads as W
+from ghex_b200.structured import cubed_sphere as C
+from ghex_b200.structured import regular as R
+from gpu_helpers import RegularRun, bits_equal
+from oracle import cubed_sphere as OC
+from oracle import unstructured as OU
+
+pytestmark = pytest.mark.gpu
+
+
+def pinned(a: np.ndarray) -> torch.Tensor:
+    src = torch.from_numpy(a)
+    t = torch.empty_strided(tuple(src.shape), tuple(src.stride()), dtype=src.dtype, pin_memory=True)
+    t.copy_(src)
+    assert t.is_pinned() and t.stride() == src.stride()
+    return t
+
+
+def test_regular_pinned_host_fields(cuda):
+    w = W.config1(shape=(40, 30, 12))
+    run = RegularRun(w, cuda)
+    expected = run.oracle()
+    host = {name: [pinned(a) for a in arrays] for name, arrays in run.host.items()}
+    bis = []
+    for halos, specs in w.halo_groups().items():
+        pat = run.patterns[halos]
+        for spec in specs:
+            for dm, d, t in zip(pat.domains, w.domains, host[spec.name]):
+                bis.append(pat(R.make_field_descriptor(dm, t, w.offsets(spec), w.extents(d, spec),
+                                                       arch=Architecture.CPU)))
+    co = R.make_communication_object(run.ctx)
+    co.exchange(bis).wait()
+    for name, ts in host.items():
+        assert sum(bits_equal(t.numpy(), e) for t, e in zip(ts, expected[name])) == 0
+    plan = R.make_exchange_plan(run.ctx, bis)
+    for form in (plan.BATCHED, plan.PER_FIELD, plan.PER_BOX):
+        for name, ts in host.items():
+            for t, a in zip(ts, run.host[name]):
+                t.copy_(torch.from_numpy(a))
+        plan.launch(form)
+        torch.cuda.synchronize()
+        for name, ts in host.items():
+            assert sum(bits_equal(t.numpy(), e) for t, e in zip(ts, expected[name])) == 0
+
+
+def test_unstructured_pinned_host_fields(cuda):
+    w = W.config2(ni=48, nj=64, parts=6, levels=8)
+    host = [w.domain_array(d, np.float64, 1) for d in w.domains]
+    odoms = [OU.Domain(*d) for d in w.domains]
+    recv, send, _ = OU.make_pattern(odoms)
+    expected = [a.copy() for a in host]
+    OU.exchange(recv, send, expected)
+    ctx = U.make_context()
+    ud = [U.DomainDescriptor(*d) for d in w.domains]
+    pat = U.make_pattern(ctx, U.HaloGenerator(), ud)
+    ts = [pinned(a) for a in host]
+    bis = [pat(U.make_field_descriptor(d, t)) for d, t in zip(ud, ts)]
+    U.make_communication_object(ctx).exchange(bis).wait()
+    assert sum(bits_equal(t.numpy(), e) for t, e in zip(ts, expected)) == 0
+
+
+def test_cubed_sphere_pinned_host_vector_field(cuda):
+    w = W.config3(edge=48, levels=4, split=2)
+    host = [w.domain_array(d, 2, 2) for d in w.domains]
+    odoms = [OC.Domain(t, (x0, x1), (y0, y1), w.levels) for t, x0, x1, y0, y1 in w.domains]
+    expected = [a.copy(order="K") for a in host]
+    OC.exchange(OC.make_pattern(w.edge, (w.halo,) * 4, odoms), odoms, expected, [w.offsets()] * len(odoms), w.edge,
+                True)
+    ctx = C.make_context()
+    cube = C.cube(w.edge, w.levels)
+    doms = [C.DomainDescriptor(cube, *b) for b in w.domains]
+    pat = C.make_pattern(ctx, C.HaloGenerator(w.halo), doms)
+    ts = [pinned(a) for a in host]
+    bis = [pat(C.make_field_descriptor(d, t, w.offsets(), a.shape[:3], 2, True)) for d, t, a in zip(doms, ts, host)]
+    C.make_communication_object(ctx).exchange(bis).wait()
+    assert sum(bits_equal(t.numpy(), e) for t, e in zip(ts, expected)) == 0
+
+
+def test_pageable_and_mismatched_memory_refused(cuda):
+    w = W.config0()
+    run = RegularRun(w, cuda)
+    halos, specs = next(iter(w.halo_groups().items()))
+    pat = run.patterns[halos]
+    dm, d = pat.domains[0], w.domains[0]
+    pageable = torch.from_numpy(run.host[specs[0].name][0])
+    with pytest.raises(TypeError, match="pinned"):
+        R.make_field_descriptor(dm, pageable, w.offsets(specs[0]), w.extents(d, specs[0]))
+    with pytest.raises(TypeError, match="pinned host array"):
+        R.make_field_descriptor(dm, run.dev[specs[0].name][0], w.offsets(specs[0]), w.extents(d, specs[0]),
+                                arch=Architecture.CPU)
