@@ -159,3 +159,66 @@ def staged_cases() -> dict:
                         "arrays": arrays3}
     return out
 
+
+
+# ---- 3-D mixed element types (test/structured/regular/test_regular_domain.cpp) ---------------
+MIXED_EXT = (4, 3, 2)                 # local_ext
+MIXED_OFFSET = (3, 3, 3)              # offset (the largest halo)
+MIXED_HALOS_1 = (0, 0, 1, 0, 1, 2)    # pattern 1: fields 1 and 3
+MIXED_HALOS_2 = (2, 2, 2, 2, 2, 2)    # pattern 2: field 2
+
+
+def mixed_3d_domains(ranks: int):
+    """(id, first, last) of the 2 x ranks domains of parameters::parameters (:559-590): rank r
+    owns domains 2r and 2r+1, x blocks 2(r%2) and 2(r%2)+1 of 4, y block r/2, one z block; the
+    global box is 4 x-blocks wide whatever the number of ranks."""
+    ex, ey, ez = MIXED_EXT
+    doms = []
+    for r in range(ranks):
+        for k in range(2):
+            xb = (r % 2) * 2 + k
+            yb = r // 2
+            doms.append((2 * r + k, (xb * ex, yb * ey, 0), ((xb + 1) * ex - 1, (yb + 1) * ey - 1, ez - 1)))
+    g_last = (ex * 4 - 1, ((ranks - 1) // 2 + 1) * ey - 1, ez - 1)
+    return doms, g_last
+
+
+def mixed_3d_field(dom, dtype):
+    """fill_values (:606-620): interior cells hold their global (x, y, z) as 3 components of the
+    element type, every other cell zero; memory x fastest with the 3 components innermost (an
+    array<T, 3> per cell), extents local_ext + 2 * offset."""
+    _, first, _ = dom
+    ext = tuple(MIXED_EXT[k] + 2 * MIXED_OFFSET[k] for k in range(3))
+    buf = np.zeros((ext[2], ext[1], ext[0], 3), dtype=dtype)  # C order: z, y, x, component
+    a = buf.transpose(2, 1, 0, 3)                                # indexed (x, y, z, component)
+    o = MIXED_OFFSET
+    for k in range(3):
+        g = np.arange(MIXED_EXT[k]) + first[k]
+        shape = [1, 1, 1]
+        shape[k] = MIXED_EXT[k]
+        a[o[0]:o[0] + MIXED_EXT[0], o[1]:o[1] + MIXED_EXT[1], o[2]:o[2] + MIXED_EXT[2], k] = g.reshape(shape)
+    return a
+
+
+def mixed_3d_check(a, dom, halos, ranks: int, g_last) -> int:
+    """check_values (:633-690) with all dimensions periodic: every cell of the domain grown by its
+    halos holds its wrapped global coordinate. With one rank the global box is not covered, and
+    the reference skips the low-x halo of the even domain and the high-x halo of the odd one.
+    Returns the number of mismatching cells."""
+    d_id, first, last = dom
+    i = d_id % 2
+    hxl, hxr = halos[0], halos[1]
+    if ranks == 1 and i == 0:
+        hxl = 0
+    if ranks == 1 and i == 1:
+        hxr = 0
+    bad = 0
+    o = MIXED_OFFSET
+    for x in range(first[0] - hxl, last[0] + hxr + 1):
+        for y in range(first[1] - halos[2], last[1] + halos[3] + 1):
+            for z in range(first[2] - halos[4], last[2] + halos[5] + 1):
+                want = [(c % (g_last[k] + 1)) for k, c in enumerate((x, y, z))]
+                v = a[x - first[0] + o[0], y - first[1] + o[1], z - first[2] + o[2]]
+                if [int(t) for t in v] != want:
+                    bad += 1
+    return bad

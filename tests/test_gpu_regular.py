@@ -186,3 +186,35 @@ def test_paired_x_faces_bitexact(cuda, halos, dtype):
     run.reset()
     plan.graph_launch()
     assert run.mismatches(expected) == {}
+
+
+@pytest.mark.parametrize("ranks", [1, 2, 4])
+def test_mixed_3d_known_answers(cuda, ranks):
+    """test_regular_domain.cpp on the device: fields of array<double, 3>, array<float, 3> and
+    array<int, 3> cells (components innermost, x fastest) on two patterns with different halos,
+    all exchanged by one communication object call; bit-exact against the oracle and passing the
+    test's check_values."""
+    import regular_cases as RC
+    from oracle import regular as O
+    doms, g_last = RC.mixed_3d_domains(ranks)
+    ctx = R.make_context()
+    dds = [R.DomainDescriptor(i, (f, l)) for i, f, l in doms]
+    pats = {h: R.make_pattern(ctx, R.HaloGenerator(((0, 0, 0), g_last), [(h[2 * k], h[2 * k + 1]) for k in range(3)],
+                                                   (True, True, True)), dds)
+            for h in (RC.MIXED_HALOS_1, RC.MIXED_HALOS_2)}
+    odoms = [O.Domain(i, f, l) for i, f, l in doms]
+    bis, runs = [], []
+    ext = tuple(RC.MIXED_EXT[k] + 2 * RC.MIXED_OFFSET[k] for k in range(3))
+    for dtype, halos in ((np.float64, RC.MIXED_HALOS_1), (np.float32, RC.MIXED_HALOS_2), (np.int32, RC.MIXED_HALOS_1)):
+        host = [RC.mixed_3d_field(d, dtype) for d in doms]
+        tens = [to_device(a, cuda) for a in host]
+        bis += [pats[halos](R.make_field_descriptor(dd, t, RC.MIXED_OFFSET, ext)) for dd, t in zip(dds, tens)]
+        expected = [a.copy() for a in host]
+        O.exchange(O.make_pattern((0, 0, 0), g_last, halos, (True, True, True), odoms), odoms, expected,
+                   [RC.MIXED_OFFSET] * len(doms))
+        runs.append((halos, tens, expected))
+    R.make_communication_object(ctx).exchange(bis).wait()
+    for halos, tens, expected in runs:
+        got = [t.cpu().numpy() for t in tens]
+        assert sum(bits_equal(g, e) for g, e in zip(got, expected)) == 0
+        assert sum(RC.mixed_3d_check(g, d, halos, ranks, g_last) for g, d in zip(got, doms)) == 0

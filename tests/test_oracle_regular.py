@@ -84,3 +84,17 @@ def test_adjoint_is_transpose():
     lhs = sum(float((a * b).sum()) for a, b in zip(Ex, y))
     rhs = sum(float((a * b).sum()) for a, b in zip(x, ETy))
     assert abs(lhs - rhs) <= 1e-10 * max(1.0, abs(lhs))
+
+
+@pytest.mark.parametrize("ranks", [1, 2, 4])
+def test_mixed_3d_known_answers(ranks):
+    """test_regular_domain.cpp: three fields of array<double|float|int, 3> cells, two patterns with
+    different halos, every cell of the grown domains holding its wrapped global coordinate."""
+    import regular_cases as RC
+    doms, g_last = RC.mixed_3d_domains(ranks)
+    odoms = [O.Domain(i, f, l) for i, f, l in doms]
+    for dtype, halos in ((np.float64, RC.MIXED_HALOS_1), (np.float32, RC.MIXED_HALOS_2), (np.int32, RC.MIXED_HALOS_1)):
+        pat = O.make_pattern((0, 0, 0), g_last, halos, (True, True, True), odoms)
+        arrs = [RC.mixed_3d_field(d, dtype) for d in doms]
+        O.exchange(pat, odoms, arrs, [RC.MIXED_OFFSET] * len(doms))
+        assert sum(RC.mixed_3d_check(a, d, halos, ranks, g_last) for a, d in zip(arrs, doms)) == 0
