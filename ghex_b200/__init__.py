@@ -15,7 +15,8 @@ The shared library is loaded on first use of the API (not by `python -m ghex_b20
 """
 __version__ = "0.1.0"
 
-_CORE_NAMES = ("Architecture", "context", "make_context", "make_communication_object", "make_exchange_plan")
+_CORE_NAMES = ("Architecture", "context", "make_context", "make_communication_object", "make_exchange_plan",
+               "make_bulk_communication_object", "BulkCommunicationObject", "GenericBulkCommunicationObject")
 
 
 def __getattr__(name):

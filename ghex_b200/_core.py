@@ -322,6 +322,59 @@ def make_communication_object(ctx: context) -> CommunicationObject:
     return CommunicationObject(ctx)
 
 
+class BulkCommunicationObject:
+    """bulk_communication_object<rma_range_generator, Pattern, Fields...>
+    (bulk_communication_object.hpp:207-687): fields are registered ahead with add_field /
+    add_fields, init() closes the registration, exchange() exchanges every registered field and
+    returns a handle (wait / is_ready / progress).
+
+    GHEX puts the halos of fields it can address directly (threads and processes of a node,
+    rma_put.hpp:200-240) and sends the rest. Here every field lives in one process and the
+    exchange kernel already copies each halo cell straight from its owner, so the registered
+    fields are exchanged as one work table, built at the first exchange and replayed as one graph
+    launch on the fields' stream."""
+
+    def __init__(self, ctx: context):
+        self.context = ctx
+        self._co = CommunicationObject(ctx)
+        self._bis: list[BufferInfo] = []
+        self._initialized = False
+
+    def add_field(self, buffer_info: BufferInfo) -> None:
+        if self._initialized:
+            raise RuntimeError("error: this CO has been initialized already")
+        self._bis += _flatten((buffer_info,))
+
+    def add_fields(self, *buffer_infos) -> None:
+        for bi in _flatten(buffer_infos):
+            self.add_field(bi)
+
+    def init(self) -> None:
+        if not self._bis:
+            raise RuntimeError("a bulk communication object needs at least one field")
+        self._initialized = True
+
+    def exchange(self) -> Handle:
+        if not self._initialized:
+            self.init()
+        return self._co.exchange(self._bis)
+
+
+class GenericBulkCommunicationObject:
+    """generic_bulk_communication_object (bulk_communication_object.hpp:120-171): a type-erased
+    holder of a bulk communication object, exchanged through the same exchange()."""
+
+    def __init__(self, bulk: BulkCommunicationObject):
+        self._impl = bulk
+
+    def exchange(self) -> Handle:
+        return self._impl.exchange()
+
+
+def make_bulk_communication_object(ctx: context) -> BulkCommunicationObject:
+    return BulkCommunicationObject(ctx)
+
+
 # --------------------------------------------------------------------------------------------
 # explicit plans (no reference counterpart): batched / per-field / per-box forms, graph,
 # adjoint, autotuning

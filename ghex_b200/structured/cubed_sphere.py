@@ -14,11 +14,11 @@ from typing import Any, Sequence, Union
 
 from .._capi import call, int_array, int64_array
 from .._core import (Architecture, FieldDescriptorBase, PatternContainer, array_info, check_arch, context,
-                     make_communication_object, make_context, make_exchange_plan)
+                     make_bulk_communication_object, make_communication_object, make_context, make_exchange_plan)
 from .regular import _layout_order
 
 __all__ = ["cube", "DomainDescriptor", "HaloGenerator", "make_pattern", "make_field_descriptor",
-           "make_communication_object", "make_context", "make_exchange_plan"]
+           "make_communication_object", "make_bulk_communication_object", "make_context", "make_exchange_plan"]
 
 
 @dataclass(frozen=True)

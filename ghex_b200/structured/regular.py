@@ -20,12 +20,12 @@ from typing import Any, Sequence, Union
 from .. import _capi
 from .._capi import call, int_array, int64_array
 from .._core import (Architecture, BufferInfo, CommunicationObject, ExchangePlan, FieldDescriptorBase,
-                     PatternContainer, array_info, check_arch, context, make_communication_object, make_context,
+                     PatternContainer, array_info, check_arch, context, make_bulk_communication_object, make_communication_object, make_context,
                      make_exchange_plan)
 
 __all__ = ["Architecture", "DomainDescriptor", "HaloGenerator", "make_pattern", "make_staged_pattern",
            "make_field_descriptor",
-           "wrap_field", "make_communication_object", "make_context", "make_exchange_plan", "ExchangePlan",
+           "wrap_field", "make_communication_object", "make_bulk_communication_object", "make_context", "make_exchange_plan", "ExchangePlan",
            "CommunicationObject", "BufferInfo"]
 
 

@@ -14,15 +14,16 @@ from __future__ import annotations
 
 import ctypes as C
 import threading
+import weakref
 from typing import Any, Optional, Sequence, Union
 
 from ._capi import call, int64_array
 from ._core import (Architecture, BufferInfo, CommunicationObject, FieldDescriptorBase, PatternContainer, check_arch,
-                    _flatten, array_info, context, make_communication_object, make_context,
+                    _flatten, array_info, context, make_bulk_communication_object, make_communication_object, make_context,
                     make_exchange_plan)
 
 __all__ = ["DomainDescriptor", "HaloGenerator", "make_pattern", "make_field_descriptor", "wrap_field",
-           "make_communication_object", "make_communication_object_ipr", "make_context", "make_exchange_plan"]
+           "make_communication_object", "make_bulk_communication_object", "make_communication_object_ipr", "make_context", "make_exchange_plan"]
 
 
 class DomainDescriptor:
@@ -217,13 +218,14 @@ class _InPlaceGroup:
 
     @staticmethod
     def of(ctx: context, pattern: "Pattern") -> "_InPlaceGroup":
+        """The group of `pattern` in `ctx`, made on first use and dropped with the pattern."""
         with _groups_lock:
-            groups = ctx.__dict__.setdefault("_in_place_groups", {})
-            entry = groups.get(id(pattern))
-            if entry is None or entry[0] is not pattern:
-                entry = (pattern, _InPlaceGroup(ctx, pattern))
-                groups[id(pattern)] = entry
-            return entry[1]
+            groups = ctx.__dict__.setdefault("_in_place_groups", weakref.WeakKeyDictionary())
+            group = groups.get(pattern)
+            if group is None:
+                group = _InPlaceGroup(ctx, pattern)
+                groups[pattern] = group
+            return group
 
     def post(self, bis: list) -> _InPlaceRound:
         with self.cond:
