@@ -96,6 +96,8 @@ SIGNATURES = {
     "ghexb_field_wrap": [_vp, _i64, _i, _vp, _i, _pi, _pi, _pi, _pi64, _i, _i, C.POINTER(_vp)],
     "ghexb_field_wrap_unstructured": [_vp, _i64, _i, _vp, _i64, _i, _i64, C.POINTER(_vp)],
     "ghexb_field_destroy": [_vp],
+    "ghexb_host_register": [_vp, C.c_size_t, _pi],
+    "ghexb_host_unregister": [_vp],
     "ghexb_co_create": [_vp, C.POINTER(_vp)],
     "ghexb_co_create_ipr": [_vp, C.POINTER(_vp)],
     "ghexb_co_destroy": [_vp],

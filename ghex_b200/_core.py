@@ -9,6 +9,8 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
+import os
+import threading
 from typing import Any, Iterable, Sequence
 
 from . import _capi
@@ -16,7 +18,9 @@ from ._capi import call
 
 
 class Architecture(enum.Enum):
-    """Where a field lives (bindings/python/src/ghex/util.py:22-24). Only GPU is supported."""
+    """Where a field lives (bindings/python/src/ghex/util.py:22-24). Both are exchanged by the
+    device kernels: GPU fields in device memory, CPU fields in host memory over the host
+    interconnect."""
 
     CPU = "cpu"
     GPU = "gpu"
@@ -38,24 +42,26 @@ def _torch():
 
 
 def check_arch(field: Any, arch) -> None:
-    """arch=Architecture.CPU names a host field: it must be pinned host memory, which the device
-    kernels read and write in place; arch=Architecture.GPU accepts device or pinned host memory."""
+    """arch=Architecture.CPU names a host field (host memory, read and written in place by the
+    device kernels); arch=Architecture.GPU, or None as in GHEX's bindings, accepts either."""
     if arch == Architecture.CPU and array_info(field)["device"] != "host":
-        raise TypeError("arch=Architecture.CPU needs a pinned host array")
+        raise TypeError("arch=Architecture.CPU needs a host array")
 
 
 def array_info(field: Any) -> dict:
-    """Pointer, shape, byte strides, dtype code and device of a CUDA array.
+    """Pointer, shape, byte strides, dtype code and device of an array.
 
-    Accepts torch tensors on a CUDA device, pinned (page-locked) host tensors — the exchange
-    kernels then read and write them in host memory over the host interconnect — and any object
-    exposing ``__cuda_array_interface__``. Pageable host arrays are rejected.
+    Accepts torch tensors on a CUDA device and any object exposing ``__cuda_array_interface__``
+    (device memory), and host memory: torch CPU tensors and objects exposing
+    ``__array_interface__`` (numpy). Host fields are exchanged in place by the device kernels over
+    the host interconnect once a field descriptor has page-locked their pages (``host_pages`` in
+    the result); pinned allocations are recognised there page by page (a tensor's is_pinned()
+    looks at its first byte only, which may sit on a page locked for a neighbouring array).
     """
     torch = _torch()
     if torch is not None and isinstance(field, torch.Tensor):
-        if not field.is_cuda and not (field.device.type == "cpu" and field.is_pinned()):
-            raise TypeError("ghex_b200 exchanges device memory or pinned host memory: the tensor is a pageable "
-                            "host tensor (use tensor.pin_memory())")
+        if not field.is_cuda and field.device.type != "cpu":
+            raise TypeError(f"unsupported tensor device {field.device}")
         codes = {torch.float32: _capi.F32, torch.float64: _capi.F64, torch.int32: _capi.I32,
                  torch.int64: _capi.I64, torch.uint8: _capi.U8, torch.uint16: _capi.U16}
         if field.dtype not in codes:
@@ -63,24 +69,116 @@ def array_info(field: Any) -> dict:
         es = field.element_size()
         return {"ptr": field.data_ptr(), "shape": tuple(field.shape),
                 "strides": tuple(s * es for s in field.stride()), "dtype": codes[field.dtype],
-                "itemsize": es, "device": (field.device.index or 0) if field.is_cuda else "host"}
+                "itemsize": es, "device": (field.device.index or 0) if field.is_cuda else "host",
+                "host_pages": not field.is_cuda}
     cai = getattr(field, "__cuda_array_interface__", None)
     if cai is None:
-        raise TypeError("ghex_b200 exchanges device memory only: expected a CUDA tensor or an object "
-                        "with __cuda_array_interface__")
-    typestr = cai["typestr"]
+        hai = getattr(field, "__array_interface__", None)
+        if hai is None:
+            raise TypeError("expected a CUDA tensor, a host tensor or array, or an object with "
+                            "__cuda_array_interface__ / __array_interface__")
+        info = _interface_info(hai)
+        info.update(device="host", host_pages=True)
+        return info
+    info = _interface_info(cai)
+    info["device"] = None
+    return info
+
+
+def _interface_info(iface: dict) -> dict:
+    typestr = iface["typestr"]
     if typestr not in _TYPESTR:
         raise TypeError(f"unsupported dtype {typestr}")
-    shape = tuple(cai["shape"])
+    shape = tuple(iface["shape"])
     itemsize = int(typestr[2:])
-    strides = cai.get("strides")
+    strides = iface.get("strides")
     if strides is None:  # C-contiguous
         strides, s = [], itemsize
         for n in reversed(shape):
             strides.insert(0, s)
             s *= n
-    return {"ptr": int(cai["data"][0]), "shape": shape, "strides": tuple(strides),
-            "dtype": _TYPESTR[typestr], "itemsize": itemsize, "device": None}
+    return {"ptr": int(iface["data"][0]), "shape": shape, "strides": tuple(strides),
+            "dtype": _TYPESTR[typestr], "itemsize": itemsize}
+
+
+class _HostPages:
+    """Page-locked ranges of ordinary host memory that fields live in, registered with
+    ghexb_host_register page-aligned and reference-counted, so that fields sharing pages (views of
+    one buffer, small arrays next to each other) share registrations and a range is unregistered
+    when its last field is gone."""
+
+    def __init__(self):
+        self.lock = threading.Lock()
+        self.regs: dict[int, list] = {}       # start -> [end, references, owned]
+        self.page_of: dict[int, int] = {}     # page -> start of the registration holding it
+        self.page = os.sysconf("SC_PAGE_SIZE")
+        self._unregister = _capi.release      # held here: module globals may be gone at exit
+
+    def acquire(self, lo: int, hi: int) -> list[int]:
+        P = self.page
+        p, end = lo // P * P, -(-hi // P) * P
+        held: list[int] = []
+        with self.lock:
+            try:
+                while p < end:
+                    start = self.page_of.get(p)
+                    if start is not None:
+                        self.regs[start][1] += 1
+                        held.append(start)
+                        p = self.regs[start][0]
+                        continue
+                    q = p
+                    while q < end and q not in self.page_of:
+                        q += P
+                    owned = C.c_int()
+                    call("ghexb_host_register", C.c_void_p(p), q - p, C.byref(owned))
+                    self.regs[p] = [q, 1, bool(owned.value)]
+                    for page in range(p, q, P):
+                        self.page_of[page] = p
+                    held.append(p)
+                    p = q
+            except BaseException:
+                self._release(held)
+                raise
+        return held
+
+    def release(self, held: list[int]) -> None:
+        with self.lock:
+            self._release(held)
+
+    def _release(self, held: list[int]) -> None:
+        for start in held:
+            reg = self.regs.get(start)
+            if reg is None:
+                continue
+            reg[1] -= 1
+            if reg[1] == 0:
+                if reg[2]:
+                    self._unregister("ghexb_host_unregister", C.c_void_p(start))
+                for page in range(start, reg[0], self.page):
+                    self.page_of.pop(page, None)
+                del self.regs[start]
+
+
+_host_pages = _HostPages()
+
+
+class _HostRegistration:
+    """The page-locked ranges one field's host memory is held by, released with the field."""
+
+    def __init__(self, info: dict):
+        lo = hi = info["ptr"]
+        for n, st in zip(info["shape"], info["strides"]):
+            if n == 0:
+                self.held = []
+                return
+            lo += min(0, (n - 1) * st)
+            hi += max(0, (n - 1) * st)
+        self.held = _host_pages.acquire(lo, hi + info["itemsize"])
+
+    def __del__(self, _pages=_host_pages):
+        _pages.release(getattr(self, "held", []))
+        self.held = []
 
 
 def _layout_of(a: Any) -> tuple:
@@ -223,6 +321,10 @@ class FieldDescriptorBase:
     def __init__(self, array: Any):
         self.array = array
         self._handles: dict[int, C.c_void_p] = {}
+        info = array_info(array)
+        if info.get("host_pages"):
+            # ordinary host memory: page-locked and mapped for the device while this field lives
+            self._host = _HostRegistration(info)
 
     def domain_key(self) -> Any:  # pragma: no cover - abstract
         raise NotImplementedError

@@ -454,6 +454,45 @@ int ghexb_field_destroy(ghexb_field f)
     return GHEXB_OK;
 }
 
+// ---- host memory for fields --------------------------------------------------------------------
+int ghexb_host_register(void* ptr, size_t bytes, int* owned)
+{
+    return guarded([&] {
+        require(ptr && bytes > 0 && owned, "null argument");
+        cudaPointerAttributes a{};
+        ghexb::check_cuda(cudaPointerGetAttributes(&a, ptr), "cudaPointerGetAttributes");
+        if (a.type == cudaMemoryTypeHost)
+        {
+            // page-locked already (a pinned allocation, or a registration of other code): every
+            // page must be, at its own address
+            *owned = 0;
+            ghexb::check_accessible(ptr, bytes);
+            return;
+        }
+        ghexb::check_cuda(cudaHostRegister(ptr, bytes, cudaHostRegisterMapped | cudaHostRegisterPortable),
+            "cudaHostRegister");
+        *owned = 1;
+        try
+        {
+            ghexb::check_accessible(ptr);
+            ghexb::check_accessible(static_cast<char*>(ptr) + bytes - 1);
+        }
+        catch (...)
+        {
+            (void)cudaHostUnregister(ptr);
+            throw;
+        }
+    });
+}
+
+int ghexb_host_unregister(void* ptr)
+{
+    return guarded([&] {
+        require(ptr != nullptr, "null argument");
+        ghexb::check_cuda(cudaHostUnregister(ptr), "cudaHostUnregister");
+    });
+}
+
 // ---- communication object --------------------------------------------------------------------
 int ghexb_co_create(ghexb_context ctx, ghexb_co* out)
 {

@@ -64,7 +64,7 @@ extern "C" int ghexb_exchange_noalloc(ghexb_context ctx, const ghexb_field* fiel
         // host tables of the batched form at the default tuning
         ghexb_plan_s plan;
         ghexb::build_tables(plan, ctx, fields, n);
-        for (const auto& f : plan.fields) ghexb::check_accessible(f.data);
+        for (const auto& f : plan.fields) ghexb::check_accessible(f.data, ghexb::field_bytes(f));
 
         // layout: index lists | forward tiles (the tiles carry everything else the kernel needs)
         const size_t off_idx = 0;

@@ -808,7 +808,12 @@ void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* f
     find_pairs(plan);
 }
 
-void check_accessible(const void* p)
+namespace
+{
+int64_t field_span(const ghexb_field_s& f);
+
+// memory type of the byte at p; host memory must be mapped at its own address
+cudaMemoryType accessible_type(const void* p)
 {
     cudaPointerAttributes a{};
     const cudaError_t e = cudaPointerGetAttributes(&a, p);
@@ -821,19 +826,33 @@ void check_accessible(const void* p)
     switch (a.type)
     {
         case cudaMemoryTypeDevice:
-        case cudaMemoryTypeManaged: return;
+        case cudaMemoryTypeManaged: return a.type;
         case cudaMemoryTypeHost:
-            if (a.devicePointer == p) return;
-            throw error(GHEXB_ERR_INVALID, "pinned host memory of a field is not mapped at the same address on the device");
+            if (a.devicePointer == p) return a.type;
+            throw error(GHEXB_ERR_INVALID, "page-locked host memory of a field is not mapped at the same address on the device");
         default:
             throw error(GHEXB_ERR_INVALID,
-                "field memory is neither device memory nor pinned (page-locked) host memory");
+                "field memory is neither device memory nor page-locked host memory (a host field's pages must be "
+                "locked for the device: ghexb_host_register)");
     }
+}
+} // namespace
+
+void check_accessible(const void* p) { (void)accessible_type(p); }
+
+void check_accessible(const void* p, size_t bytes)
+{
+    // page-locked host memory is locked page by page, possibly by several registrations: every
+    // page of the range is checked, not only its first byte
+    if (accessible_type(p) != cudaMemoryTypeHost || bytes <= 1) return;
+    const char* c = static_cast<const char*>(p);
+    for (size_t off = 4096 - reinterpret_cast<uintptr_t>(c) % 4096; off < bytes; off += 4096) (void)accessible_type(c + off);
+    (void)accessible_type(c + bytes - 1);
 }
 
 void upload_plan(ghexb_plan_s& plan)
 {
-    for (const auto& f : plan.fields) check_accessible(f.data);
+    for (const auto& f : plan.fields) check_accessible(f.data, (size_t)(field_span(f) * f.esize));
     // upload index lists, patch device pointers, upload descriptor tables
     upload(plan.d_idx, plan.idx);
     for (size_t i = 0; i < plan.lists.size(); ++i)
@@ -885,6 +904,8 @@ void check_offset(const ghexb_field_s& f, const char* base, int64_t rel, int64_t
                                          " outside the field's memory span " + std::to_string(span));
 }
 } // namespace
+
+size_t field_bytes(const ghexb_field_s& f) { return (size_t)(field_span(f) * f.esize); }
 
 namespace
 {
@@ -1593,7 +1614,7 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
         if (plan.lists[i].unit == 16 && (reinterpret_cast<uintptr_t>(data[plan.list_src_slot[i]]) % 16 ||
                                            reinterpret_cast<uintptr_t>(data[plan.list_dst_slot[i]]) % 16))
             throw error(GHEXB_ERR_INVALID, "rebind: 16-byte column alignment of the plan is not met by the new memory");
-    for (int i = 0; i < n; ++i) check_accessible(data[i]);
+    for (int i = 0; i < n; ++i) check_accessible(data[i], (size_t)(field_span(plan.fields[i]) * plan.fields[i].esize));
     for (int i = 0; i < n; ++i) plan.fields[i].data = static_cast<char*>(data[i]);
     for (size_t i = 0; i < plan.boxes.size(); ++i)
     {

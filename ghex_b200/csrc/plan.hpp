@@ -120,6 +120,10 @@ void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* f
 // mapped at the same address (unified addressing; the kernels then move its bytes over the host
 // interconnect). Anything else is refused before a launch could touch it.
 void check_accessible(const void* p);
+// ... every page of [p, p + bytes) when it is host memory
+void check_accessible(const void* p, size_t bytes);
+// bytes from a field's data pointer to one past its last element
+size_t field_bytes(const ghexb_field_s& f);
 // Uploads the tables and tiles to the device.
 void upload_plan(ghexb_plan_s& plan);
 // build_tables + upload_plan

@@ -178,6 +178,18 @@ int ghexb_field_wrap_unstructured(ghexb_pattern p, int64_t domain_id, int dtype,
 
 int ghexb_field_destroy(ghexb_field f);
 
+/* ---- host memory for fields (no GHEX counterpart: GHEX exchanges CPU fields on the CPU). A field
+ * may live in host memory that the device addresses at the same address: pinned memory
+ * (cudaHostAlloc) as it is, ordinary pageable memory after ghexb_host_register, which page-locks
+ * [ptr, ptr + bytes) and maps it for the device (cudaHostRegister, mapped and portable). The
+ * exchange kernels then read and write such fields in place over the host interconnect. *owned is
+ * 1 when the call registered the range (undo with ghexb_host_unregister(ptr)) and 0 when the range
+ * was page-locked already (every page is then checked). Fails with GHEXB_ERR_INVALID when the
+ * device cannot address the memory at its host address. Plans check every page of a host field
+ * and refuse memory that the device cannot address, before any launch. */
+int ghexb_host_register(void* ptr, size_t bytes, int* owned);
+int ghexb_host_unregister(void* ptr);
+
 /* ---- communication object: replaces make_communication_object<Pattern>(ctx)
  * (communication_object.hpp:653-660), exchange(buffer_info...) (:233-240) and
  * communication_handle::wait/is_ready (:627-640). The exchange of the given fields is ordered on

@@ -1,6 +1,8 @@
-"""Fields in pinned host memory: the device kernels read the source cells from host memory and
-write the halo cells into it, bit-exact against the oracle, for the three grids, through the
-communication object and explicit plans; pageable host memory is refused before any launch."""
+"""Fields in host memory: the device kernels read the source cells from host memory and write
+the halo cells into it, bit-exact against the oracle, for the three grids, through the
+communication object and explicit plans; pinned tensors as they are, ordinary numpy arrays and
+torch CPU tensors page-locked by their field descriptors (the reference's own Python test runs on
+numpy arrays this way)."""
 import numpy as np
 import pytest
 import torch
@@ -85,15 +87,75 @@ def test_cubed_sphere_pinned_host_vector_field(cuda):
     assert sum(bits_equal(t.numpy(), e) for t, e in zip(ts, expected)) == 0
 
 
-def test_pageable_and_mismatched_memory_refused(cuda):
+def test_pageable_host_fields(cuda):
+    """Ordinary numpy arrays and torch CPU tensors: the field descriptor page-locks their memory
+    (shared pages reference-counted) and the exchange runs on it in place."""
+    w = W.config1(shape=(40, 30, 12))
+    run = RegularRun(w, cuda)
+    expected = run.oracle()
+    host = {name: [np.array(a, order="K") if i % 2 else torch.from_numpy(np.array(a, order="K"))
+                   for i, a in enumerate(arrays)] for name, arrays in run.host.items()}
+    bis = []
+    for halos, specs in w.halo_groups().items():
+        pat = run.patterns[halos]
+        for spec in specs:
+            for dm, d, t in zip(pat.domains, w.domains, host[spec.name]):
+                bis.append(pat(R.make_field_descriptor(dm, t, w.offsets(spec), w.extents(d, spec),
+                                                       arch=Architecture.CPU)))
+    for _ in range(2):
+        R.make_communication_object(run.ctx).exchange(bis).wait()
+    for name, ts in host.items():
+        got = [t.numpy() if isinstance(t, torch.Tensor) else t for t in ts]
+        assert sum(bits_equal(g, e) for g, e in zip(got, expected[name])) == 0
+
+
+def test_numpy_fields_as_in_the_reference_python_test(cuda):
+    """test/bindings/python/test_structured_pattern.py with every process's domain in this one:
+    2x2x1 domains of a (2*26) x 26 x 1 grid, halos ((2, 1), (1, 1), (0, 0)), periodic in x and y,
+    three float64 numpy fields (x fastest) holding their domain's grid coordinate along one
+    dimension each, and a field holding the domain's id; after one exchange every halo cell inside
+    the global grid holds the coordinates and id of the domain that owns it."""
+    nx, ny, nz = 2 * 26, 26, 1
+    dims = (2, 2, 1)
+    halos = ((2, 1), (1, 1), (0, 0))
+    periodic = (True, True, False)
+    spec = W.regular_decomposition((nx, ny, nz), dims)
+    coords = {i: (f[0] // (nx // dims[0]), f[1] // (ny // dims[1]), 0) for i, f, _ in spec}
+    ctx = R.make_context()
+    doms = [R.DomainDescriptor(i, (f, l)) for i, f, l in spec]
+    pat = R.make_pattern(ctx, R.HaloGenerator(((0, 0, 0), (nx - 1, ny - 1, nz - 1)), halos, periodic), doms)
+    fields, bis = {}, []
+    for d, (i, f, l) in zip(doms, spec):
+        ext = tuple(l[k] - f[k] + 1 + halos[k][0] + halos[k][1] for k in range(3))
+        off = tuple(h[0] for h in halos)
+        arrs = [np.zeros(ext, dtype=np.float64, order="F") for _ in range(4)]
+        inner = tuple(slice(off[k], off[k] + l[k] - f[k] + 1) for k in range(3))
+        for k in range(3):
+            arrs[k][inner] = coords[i][k]
+        arrs[3][inner] = i
+        fields[i] = (f, arrs, off)
+        bis += [pat(R.make_field_descriptor(d, a, off, ext)) for a in arrs]
+    R.make_communication_object(ctx).exchange(bis).wait()
+    owner_of = {c: i for i, c in coords.items()}
+    box = {i: (f, l) for i, f, l in spec}
+    for i, (f, arrs, off) in fields.items():
+        for m in np.ndindex(*arrs[0].shape):
+            g = tuple(m[k] - off[k] + f[k] for k in range(3))
+            if not all(0 <= g[k] < (nx, ny, nz)[k] for k in range(3)):
+                continue
+            c = tuple(int(arrs[k][m]) for k in range(3))
+            owner = owner_of[c]
+            lo, hi = box[owner]
+            assert all(lo[k] <= g[k] <= hi[k] for k in range(3)), (i, m, c)
+            assert int(arrs[3][m]) == owner
+
+
+def test_device_array_with_cpu_arch_refused(cuda):
     w = W.config0()
     run = RegularRun(w, cuda)
     halos, specs = next(iter(w.halo_groups().items()))
     pat = run.patterns[halos]
     dm, d = pat.domains[0], w.domains[0]
-    pageable = torch.from_numpy(run.host[specs[0].name][0])
-    with pytest.raises(TypeError, match="pinned"):
-        R.make_field_descriptor(dm, pageable, w.offsets(specs[0]), w.extents(d, specs[0]))
-    with pytest.raises(TypeError, match="pinned host array"):
+    with pytest.raises(TypeError, match="host array"):
         R.make_field_descriptor(dm, run.dev[specs[0].name][0], w.offsets(specs[0]), w.extents(d, specs[0]),
                                 arch=Architecture.CPU)
