@@ -1385,7 +1385,13 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
         std::vector<gtile> all;
         for (const auto& g : plan.cells)
         {
-            const uint32_t gc = (uint32_t)(gather_per_thread(g.nimg) * k_gather_block);
+            // tiles of short rows shrink as the forward's do (row_cap): rows along the first axis
+            // only where the owner and every image are contiguous along it
+            bool contiguous = g.o[0] == 1;
+            for (int k = 0; k < g.nimg && contiguous; ++k) contiguous = g.img[k].t[0] == 1 || g.img[k].t[0] == -1;
+            const int64_t w = (contiguous ? g.n[0] : 1) * (int64_t)g.esize;
+            const int64_t full = (int64_t)gather_per_thread(g.nimg) * k_gather_block;
+            const uint32_t gc = (uint32_t)std::max<int64_t>(k_gather_block, std::min<int64_t>(full, full * w / (w + 32)));
             const auto& of = plan.fields[g.own_slot];
             const fast_div f0 = fast_div::make((uint32_t)g.n[0]), f1 = fast_div::make((uint32_t)g.n[1]);
             const uint32_t n = (uint32_t)((int64_t)g.n[0] * g.n[1] * g.n[2]);
