@@ -6,6 +6,8 @@ neighbour's halo with one read and one write, in a single kernel that walks a wo
 table built once per field set (libghex_b200.so, C ABI in include/ghex_b200.h).
 
 Modules:
+    ghex_b200.context                  drop-in for ghex.context (make_context)
+    ghex_b200.util                     drop-in for ghex.util (Architecture)
     ghex_b200.structured.regular       drop-in for ghex.structured.regular
     ghex_b200.structured.cubed_sphere  the cubed-sphere grids of GHEX's C++ API
     ghex_b200.unstructured             drop-in for ghex.unstructured
@@ -15,7 +17,7 @@ The shared library is loaded on first use of the API (not by `python -m ghex_b20
 """
 __version__ = "0.1.0"
 
-_CORE_NAMES = ("Architecture", "context", "make_context", "make_communication_object", "make_exchange_plan",
+_CORE_NAMES = ("Architecture", "make_context", "make_communication_object", "make_exchange_plan",
                "make_bulk_communication_object", "BulkCommunicationObject", "GenericBulkCommunicationObject")
 
 

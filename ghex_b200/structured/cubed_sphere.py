@@ -17,7 +17,7 @@ from .._core import (Architecture, FieldDescriptorBase, PatternContainer, array_
                      make_bulk_communication_object, make_communication_object, make_context, make_exchange_plan)
 from .regular import _layout_order
 
-__all__ = ["cube", "DomainDescriptor", "HaloGenerator", "make_pattern", "make_field_descriptor",
+__all__ = ["cube", "DomainDescriptor", "HaloGenerator", "make_pattern", "make_field_descriptor", "wrap_field",
            "make_communication_object", "make_bulk_communication_object", "make_context", "make_exchange_plan"]
 
 
@@ -123,3 +123,7 @@ def make_field_descriptor(domain: DomainDescriptor, field: Any, offsets: Sequenc
                           arch: Architecture = Architecture.GPU) -> FieldDescriptor:
     check_arch(field, arch)
     return FieldDescriptor(domain, field, offsets, extents, num_components, is_vector)
+
+
+def wrap_field(*args, **kwargs) -> FieldDescriptor:
+    return make_field_descriptor(*args, **kwargs)

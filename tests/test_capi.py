@@ -82,3 +82,20 @@ def test_field_wrap_checks():
     _capi.call("ghexb_field_wrap", p._h, 0, _capi.F64, C.c_void_p(4096), 1, _capi.int_array([1]),
                _capi.int_array([7]), None, None, 1, 0, C.byref(f))
     _capi.lib.ghexb_field_destroy(f)
+
+
+def test_ghex_module_names():
+    """The module layout of GHEX's Python package: ghex.context.make_context, ghex.util.Architecture,
+    and make_communication_object / make_pattern / make_field_descriptor in each grid module."""
+    from ghex_b200 import unstructured
+    from ghex_b200.context import context, make_context
+    from ghex_b200.structured import cubed_sphere, regular
+    from ghex_b200.util import Architecture
+    ctx = make_context(None, False, device=0)
+    assert isinstance(ctx, context) and ctx.rank() == 0 and ctx.size() == 1
+    assert {a.name for a in Architecture} == {"CPU", "GPU"}
+    for mod in (regular, cubed_sphere, unstructured):
+        for name in ("make_communication_object", "make_pattern", "make_field_descriptor", "wrap_field",
+                     "make_bulk_communication_object", "make_exchange_plan"):
+            assert callable(getattr(mod, name)), (mod.__name__, name)
+    assert callable(regular.make_staged_pattern) and callable(unstructured.make_communication_object_ipr)
