@@ -534,7 +534,7 @@ def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline
     """Batched and per-field exchange of one workload (plus the adjoint of the differentiable one)."""
     case = Case(cfg, dev, dev.index)
     plan = case.plan
-    tuning = plan.autotune(repeats=5) if autotune else plan.info()
+    tuning = plan.autotune(repeats=15) if autotune else plan.info()
     s = timer.stream.cuda_stream
     ms_b = timer(lambda: plan.graph_launch(s), steps, warmup)
     ms_f = timer(lambda: plan.launch(plan.PER_FIELD, s), max(10, steps // 2), warmup)
@@ -562,9 +562,9 @@ def measure_staged(dev, timer, peak, steps, warmup, autotune=True, baseline=True
     case = Case("cfg1_staged", dev, dev.index)
     s = timer.stream.cuda_stream
     if autotune:
-        case.plan.autotune(repeats=5)
+        case.plan.autotune(repeats=15)
         for pl in case.stage_plans:
-            pl.autotune(repeats=5)
+            pl.autotune(repeats=15)
     ms_staged = timer(lambda: [pl.graph_launch(s) for pl in case.stage_plans], steps, warmup)
     ms_full = timer(lambda: case.plan.graph_launch(s), steps, warmup)
     out = {"workload": case.w.name + ", staged pattern", "algorithmic_bytes": case.alg, "dtype": case.dtype,
@@ -649,7 +649,7 @@ def main():
         print(json.dumps({"profile": args.profile, "config": case.w.name, "launches": args.warmup + args.steps,
                           "plan": plan.info()}), flush=True)
         return
-    tuning = plan.info() if args.no_autotune else plan.autotune(repeats=5)
+    tuning = plan.info() if args.no_autotune else plan.autotune(repeats=15)
     info = plan.info()
     alg = case.alg
     stream = torch.cuda.Stream(device=dev)

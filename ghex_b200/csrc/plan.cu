@@ -1695,7 +1695,9 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
             plan.per_thread = c.k, plan.block = c.block, plan.use_pairs = c.pairs;
             retile(plan, stream);
             launch_plan(plan, GHEXB_FORM_BATCHED, stream); // warm-up
-            float total = 0.f;
+            // the median of the repeats: one slow launch (another process, a clock change) must
+            // not decide the choice
+            std::vector<float> times;
             for (int r = 0; r < repeats; ++r)
             {
                 check_cuda(launch_l2_flush(flush, flush_bytes / 16, sink, fgrid, stream), "l2 flush");
@@ -1705,9 +1707,11 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
                 check_cuda(cudaEventSynchronize(e1), "cudaEventSynchronize");
                 float ms = 0.f;
                 check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
-                total += ms;
+                times.push_back(ms);
             }
-            if (total < best) best = total, bestc = c;
+            std::nth_element(times.begin(), times.begin() + times.size() / 2, times.end());
+            const float med = times[times.size() / 2];
+            if (med < best) best = med, bestc = c;
         }
     }
     catch (...)
