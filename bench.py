@@ -530,29 +530,12 @@ def e2e_host_ms(case, steps, warmup, world, dev):
     return max_over_ranks(ms, world, dev), case.alg // 2, case.alg // 2, ok
 
 
-def tune(plan, timer, s, steps: int = 20) -> dict:
-    """The tuning search of the plan's autotuner (elements per thread x threads per CTA x x-face
-    pairs on or off), timed with this benchmark's own protocol (cold L2 before every launch, CUDA
-    events, the batched form) so that the pick is the fastest under the measurement it serves."""
-    has_pairs = plan.info()["pairs"] > 0
-    best = None
-    for k in (4, 8, 16):
-        for b in (128, 256, 512):
-            for p in ((0, 1) if has_pairs else (0,)):
-                plan.set_tuning(k, b, p)
-                ms = timer(lambda: plan.launch(plan.BATCHED, s), steps, 3)
-                if best is None or ms < best[0]:
-                    best = (ms, k, b, p)
-    plan.set_tuning(best[1], best[2], best[3])
-    return plan.info()
-
-
 def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline=True) -> dict:
     """Batched and per-field exchange of one workload (plus the adjoint of the differentiable one)."""
     case = Case(cfg, dev, dev.index)
     plan = case.plan
     s = timer.stream.cuda_stream
-    tuning = tune(plan, timer, s) if autotune else plan.info()
+    tuning = plan.autotune(repeats=20, stream=s) if autotune else plan.info()
     ms_b = timer(lambda: plan.graph_launch(s), steps, warmup)
     ms_f = timer(lambda: plan.launch(plan.PER_FIELD, s), max(10, steps // 2), warmup)
     out = {"workload": case.w.name, "algorithmic_bytes": case.alg, "dtype": case.dtype,
@@ -579,9 +562,9 @@ def measure_staged(dev, timer, peak, steps, warmup, autotune=True, baseline=True
     case = Case("cfg1_staged", dev, dev.index)
     s = timer.stream.cuda_stream
     if autotune:
-        tune(case.plan, timer, s)
+        case.plan.autotune(repeats=20, stream=s)
         for pl in case.stage_plans:
-            tune(pl, timer, s)
+            pl.autotune(repeats=20, stream=s)
     ms_staged = timer(lambda: [pl.graph_launch(s) for pl in case.stage_plans], steps, warmup)
     ms_full = timer(lambda: case.plan.graph_launch(s), steps, warmup)
     out = {"workload": case.w.name + ", staged pattern", "algorithmic_bytes": case.alg, "dtype": case.dtype,
@@ -673,7 +656,7 @@ def main():
     timer = Timer(stream, flush, world, dev)
     peak, peak_kind = peaks()
     s = stream.cuda_stream
-    tuning = plan.info() if args.no_autotune else tune(plan, timer, s)
+    tuning = plan.info() if args.no_autotune else plan.autotune(repeats=20, stream=s)
     info = plan.info()
 
     sampler = ClockSampler(dev.index)

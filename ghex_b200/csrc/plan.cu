@@ -1673,12 +1673,12 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
     const size_t flush_bytes = std::max<size_t>(2 * (size_t)l2, 64u << 20);
     uint4* flush = nullptr;
     unsigned* sink = nullptr;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::vector<cudaEvent_t> ev(2 * (size_t)repeats, nullptr);
     auto cleanup = [&]() {
         if (flush) cudaFree(flush);
         if (sink) cudaFree(sink);
-        if (e0) cudaEventDestroy(e0);
-        if (e1) cudaEventDestroy(e1);
+        for (auto e : ev)
+            if (e) cudaEventDestroy(e);
     };
     float best = 1e30f;
     cand bestc{plan.per_thread, plan.block, plan.use_pairs};
@@ -1687,31 +1687,31 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         check_cuda(cudaMalloc(&flush, flush_bytes), "cudaMalloc(l2 flush)");
         check_cuda(cudaMemsetAsync(flush, 0, flush_bytes, stream), "cudaMemsetAsync(l2 flush)");
         check_cuda(cudaMalloc(&sink, sizeof(unsigned)), "cudaMalloc(l2 flush sink)");
-        check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
-        check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+        for (auto& e : ev) check_cuda(cudaEventCreate(&e), "cudaEventCreate");
         const int fgrid = (plan.ctx ? plan.ctx->num_sms : 148) * 8;
         for (const auto& c : cands)
         {
             plan.per_thread = c.k, plan.block = c.block, plan.use_pairs = c.pairs;
             retile(plan, stream);
-            launch_plan(plan, GHEXB_FORM_BATCHED, stream); // warm-up
-            // the median of the repeats: one slow launch (another process, a clock change) must
-            // not decide the choice
-            std::vector<float> times;
+            for (int w = 0; w < 3; ++w) launch_plan(plan, GHEXB_FORM_BATCHED, stream); // warm-up
+            // the launches queued back to back, each after a cold-L2 read outside its events, as
+            // an application's exchanges follow its other kernels; the mean time per launch
             for (int r = 0; r < repeats; ++r)
             {
                 check_cuda(launch_l2_flush(flush, flush_bytes / 16, sink, fgrid, stream), "l2 flush");
-                check_cuda(cudaEventRecord(e0, stream), "cudaEventRecord");
+                check_cuda(cudaEventRecord(ev[2 * r], stream), "cudaEventRecord");
                 launch_plan(plan, GHEXB_FORM_BATCHED, stream);
-                check_cuda(cudaEventRecord(e1, stream), "cudaEventRecord");
-                check_cuda(cudaEventSynchronize(e1), "cudaEventSynchronize");
-                float ms = 0.f;
-                check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
-                times.push_back(ms);
+                check_cuda(cudaEventRecord(ev[2 * r + 1], stream), "cudaEventRecord");
             }
-            std::nth_element(times.begin(), times.begin() + times.size() / 2, times.end());
-            const float med = times[times.size() / 2];
-            if (med < best) best = med, bestc = c;
+            check_cuda(cudaEventSynchronize(ev[2 * repeats - 1]), "cudaEventSynchronize");
+            float total = 0.f;
+            for (int r = 0; r < repeats; ++r)
+            {
+                float ms = 0.f;
+                check_cuda(cudaEventElapsedTime(&ms, ev[2 * r], ev[2 * r + 1]), "cudaEventElapsedTime");
+                total += ms;
+            }
+            if (total < best) best = total, bestc = c;
         }
     }
     catch (...)
