@@ -13,9 +13,10 @@ value        effective GB/s of the batched, graph-captured exchange (algorithmic
              starts with a cold L2 (a read of an unrelated buffer of twice the L2 size runs before
              it, outside its events)
 e2e          the same metric through the public API (co.exchange(...).wait()) with the fields in
-             pinned host memory: host->device copy of every field, exchange, device->host copy of
-             every field, every step (consecutive steps on two device copies and two streams, so
-             that the two copy directions overlap)
+             pinned host memory: every step exchanges them in place, the kernel reading the owner
+             cells from host memory and writing the halo cells into it over the host interconnect
+             (only the touched cells cross it); `e2e.full_copy` is the other form, every field
+             copied to the device, exchanged there and copied back each step
 roofline     achieved GB/s of the exchange kernel (the only kernel of the batched form) against the
              measured HBM copy bandwidth; traffic = DRAM bytes per launch from an ncu capture
 cpu_baseline GHEX's own CPU exchange (single rank holding every domain, built from the reference
@@ -309,7 +310,11 @@ class Case:
 # ------------------------------------------------------------------------------------------
 # reference arm: GHEX's CPU exchange on all host cores
 # ------------------------------------------------------------------------------------------
-def _reference_worker(cfg: str, iterations: int, queue):
+def _reference_worker(cfg: str, seconds: float, barrier, queue):
+    """One process of the reference arm: builds its own copy of the workload, sizes its timed run
+    to about `seconds` from one measured exchange, waits for every other process at `barrier` and
+    then times its exchanges, so that the timed windows of all processes overlap. Puts
+    (seconds per exchange, kind, exchanges, window start, window end) with wall-clock window ends."""
     try:
         from oracle import reflib
         w = workload(cfg)
@@ -319,7 +324,11 @@ def _reference_worker(cfg: str, iterations: int, queue):
             for s in specs:
                 fields.append((gi, w.offsets(s), [w.domain_array(d, s) for d in w.domains]))
         if reflib.available():
-            sec = reflib.regular_exchange(w.shape, [(h, w.periodic) for h, _ in groups], w.domains, fields, iterations)
+            pg = [(h, w.periodic) for h, _ in groups]
+            est = reflib.regular_exchange(w.shape, pg, w.domains, fields, 1)
+            iters = max(2, int(np.ceil(seconds / max(est, 1e-6))))
+            barrier.wait(timeout=900)
+            sec = reflib.regular_exchange(w.shape, pg, w.domains, fields, iters)
             kind = "reference"
         else:
             from oracle import regular as O
@@ -327,18 +336,28 @@ def _reference_worker(cfg: str, iterations: int, queue):
             for h, _ in groups:
                 doms = [O.Domain(i, f, l) for i, f, l in w.domains]
                 pats.append((O.make_pattern((0,) * w.dim, tuple(n - 1 for n in w.shape), h, w.periodic, doms), doms))
-            t0 = time.perf_counter()
-            for it in range(iterations + 1):
-                if it == 1:
-                    t0 = time.perf_counter()
+
+            def once():
                 for gi, off, arrs in fields:
                     pat, doms = pats[gi]
                     O.exchange(pat, doms, arrs, [off] * len(doms))
-            sec = (time.perf_counter() - t0) / max(1, iterations)
+            t0 = time.perf_counter()
+            once()
+            iters = max(2, int(np.ceil(seconds / max(time.perf_counter() - t0, 1e-6))))
+            barrier.wait(timeout=900)
+            t0 = time.perf_counter()
+            for _ in range(iters):
+                once()
+            sec = (time.perf_counter() - t0) / iters
             kind = "port"
-        queue.put((sec, kind))
+        end = time.time()
+        queue.put((sec, kind, iters, end - sec * iters, end))
     except Exception as e:  # reported by the parent
-        queue.put((None, repr(e)))
+        try:
+            barrier.abort()
+        except Exception:
+            pass
+        queue.put((None, repr(e), 0, 0.0, 0.0))
 
 
 def alg_bytes_host(cfg: str) -> int:
@@ -367,32 +386,43 @@ def run_reference(args):
         procs = max(1, min(procs, int(psutil.virtual_memory().available / (1.5 * 2**30))))
     except Exception:
         pass
-    # every process exchanges its own copy; bounded to about a minute in all
-    iters = max(2, min(200, (args.steps + procs - 1) // procs))
+    # every process times about `seconds` of exchanges of its own copy, all windows overlapping
+    seconds = float(os.environ.get("GHEXB_REFERENCE_SECONDS", "2.0"))
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    ps = [ctx.Process(target=_reference_worker, args=(cfg, iters, q)) for _ in range(procs)]
+    barrier = ctx.Barrier(procs)
+    ps = [ctx.Process(target=_reference_worker, args=(cfg, seconds, barrier, q)) for _ in range(procs)]
     for p in ps:
         p.start()
     res = [q.get() for _ in ps]
     for p in ps:
         p.join()
     good = [r for r in res if r[0]]
-    if not good:
-        print(json.dumps({"impl": "reference", "unavailable": f"the CPU exchange failed: {res[0][1]}"}), flush=True)
+    if not good or len(good) < len(res):
+        bad = [r for r in res if not r[0]]
+        print(json.dumps({"impl": "reference", "unavailable": f"the CPU exchange failed: {bad[0][1]}"}), flush=True)
         return
     alg = alg_bytes_host(cfg)
-    rate = sum(1.0 / s for s, _ in good)  # exchanges per second, all processes
+    rates = sorted(1.0 / r[0] for r in good)  # exchanges per second of each process
+    rate = sum(rates)  # all processes, their timed windows overlapping
+    start, end = max(r[3] for r in good), min(r[4] for r in good)
+    durations = [r[4] - r[3] for r in good]
+    overlap = max(0.0, end - start) / max(durations)
     value = rate * alg / 1e9
     kind = good[0][1]
-    sample = (f"{len(good)} processes x {iters} timed exchanges (after 1 untimed) of {cfg}, each process on its "
-              f"own copy of the workload; GHEX's CPU exchange "
-              + ("built from the reference sources" if kind == "reference" else "restated in numpy"))
+    iters = sorted(r[2] for r in good)
+    sample = (f"{len(good)} processes, each timing {iters[0]}-{iters[-1]} exchanges (about {seconds:g} s, after 1 "
+              f"untimed) of {cfg} on its own copy of the workload, started together at a barrier; GHEX's CPU "
+              "exchange " + ("built from the reference sources (g++ -O3 -march=x86-64-v2)" if kind == "reference"
+                             else "restated in numpy"))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / rate, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic (seeded splitmix64)",
-            "config": {"workload": workload(cfg).name, "processes": len(good)},
+            "config": {"workload": workload(cfg).name},
             "exchanges_per_s": rate,
+            "processes": {"count": len(good), "window_overlap": overlap,
+                          "exchanges_per_s_each": {"min": rates[0], "median": float(np.median(rates)), "max": rates[-1]},
+                          "seconds_each": {"min": min(durations), "max": max(durations)}},
             "cpu_baseline": {"value": value, "unit": "GB/s", "cores": len(good), "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

@@ -7,8 +7,10 @@
 // tables live in a fixed, file-scope device array instead of per-plan allocations.
 //
 // The array is k_noalloc_scratch_bytes large and exists once per device for as long as the
-// library is loaded. Every call rebuilds the tables on the host, copies them into the array on the
-// caller's stream and launches the batched kernel on the same stream. All calls share the array, which keeps the
+// library is loaded. Every call rebuilds the tables on the host (index lists, then forward tiles),
+// copies them into the array on the caller's stream and launches the one batched exchange kernel
+// on the same stream at the default tuning. A stream that is being captured is refused: the copy
+// reads a host buffer that exists only during the call. All calls share the array, which keeps the
 // contents of the last call: calls whose work overlaps on the GPU (on different streams, without
 // ordering between them) race on it and must not be made.
 #include <cuda_runtime.h>
@@ -31,15 +33,17 @@ std::map<int, unsigned char*> g_scratch_address; // device -> device address of 
 
 // The device address of the scratch array on `device`, looked up once per device with that device
 // current. In host code the array's name is only a host-side stand-in, never a device address.
+// Every call checks that `device` is the current device: the copy and the launch go to the current
+// device, and the tables and fields live on `device`.
 unsigned char* scratch_address(int device)
 {
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    auto it = g_scratch_address.find(device);
-    if (it != g_scratch_address.end()) return it->second;
     int current = -1;
     ghexb::check_cuda(cudaGetDevice(&current), "cudaGetDevice");
     if (current != device)
         throw ghexb::error(GHEXB_ERR_INVALID, "ghexb_exchange_noalloc: the context's device must be the current device");
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    auto it = g_scratch_address.find(device);
+    if (it != g_scratch_address.end()) return it->second;
     void* p = nullptr;
     ghexb::check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(no-alloc scratch)");
     g_scratch_address[device] = static_cast<unsigned char*>(p);
@@ -61,6 +65,13 @@ extern "C" int ghexb_exchange_noalloc(ghexb_context ctx, const ghexb_field* fiel
     try
     {
         if (!ctx || !fields) throw ghexb::error(GHEXB_ERR_INVALID, "null argument");
+        auto s = static_cast<cudaStream_t>(stream);
+        // The tables are copied from a host buffer that lives only for this call: a captured copy
+        // would read freed memory at every replay, so a capturing stream is refused.
+        cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+        ghexb::check_cuda(cudaStreamIsCapturing(s, &capture), "cudaStreamIsCapturing");
+        if (capture != cudaStreamCaptureStatusNone)
+            throw ghexb::error(GHEXB_ERR_INVALID, "ghexb_exchange_noalloc cannot be captured into a CUDA graph");
         // host tables of the batched form at the default tuning
         ghexb_plan_s plan;
         ghexb::build_tables(plan, ctx, fields, n);
@@ -80,7 +91,6 @@ extern "C" int ghexb_exchange_noalloc(ghexb_context ctx, const ghexb_field* fiel
         put(host, off_idx, plan.idx);
         put(host, off_tiles, plan.xf);
 
-        auto s = static_cast<cudaStream_t>(stream);
         // from pageable memory: the call returns once the data is staged, so `host` may go
         ghexb::check_cuda(cudaMemcpyAsync(dev, host.data(), end, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync(no-alloc tables)");
         ghexb::check_cuda(ghexb::launch_exchange(reinterpret_cast<const ghexb::xtile*>(dev + off_tiles), (int)plan.xf.size(),

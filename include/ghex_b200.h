@@ -253,10 +253,12 @@ int ghexb_plan_autotune(ghexb_plan plan, void* stream, int repeats, ghexb_plan_i
  * cudaMalloc as a failure), or code that must not call cudaMalloc/cudaFree because they may
  * synchronize the device. The work tables go into one fixed device array of 4 MiB that every GPU
  * holds while the library is loaded; exchanges whose tables are larger fail with
- * GHEXB_ERR_RANGE. Each call copies the tables (scheduler counters zeroed) and launches the
- * batched kernels on `stream`; no cudaMalloc or cudaFree is called. The first call on a device
- * looks up the array's device address and must be made with that device current and before any
- * stream capture. All calls share the array and it keeps the last call's tables: calls that
+ * GHEXB_ERR_RANGE. Each call copies the index lists and forward tiles into the array and
+ * launches one batched exchange kernel on `stream` at the default tuning; no cudaMalloc or
+ * cudaFree is called. Every call must be made with the context's device current (else
+ * GHEXB_ERR_INVALID); the first call on a device also looks up the array's device address. The
+ * call cannot be captured into a CUDA graph: a capturing stream is refused with
+ * GHEXB_ERR_INVALID. All calls share the array and it keeps the last call's tables: calls that
  * overlap on the GPU race on it. */
 int ghexb_exchange_noalloc(ghexb_context ctx, const ghexb_field* fields, int n, void* stream);
 

@@ -1,0 +1,427 @@
+/*
+ * ghex_b200.hpp — C++ front end over the C ABI of ghex_b200.h, with the names and call shapes of
+ * GHEX's own C++ interface for the regular structured grid, so that GHEX code of the form
+ *
+ *     auto ctxt    = ghexb::context(device);
+ *     auto pattern = ghexb::make_pattern<ghexb::structured::grid>(ctxt, halo_gen, local_domains);
+ *     auto co      = ghexb::make_communication_object<decltype(pattern)>(ctxt);
+ *     auto field   = ghexb::wrap_field<ghexb::gpu, ghexb::layout_map<2, 1, 0>>(dom, ptr, offsets, extents);
+ *     co.exchange(pattern(field)).wait();
+ *
+ * runs on the B200 kernels. It replaces (paths relative to the GHEX 0.4.0 source tree):
+ *   ghex::context                         context.hpp:20-35
+ *   structured::regular::domain_descriptor structured/regular/domain_descriptor.hpp:248-254
+ *   structured::regular::halo_generator    structured/regular/halo_generator.hpp:68-78
+ *   make_pattern<structured::grid>         pattern_container.hpp:112-120
+ *   pattern(field) -> buffer_info          pattern_container.hpp:88-95
+ *   wrap_field<Arch, Layout>               structured/regular/field_descriptor.hpp:167-194
+ *   make_communication_object<Pattern>     communication_object.hpp:653-660
+ *   communication_object::exchange         communication_object.hpp:233-274
+ *   communication_handle::wait/is_ready    communication_object.hpp:627-648
+ *
+ * Header only; link with libghex_b200.so. Every failing C call throws ghexb::error (a
+ * std::runtime_error carrying the status code and the library's message), as GHEX throws
+ * std::runtime_error. Differences from GHEX: one process owns every domain (the context takes a
+ * CUDA device, not an MPI communicator); ghexb::cpu fields are exchanged by the GPU kernels in
+ * place in host memory, which the field's buffer_info page-locks for as long as it lives.
+ */
+#ifndef GHEX_B200_HPP
+#define GHEX_B200_HPP
+
+#include <array>
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+#include "ghex_b200.h"
+
+namespace ghexb
+{
+// ---- errors -------------------------------------------------------------------------------------
+class error : public std::runtime_error
+{
+  public:
+    error(int code, const std::string& what)
+    : std::runtime_error(what)
+    , m_code(code)
+    {
+    }
+    int code() const noexcept { return m_code; }
+
+  private:
+    int m_code;
+};
+
+inline void check(int status)
+{
+    if (status != GHEXB_OK)
+    {
+        char msg[1024] = {0};
+        ghexb_last_error(msg, sizeof msg);
+        throw error(status, msg);
+    }
+}
+
+// ---- architecture tags and layouts (ghex::cpu / ghex::gpu, gridtools::layout_map) ---------------
+struct cpu
+{
+};
+struct gpu
+{
+};
+
+// gridtools convention: the dimension with the largest value has stride 1
+template<int... L>
+struct layout_map
+{
+    static constexpr int size = sizeof...(L);
+    static std::array<int, sizeof...(L)> values() { return {{L...}}; }
+};
+
+namespace detail
+{
+template<typename T> struct dtype_of;
+template<> struct dtype_of<float> : std::integral_constant<int, GHEXB_F32> {};
+template<> struct dtype_of<double> : std::integral_constant<int, GHEXB_F64> {};
+template<> struct dtype_of<std::int32_t> : std::integral_constant<int, GHEXB_I32> {};
+template<> struct dtype_of<std::int64_t> : std::integral_constant<int, GHEXB_I64> {};
+template<> struct dtype_of<std::uint8_t> : std::integral_constant<int, GHEXB_U8> {};
+template<> struct dtype_of<std::uint16_t> : std::integral_constant<int, GHEXB_U16> {};
+
+template<typename H, int (*Destroy)(H)>
+struct handle_deleter
+{
+    void operator()(H h) const noexcept
+    {
+        if (h) Destroy(h);
+    }
+};
+template<typename S, int (*Destroy)(S*)>
+using owned = std::unique_ptr<S, handle_deleter<S*, Destroy>>;
+} // namespace detail
+
+// ---- context --------------------------------------------------------------------------------------
+class context
+{
+  public:
+    explicit context(int device = 0)
+    {
+        ghexb_context h = nullptr;
+        check(ghexb_context_create(device, &h));
+        m_h.reset(h);
+    }
+    ghexb_context get() const noexcept { return m_h.get(); }
+    int rank() const noexcept { return 0; } // one process owns every domain
+    int size() const noexcept { return 1; }
+
+  private:
+    detail::owned<ghexb_context_s, ghexb_context_destroy> m_h;
+};
+
+namespace structured
+{
+struct grid
+{
+};
+
+namespace regular
+{
+// domain_descriptor<DomainId, Dimension>(id, first, last): inclusive global coordinates
+template<typename DomainId, typename Dimension>
+class domain_descriptor
+{
+  public:
+    static constexpr int dim = Dimension::value;
+    using domain_id_type = DomainId;
+    using coordinate_type = std::array<int, dim>;
+
+    domain_descriptor(DomainId id, const coordinate_type& first, const coordinate_type& last)
+    : m_id(id)
+    , m_first(first)
+    , m_last(last)
+    {
+    }
+    DomainId domain_id() const noexcept { return m_id; }
+    const coordinate_type& first() const noexcept { return m_first; }
+    const coordinate_type& last() const noexcept { return m_last; }
+
+  private:
+    DomainId m_id;
+    coordinate_type m_first, m_last;
+};
+
+// halo_generator<DomainId, Dimension>(g_first, g_last, halos, periodic); halos holds 2*dim values
+// (dim0-, dim0+, dim1-, ...)
+template<typename DomainId, typename Dimension>
+class halo_generator
+{
+  public:
+    static constexpr int dim = Dimension::value;
+    using coordinate_type = std::array<int, dim>;
+
+    halo_generator(const coordinate_type& g_first, const coordinate_type& g_last, const std::array<int, 2 * dim>& halos,
+        const std::array<bool, dim>& periodic)
+    : m_first(g_first)
+    , m_last(g_last)
+    , m_halos(halos)
+    , m_periodic(periodic)
+    {
+    }
+    const coordinate_type& global_first() const noexcept { return m_first; }
+    const coordinate_type& global_last() const noexcept { return m_last; }
+    const std::array<int, 2 * dim>& halos() const noexcept { return m_halos; }
+    const std::array<bool, dim>& periodic() const noexcept { return m_periodic; }
+
+  private:
+    coordinate_type m_first, m_last;
+    std::array<int, 2 * dim> m_halos;
+    std::array<bool, dim> m_periodic;
+};
+
+// field_descriptor<T, Arch, DomainDescriptor, Layout>: borrows the user's memory
+template<typename T, typename Arch, typename DomainDescriptor, typename Layout>
+class field_descriptor
+{
+  public:
+    static constexpr int dim = DomainDescriptor::dim;
+    using value_type = T;
+    using arch_type = Arch;
+    using domain_descriptor_type = DomainDescriptor;
+    static_assert(Layout::size == dim, "the layout map must have one entry per dimension");
+
+    field_descriptor(const DomainDescriptor& dom, T* data, const std::array<int, dim>& offsets,
+        const std::array<int, dim>& extents, const std::vector<std::int64_t>& byte_strides = {})
+    : m_dom(dom)
+    , m_data(data)
+    , m_offsets(offsets)
+    , m_extents(extents)
+    , m_byte_strides(byte_strides)
+    {
+        if (!byte_strides.empty() && (int)byte_strides.size() != dim)
+            throw error(GHEXB_ERR_INVALID, "wrap_field: one byte stride per dimension");
+    }
+    const DomainDescriptor& domain() const noexcept { return m_dom; }
+    typename DomainDescriptor::domain_id_type domain_id() const noexcept { return m_dom.domain_id(); }
+    T* data() const noexcept { return m_data; }
+    const std::array<int, dim>& offsets() const noexcept { return m_offsets; }
+    const std::array<int, dim>& extents() const noexcept { return m_extents; }
+    const std::vector<std::int64_t>& byte_strides() const noexcept { return m_byte_strides; }
+
+    // bytes from data() to one past the last element
+    std::size_t span_bytes() const
+    {
+        std::array<std::int64_t, dim> st{};
+        if (!m_byte_strides.empty())
+            for (int a = 0; a < dim; ++a) st[a] = m_byte_strides[a];
+        else
+        {
+            // strides from the layout map: the largest value is contiguous
+            const auto lm = Layout::values();
+            std::int64_t s = sizeof(T);
+            for (int v = dim - 1; v >= 0; --v)
+                for (int a = 0; a < dim; ++a)
+                    if (lm[a] == v) st[a] = s, s *= m_extents[a];
+        }
+        std::int64_t end = 0;
+        for (int a = 0; a < dim; ++a) end += (std::int64_t)(m_extents[a] - 1) * st[a];
+        return (std::size_t)end + sizeof(T);
+    }
+
+  private:
+    DomainDescriptor m_dom;
+    T* m_data;
+    std::array<int, dim> m_offsets, m_extents;
+    std::vector<std::int64_t> m_byte_strides;
+};
+} // namespace regular
+} // namespace structured
+
+// wrap_field<Arch, Layout>(dom, data, offsets, extents[, byte_strides])
+template<typename Arch, typename Layout, typename DomainDescriptor, typename T>
+structured::regular::field_descriptor<T, Arch, DomainDescriptor, Layout> wrap_field(const DomainDescriptor& dom, T* data,
+    const std::array<int, DomainDescriptor::dim>& offsets, const std::array<int, DomainDescriptor::dim>& extents,
+    const std::vector<std::int64_t>& byte_strides = {})
+{
+    return {dom, data, offsets, extents, byte_strides};
+}
+
+// A field bound to a pattern (GHEX's buffer_info): owns the library's field handle, and for cpu
+// fields the page-locking of their memory.
+class buffer_info
+{
+  public:
+    ghexb_field get() const noexcept { return m_state->field.get(); }
+
+  private:
+    struct state
+    {
+        detail::owned<ghexb_field_s, ghexb_field_destroy> field;
+        void* registered = nullptr;
+        ~state()
+        {
+            if (registered) ghexb_host_unregister(registered);
+        }
+    };
+    std::shared_ptr<state> m_state = std::make_shared<state>();
+    template<typename, typename> friend class pattern_container;
+};
+
+// The pattern of a set of domains (pattern_container<grid, domain_id>)
+template<typename Grid, typename DomainDescriptor>
+class pattern_container
+{
+  public:
+    using domain_descriptor_type = DomainDescriptor;
+    using grid_type = Grid;
+
+    ghexb_pattern get() const noexcept { return m_h.get(); }
+    int size() const
+    {
+        int n = 0;
+        check(ghexb_pattern_num_domains(get(), &n));
+        return n;
+    }
+    int max_tag() const
+    {
+        int t = 0;
+        check(ghexb_pattern_max_tag(get(), &t));
+        return t;
+    }
+
+    // pattern(field) -> buffer_info; throws "field incompatible with available domains!" for a
+    // field of a domain that is not part of the pattern
+    template<typename T, typename Arch, typename Layout>
+    buffer_info operator()(const structured::regular::field_descriptor<T, Arch, DomainDescriptor, Layout>& f) const
+    {
+        constexpr int dim = DomainDescriptor::dim;
+        const auto lm = Layout::values();
+        buffer_info bi;
+        if (std::is_same<Arch, cpu>::value)
+        {
+            int owned = 0;
+            check(ghexb_host_register(f.data(), f.span_bytes(), &owned));
+            if (owned) bi.m_state->registered = f.data();
+        }
+        ghexb_field h = nullptr;
+        check(ghexb_field_wrap(get(), (std::int64_t)f.domain_id(), detail::dtype_of<T>::value, f.data(), dim,
+            f.offsets().data(), f.extents().data(), lm.data(), f.byte_strides().empty() ? nullptr : f.byte_strides().data(),
+            1, 0, &h));
+        bi.m_state->field.reset(h);
+        return bi;
+    }
+
+  private:
+    std::shared_ptr<ghexb_pattern_s> m_h;
+    explicit pattern_container(ghexb_pattern h)
+    : m_h(h, [](ghexb_pattern p) { if (p) ghexb_pattern_destroy(p); })
+    {
+    }
+    template<typename G, typename H, typename R>
+    friend auto make_pattern(context&, const H&, const R&);
+};
+
+// make_pattern<structured::grid>(ctxt, halo_gen, domain_range)
+template<typename Grid, typename HaloGenerator, typename DomainRange>
+auto make_pattern(context& ctxt, const HaloGenerator& hg, const DomainRange& domains)
+{
+    static_assert(std::is_same<Grid, structured::grid>::value, "this front end covers the regular structured grid");
+    using dom_type = typename std::decay<decltype(*std::begin(domains))>::type;
+    constexpr int dim = dom_type::dim;
+    std::vector<std::int64_t> ids;
+    std::vector<int> firsts, lasts;
+    for (const auto& d : domains)
+    {
+        ids.push_back((std::int64_t)d.domain_id());
+        firsts.insert(firsts.end(), d.first().begin(), d.first().end());
+        lasts.insert(lasts.end(), d.last().begin(), d.last().end());
+    }
+    std::array<int, dim> periodic{};
+    for (int a = 0; a < dim; ++a) periodic[a] = hg.periodic()[a] ? 1 : 0;
+    ghexb_pattern h = nullptr;
+    check(ghexb_pattern_create_regular(ctxt.get(), dim, hg.global_first().data(), hg.global_last().data(), hg.halos().data(),
+        periodic.data(), (int)ids.size(), ids.data(), firsts.data(), lasts.data(), &h));
+    return pattern_container<Grid, dom_type>(h);
+}
+
+// The handle of one exchange: wait() blocks until the halos are written (communication_handle)
+class [[nodiscard]] communication_handle
+{
+  public:
+    void wait()
+    {
+        if (!m_h) return;
+        check(ghexb_handle_wait(m_h.get()));
+        m_h.reset();
+        m_keep.clear();
+    }
+    bool is_ready()
+    {
+        if (!m_h) return true;
+        int ready = 0;
+        check(ghexb_handle_is_ready(m_h.get(), &ready));
+        return ready != 0;
+    }
+    void progress() {} // nothing to progress: the exchange is a stream-ordered kernel
+
+  private:
+    detail::owned<ghexb_handle_s, ghexb_handle_destroy> m_h;
+    std::vector<buffer_info> m_keep; // the fields stay bound until the exchange completed
+    template<typename> friend class communication_object;
+};
+
+template<typename Pattern>
+class communication_object
+{
+  public:
+    explicit communication_object(context& ctxt)
+    {
+        ghexb_co h = nullptr;
+        check(ghexb_co_create(ctxt.get(), &h));
+        m_h.reset(h);
+    }
+
+    // exchange(pattern(f1), pattern(f2), ...); throws "earlier exchange operation was not
+    // finished" when the previous exchange has not been waited for
+    template<typename... BufferInfos>
+    communication_handle exchange(const buffer_info& first, const BufferInfos&... rest)
+    {
+        std::vector<buffer_info> bis{first, rest...};
+        return exchange(bis.begin(), bis.end());
+    }
+
+    // exchange(first, last) over a range of buffer_infos
+    template<typename Iterator,
+        typename = typename std::enable_if<!std::is_same<typename std::decay<Iterator>::type, buffer_info>::value>::type>
+    communication_handle exchange(Iterator first, Iterator last)
+    {
+        communication_handle hd;
+        std::vector<ghexb_field> fields;
+        for (auto it = first; it != last; ++it)
+        {
+            fields.push_back(it->get());
+            hd.m_keep.push_back(*it);
+        }
+        ghexb_handle h = nullptr;
+        check(ghexb_co_exchange(m_h.get(), fields.data(), (int)fields.size(), nullptr, &h));
+        hd.m_h.reset(h);
+        return hd;
+    }
+
+  private:
+    detail::owned<ghexb_co_s, ghexb_co_destroy> m_h;
+};
+
+// make_communication_object<Pattern>(ctxt)
+template<typename Pattern>
+communication_object<Pattern> make_communication_object(context& ctxt)
+{
+    return communication_object<Pattern>(ctxt);
+}
+} // namespace ghexb
+
+#endif /* GHEX_B200_HPP */

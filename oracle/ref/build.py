@@ -2,14 +2,18 @@
 the reference sources where they lie, against the stand-ins of oracle/ref/shim — test
 infrastructure only.
 
-    python oracle/ref/build.py [--reference /root/reference] [--force]
+    python oracle/ref/build.py --reference <GHEX source tree> [--force]
+    GHEX_REFERENCE=<GHEX source tree> python oracle/ref/build.py
 
 Nothing is copied from the reference tree; without it the build is skipped. The product never
-links or loads this library.
+links or loads this library. It is compiled with -O3 -march=x86-64-v2: it is built where the
+reference sources are and runs on other hosts (the GPU machines), so it cannot target the build
+host's own instruction set; memcpy, the reference's hot loop, dispatches on the CPU at run time.
 """
 from __future__ import annotations
 
 import argparse
+import os
 import subprocess
 import sys
 from pathlib import Path
@@ -20,7 +24,12 @@ LIB = OUT / "libghex_ref.so"
 SOURCES = ["ghex_ref.cpp", "cs_checks.cpp"]
 
 
-def build(reference: str = "/root/reference", force: bool = False) -> Path | None:
+def build(reference: str | None = None, force: bool = False) -> Path | None:
+    """Builds the library from the GHEX tree at `reference` (default: $GHEX_REFERENCE); returns
+    None without building when no tree is given or found."""
+    reference = reference or os.environ.get("GHEX_REFERENCE")
+    if not reference:
+        return None
     ref = Path(reference)
     if not (ref / "include" / "ghex").is_dir():
         return None
@@ -40,7 +49,7 @@ def build(reference: str = "/root/reference", force: bool = False) -> Path | Non
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None, help="GHEX source tree (default: $GHEX_REFERENCE)")
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
     print(build(a.reference, a.force))

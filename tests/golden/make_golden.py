@@ -1,6 +1,6 @@
 """Generates the golden fixtures of tests/golden/ from the reference.
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <GHEX source tree>   (or GHEX_REFERENCE=<tree>)
 
 * unstructured_4domain.json — the hand-built 4-domain unstructured test case of GHEX's Python
   test (test/bindings/python/test_unstructured_domain_descriptor.py: the `domains` literal, read
@@ -37,6 +37,7 @@ Every input is seeded or analytic; the script needs the reference tree and oracl
 from __future__ import annotations
 
 import argparse
+import os
 import ast
 import json
 import sys
@@ -149,8 +150,11 @@ def unstructured_fields(dom: dict, rank: int, levels: int, order: str) -> np.nda
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("GHEX_REFERENCE"),
+                    help="GHEX source tree (default: $GHEX_REFERENCE)")
     a = ap.parse_args()
+    if not a.reference:
+        raise SystemExit("give the GHEX source tree with --reference or GHEX_REFERENCE")
     reference = Path(a.reference)
     from oracle import reflib
     from oracle.ref import build as refbuild
