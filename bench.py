@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["cfg0", "cfg1", "cfg1_staged", "cfg2", "cfg2_ipr", "cfg3", "cfg4"],
+    ap.add_argument("--config", choices=["cfg0", "cfg1", "cfg1_staged", "cfg2", "cfg2_ipr", "cfg3", "cfg4", "cfg4_f32"],
                     default="cfg1")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline leg")
@@ -151,6 +151,8 @@ def workload(cfg: str):
         return W.config2(halo_by_owner=True)
     if cfg == "cfg1_staged":
         return W.config1()
+    if cfg == "cfg4_f32":
+        return W.config4(dtype=np.float32)
     return {"cfg0": W.config0, "cfg1": W.config1, "cfg2": W.config2, "cfg3": W.config3, "cfg4": W.config4}[cfg]()
 
 
@@ -443,16 +445,25 @@ def max_over_ranks(value: float, world: int, device) -> float:
 
 
 class Timer:
-    """Device time of `launch` per step with CUDA events on `stream`, max over ranks; every timed
-    step starts with a cold L2 (a read of `flush`, outside the events)."""
+    """Device time of `launch` per step with CUDA events on `stream`, max over ranks.
+
+    mode "cold" (the headline protocol): every timed step starts with a cold L2 (a read of
+    `flush`, twice the L2 size, outside the events); the launch's dirty lines are written back
+    during the next step's flush, outside the events.
+    mode "warm": steps back to back with no flush (the steady state of repeated exchanges whose
+    working set stays in L2).
+    mode "writeback": as "cold", but the events also span the flush that follows the launch, and
+    the time of a flush that follows a flush is subtracted: the exchange plus the write-back of
+    the lines it dirtied."""
 
     def __init__(self, stream, flush, world, dev):
         self.stream, self.flush, self.world, self.dev = stream, flush, world, dev
 
-    def __call__(self, launch, steps, warmup):
+    def _run(self, launch, steps, warmup, mode):
         import torch
         import torch.distributed as dist
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        flush = self.flush if mode != "warm" else None
         with torch.cuda.stream(self.stream):
             for _ in range(warmup):
                 launch()
@@ -461,15 +472,23 @@ class Timer:
                 dist.barrier()
             torch.cuda.synchronize()
             for k in range(steps):
-                if self.flush is not None:
-                    self.flush.sum()
+                if flush is not None:
+                    flush.sum()
                 ev[k][0].record(self.stream)
                 launch()
+                if mode == "writeback":
+                    flush.sum()
                 ev[k][1].record(self.stream)
             torch.cuda.synchronize()
             if self.world > 1:
                 dist.barrier()
-        return max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / steps, self.world, self.dev)
+        return sum(a.elapsed_time(b) for a, b in ev) / steps
+
+    def __call__(self, launch, steps, warmup, mode="cold"):
+        ms = self._run(launch, steps, warmup, mode)
+        if mode == "writeback":
+            ms -= self._run(lambda: None, steps, warmup, mode)
+        return max_over_ranks(ms, self.world, self.dev)
 
 
 def e2e_ms(case, stream, steps, world, dev):
@@ -574,7 +593,7 @@ def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline
            "per_field": {"ms": ms_f, "GB/s": case.alg / ms_f / 1e6, "exchanges_per_s": 1e3 / ms_f},
            "batched_vs_per_field": ms_f / ms_b,
            "tuning": {k: tuning[k] for k in ("elems_per_thread", "block", "grid", "pairs", "use_pairs")}}
-    if cfg == "cfg4":
+    if cfg in ("cfg4", "cfg4_f32"):
         ms_a = timer(lambda: plan.adjoint(s), steps, warmup)
         out["adjoint"] = {"ms": ms_a, "vs_forward": ms_a / ms_b, "launches": plan.info()["adjoint_launches"]}
     if baseline:
@@ -584,6 +603,67 @@ def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline
         out["bitexact"] = case.mismatches(expected) == 0
         out["cpu_baseline"] = {"value": case.alg / sec / 1e9, "unit": "GB/s", "cores": 1, "kind": kind, "ms": sec * 1e3}
     return out
+
+
+def measure_program(dev, timer, dtype, steps, warmup, baseline=True) -> dict:
+    """The differentiable program of the 256x256x128 workload (2x2x2 domains, halo 1, periodic): 10
+    x (halo exchange, 7-point update x <- x + 0.1 L(x)), loss = sum of squares of the final
+    interiors, forward and backward through torch.autograd. One timed step = the whole program,
+    forward and backward (the backward runs the exchange's adjoint kernel and the stencil's
+    transpose); also timed: the forward alone."""
+    import torch
+    from ghex_b200 import autograd as AG
+    from ghex_b200 import workloads as W
+    from ghex_b200.structured import regular as R
+    w = W.config4(dtype=dtype)
+    spec = w.fields[0]
+    ctx = R.make_context(device=dev.index)
+    hg = R.HaloGenerator(((0,) * 3, tuple(n - 1 for n in w.shape)), [(1, 1)] * 3, w.periodic)
+    doms = [R.DomainDescriptor(i, (f, l)) for i, f, l in w.domains]
+    pat = R.make_pattern(ctx, hg, doms)
+    host = [w.domain_array(d, spec) for d in w.domains]
+    x0 = [torch.from_numpy(a).to(dev) for a in host]
+    bis = [pat(R.make_field_descriptor(dm, t, w.offsets(spec), w.extents(d, spec))) for dm, d, t in zip(doms, w.domains, x0)]
+    dx = AG.DifferentiableExchange(ctx, bis)
+    nsteps, alpha = 10, 0.1
+    out = {}
+
+    def fwd_bwd():
+        leaves = [x.clone().requires_grad_(True) for x in x0]
+        ys = AG.diffusion_program(dx, [l.clone() for l in leaves], nsteps, alpha)
+        AG.interior_loss(ys).backward()
+        out["grad"] = [l.grad for l in leaves]
+        out["ys"] = ys
+
+    def fwd():
+        with torch.no_grad():
+            AG.diffusion_program(dx, [x.clone() for x in x0], nsteps, alpha)
+
+    with torch.cuda.stream(timer.stream):
+        ms_fb = timer(fwd_bwd, steps, warmup)
+        ms_f = timer(fwd, steps, warmup)
+        fwd_bwd()
+    torch.cuda.synchronize()
+    res = {"workload": w.name + f", {nsteps} x (exchange, 7-point update), loss = sum of squares, forward + backward",
+           "dtype": np.dtype(dtype).name.replace("float", "f"),
+           "forward_backward_ms": ms_fb, "forward_ms": ms_f, "inner_steps": nsteps,
+           "forward_backward_ms_per_inner_step": ms_fb / nsteps}
+    if baseline:
+        from oracle import regular as O
+        from oracle import stencil as S
+        odoms = [O.Domain(i, f, l) for i, f, l in w.domains]
+        opat = O.make_pattern((0,) * 3, tuple(n - 1 for n in w.shape), spec.halos, w.periodic, odoms)
+        prog = S.Program(opat, odoms, w.offsets(spec), steps=nsteps, alpha=alpha)
+        ys_ref = prog.forward(host)
+        g_ref = prog.gradient(host)
+
+        def same(a, b):
+            u = np.dtype(f"u{b.itemsize}")
+            return np.array_equal(np.ascontiguousarray(a).view(u), np.ascontiguousarray(b).view(u))
+        res["bitexact"] = all(same(y.detach().cpu().numpy(), r) for y, r in zip(out["ys"], ys_ref)) and \
+            all(same(g.cpu().numpy(), r) for g, r in zip(out["grad"], g_ref))
+        res["checked"] = "final fields and the gradient against the oracle's program and explicit transpose"
+    return res
 
 
 def measure_staged(dev, timer, peak, steps, warmup, autotune=True, baseline=True) -> dict:
@@ -749,10 +829,13 @@ def main():
     if rank == 0 and world == 1 and not args.no_configs:
         del case
         line["configs"] = {}
-        for cfg in ("cfg2", "cfg2_ipr", "cfg3", "cfg4"):
+        for cfg in ("cfg2", "cfg2_ipr", "cfg3", "cfg4", "cfg4_f32"):
             if cfg != args.config:
                 line["configs"][cfg] = measure_config(cfg, dev, timer, peak, min(args.steps, 200), max(3, args.warmup),
                                                       not args.no_autotune, not args.no_baseline)
+        for name, dt in (("cfg4_program", np.float64), ("cfg4_f32_program", np.float32)):
+            line["configs"][name] = measure_program(dev, timer, dt, min(args.steps, 50), max(3, args.warmup),
+                                                    not args.no_baseline)
         line["configs"]["cfg1_staged"] = measure_staged(dev, timer, peak, min(args.steps, 200), max(3, args.warmup),
                                                         not args.no_autotune, not args.no_baseline)
     if rank == 0:

@@ -110,6 +110,7 @@ SIGNATURES = {
     "ghexb_plan_destroy": [_vp],
     "ghexb_plan_check": [_vp, C.POINTER(_vp), _i, _pi64],
     "ghexb_plan_get_info": [_vp, C.POINTER(PlanInfo)],
+    "ghexb_plan_dram_floor": [_vp, C.POINTER(_vp), _i, _i, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
     "ghexb_plan_set_tuning": [_vp, _i, _i, _i],
     "ghexb_plan_launch": [_vp, _i, _vp],
     "ghexb_plan_graph_launch": [_vp, _vp],

@@ -505,6 +505,10 @@ class ExchangePlan:
         call("ghexb_plan_get_info", self._h, C.byref(i))
         return i.as_dict()
 
+    def dram_floor(self, sector_bytes: int = 32) -> dict:
+        """The least DRAM traffic of one exchange of this plan's fields from a cold cache."""
+        return dram_floor(self.context, self._bis, sector_bytes)
+
     def set_tuning(self, elems_per_thread: int = 0, block: int = 0, use_pairs: int = -1) -> None:
         """Elements per thread (4, 8 or 16) and threads per CTA of the forward kernel (0 keeps), and
         whether x-face pairs move as contiguous segments (1), as separate boxes (0) or as before (-1)."""
@@ -558,6 +562,19 @@ class ExchangePlan:
     def __del__(self, _release=_capi.release):
         _release("ghexb_plan_destroy", getattr(self, "_h", None))
         self._h = None
+
+
+def dram_floor(ctx: context, buffer_infos: Sequence[BufferInfo], sector_bytes: int = 32) -> dict:
+    """The least DRAM traffic of one exchange of these fields from a cold cache, with
+    `sector_bytes` as the DRAM access granularity: sectors holding halo sources are read, sectors
+    holding halo elements are written back, sectors written in part without a source element are
+    read first (host-only replay of every element's addresses; no device needed)."""
+    bis = _flatten(tuple(buffer_infos))
+    handles = [bi.handle() for bi in bis]
+    arr = (C.c_void_p * len(handles))(*handles)
+    r, w = C.c_int64(), C.c_int64()
+    call("ghexb_plan_dram_floor", ctx._h, arr, len(handles), int(sector_bytes), C.byref(r), C.byref(w))
+    return {"sector_bytes": int(sector_bytes), "read": r.value, "write": w.value, "total": r.value + w.value}
 
 
 def make_exchange_plan(ctx: context, buffer_infos: Sequence[BufferInfo], in_place_receive: bool = False) -> ExchangePlan:

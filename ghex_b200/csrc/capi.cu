@@ -609,6 +609,18 @@ int ghexb_plan_check(ghexb_context ctx, const ghexb_field* fields, int n, int64_
     });
 }
 
+int ghexb_plan_dram_floor(ghexb_context ctx, const ghexb_field* fields, int n, int sector_bytes, int64_t* read_bytes,
+    int64_t* write_bytes)
+{
+    return guarded([&] {
+        require(ctx && fields && read_bytes && write_bytes, "null argument");
+        require(sector_bytes >= 16, "the sector size must be at least 16 bytes");
+        ghexb_plan_s plan;
+        ghexb::build_tables(plan, ctx, fields, n);
+        ghexb::dram_floor(plan, sector_bytes, *read_bytes, *write_bytes);
+    });
+}
+
 int ghexb_plan_destroy(ghexb_plan plan)
 {
     delete plan;

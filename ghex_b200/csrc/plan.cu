@@ -976,6 +976,55 @@ int64_t valid_elements(const xtile& t)
 int class_of_g(const gtile& t) { return t.kind ? list_gather_class(t.esize, t.nimg) : gather_class(t.esize, t.nimg); }
 } // namespace
 
+void dram_floor(const ghexb_plan_s& plan, int sector, int64_t& read_bytes, int64_t& write_bytes)
+{
+    if (sector < 1 || (sector & (sector - 1))) throw error(GHEXB_ERR_INVALID, "the sector size must be a power of two");
+    // every element's source and destination address as (sector << 5) | bytes: elements are aligned
+    // to their size (at most 16 bytes), so none straddles a sector of 16 bytes or more
+    std::vector<uint64_t> rd, wr;
+    rd.reserve((size_t)plan.halo_elements);
+    wr.reserve((size_t)plan.halo_elements);
+    auto add = [&](const char* src, const char* dst, uint64_t bytes) {
+        rd.push_back((reinterpret_cast<uintptr_t>(src) / sector) << 5 | bytes);
+        wr.push_back((reinterpret_cast<uintptr_t>(dst) / sector) << 5 | bytes);
+    };
+    for (const auto& b : plan.boxes)
+        for (int32_t i2 = 0; i2 < b.n2; ++i2)
+            for (int32_t i1 = 0; i1 < b.n1; ++i1)
+                for (int32_t i0 = 0; i0 < b.n0; ++i0)
+                    add(b.src + ((int64_t)i0 * b.s0 + (int64_t)i1 * b.s1 + (int64_t)i2 * b.s2) * b.esize,
+                        b.dst + ((int64_t)i0 * b.d0 + (int64_t)i1 * b.d1 + (int64_t)i2 * b.d2) * b.esize, b.esize);
+    for (size_t i = 0; i < plan.lists.size(); ++i)
+    {
+        const auto& l = plan.lists[i];
+        const int32_t* sidx = plan.idx.data() + plan.list_idx_off[i];
+        const int32_t* didx = sidx + l.count;
+        for (int32_t k = 0; k < l.count; ++k)
+            for (int32_t v = 0; v < l.levels; ++v)
+                add(l.src + ((int64_t)sidx[k] * l.s_is + (int64_t)v * l.s_ls) * l.unit,
+                    l.dst + ((int64_t)didx[k] * l.d_is + (int64_t)v * l.d_ls) * l.unit, l.unit);
+    }
+    std::sort(rd.begin(), rd.end());
+    std::sort(wr.begin(), wr.end());
+    std::vector<uint64_t> rs; // sectors read
+    for (uint64_t v : rd)
+        if (rs.empty() || rs.back() != (v >> 5)) rs.push_back(v >> 5);
+    int64_t written = 0, fill = 0;
+    for (size_t a = 0; a < wr.size();)
+    {
+        const uint64_t sec = wr[a] >> 5;
+        uint64_t bytes = 0;
+        size_t b = a;
+        for (; b < wr.size() && (wr[b] >> 5) == sec; ++b) bytes += wr[b] & 31u;
+        ++written;
+        // a sector written in part whose other bytes were not read is filled from DRAM first
+        if (bytes < (uint64_t)sector && !std::binary_search(rs.begin(), rs.end(), sec)) ++fill;
+        a = b;
+    }
+    read_bytes = ((int64_t)rs.size() + fill) * sector;
+    write_bytes = written * sector;
+}
+
 int64_t check_tables(ghexb_plan_s& plan)
 {
     build_tiles(plan, plan.idx.data());

@@ -145,6 +145,10 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats);
 // recomputes the descriptor pointers and rewrites the device tables on `stream`.
 void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stream);
 void check_cuda(cudaError_t e, const char* what);
+// Host-only: the least DRAM traffic of one exchange with a cold cache at the given sector size:
+// every sector holding a source element is read, every sector holding a destination element is
+// written back, and a sector written in part that holds no source element is read first.
+void dram_floor(const ghexb_plan_s& plan, int sector, int64_t& read_bytes, int64_t& write_bytes);
 // Records a failure for ghexb_last_error() (capi.cu).
 int set_last_error(int code, const std::string& msg);
 } // namespace ghexb

@@ -225,6 +225,14 @@ int ghexb_plan_destroy(ghexb_plan plan);
  * GHEXB_ERR_RANGE if one falls outside its field's memory span. */
 int ghexb_plan_check(ghexb_context ctx, const ghexb_field* fields, int n, int64_t* elements_checked);
 int ghexb_plan_get_info(ghexb_plan plan, ghexb_plan_info_t* info);
+/* Host-only, no device needed: the least DRAM traffic of one exchange of these fields from a
+ * cold cache, with `sector_bytes` (a power of two >= 16) as the DRAM access granularity: every
+ * sector holding a halo source element is read, every sector holding a halo element is written
+ * back, and a sector written in part that holds no source element is read before it is written.
+ * The bytes no kernel can avoid, against which a kernel's measured DRAM traffic is compared. No
+ * reference counterpart. */
+int ghexb_plan_dram_floor(ghexb_context ctx, const ghexb_field* fields, int n, int sector_bytes, int64_t* read_bytes,
+    int64_t* write_bytes);
 /* elems_per_thread (4, 8 or 16) and block (a multiple of 32, at most 512); values <= 0 keep the
  * current one. A tile holds elems_per_thread * block elements (half as many 16-byte units).
  * use_pairs: 1 moves the x-face pairs as contiguous segments, 0 as separate boxes, < 0 keeps.
