@@ -66,7 +66,14 @@ class PlanInfo(C.Structure):
         ("grid", C.c_int32),
         ("pairs", C.c_int32),
         ("use_pairs", C.c_int32),
-        ("reserved", C.c_int32),
+        ("staged_mode", C.c_int32),
+        ("staged_boxes", C.c_int32),
+        ("staged_items", C.c_int32),
+        ("staged_maps", C.c_int32),
+        ("stages", C.c_int32),
+        ("stage_bytes", C.c_int32),
+        ("stage_consumers", C.c_int32),
+        ("stage_ctas_per_sm", C.c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -110,6 +117,8 @@ SIGNATURES = {
     "ghexb_plan_destroy": [_vp],
     "ghexb_plan_check": [_vp, C.POINTER(_vp), _i, _pi64],
     "ghexb_plan_get_info": [_vp, C.POINTER(PlanInfo)],
+    "ghexb_plan_set_staged": [_vp, _i, _i, _i, _i, _i],
+    "ghexb_plan_staged_status": [_vp, C.POINTER(C.c_uint)],
     "ghexb_plan_dram_floor": [_vp, C.POINTER(_vp), _i, _i, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
     "ghexb_plan_set_tuning": [_vp, _i, _i, _i],
     "ghexb_plan_launch": [_vp, _i, _vp],

@@ -514,6 +514,18 @@ class ExchangePlan:
         whether x-face pairs move as contiguous segments (1), as separate boxes (0) or as before (-1)."""
         call("ghexb_plan_set_tuning", self._h, elems_per_thread, block, use_pairs)
 
+    def set_staged(self, mode: int = -1, stages: int = 0, stage_bytes: int = 0, consumers: int = 0,
+                   ctas_per_sm: int = 0) -> None:
+        """Boxes of the batched form moved by the staged (tensor-map) kernel: mode 0 none, 1 short
+        rows and transposed edges, 2 every box it can take; and its pipeline shape (0 keeps)."""
+        call("ghexb_plan_set_staged", self._h, mode, stages, stage_bytes, consumers, ctas_per_sm)
+
+    def staged_status(self) -> int:
+        """The staged kernel's status word since the last call (0: every wait ended in time)."""
+        v = C.c_uint()
+        call("ghexb_plan_staged_status", self._h, C.byref(v))
+        return v.value
+
     def _stream(self, stream):
         if stream is None:
             return stream_of(self._arrays)

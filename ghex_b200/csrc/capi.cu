@@ -605,6 +605,15 @@ int ghexb_plan_check(ghexb_context ctx, const ghexb_field* fields, int n, int64_
         require(ctx && fields && elements_checked, "null argument");
         ghexb_plan_s plan;
         ghexb::build_tables(plan, ctx, fields, n);
+        // every staged mode at two stage sizes (host geometry only), then the element kernel alone
+        plan.encode_maps = false;
+        for (int mode : {1, 2})
+            for (int bytes : {16384, 4096})
+            {
+                plan.staged_mode = mode, plan.stage_bytes = bytes;
+                (void)ghexb::check_tables(plan);
+            }
+        plan.staged_mode = 0;
         *elements_checked = ghexb::check_tables(plan);
     });
 }
@@ -644,7 +653,16 @@ int ghexb_plan_get_info(ghexb_plan plan, ghexb_plan_info_t* info)
         info->grid = (int32_t)plan->xf.size();
         info->pairs = (int32_t)plan->pairs.size();
         info->use_pairs = plan->use_pairs ? 1 : 0;
-        info->reserved = 0;
+        info->staged_mode = plan->staged_mode;
+        int staged = 0;
+        for (char c : plan->box_staged) staged += c != 0;
+        info->staged_boxes = staged;
+        info->staged_items = (int32_t)plan->sitems.size();
+        info->staged_maps = (int32_t)plan->smaps.size();
+        info->stages = plan->stages;
+        info->stage_bytes = plan->stage_bytes;
+        info->stage_consumers = plan->stage_consumers;
+        info->stage_ctas_per_sm = plan->stage_ctas_per_sm;
     });
 }
 
@@ -666,6 +684,40 @@ int ghexb_plan_set_tuning(ghexb_plan plan, int elems_per_thread, int block, int 
         if (use_pairs >= 0) plan->use_pairs = use_pairs != 0;
         ghexb::retile(*plan);
         ghexb::check_cuda(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
+    });
+}
+
+int ghexb_plan_set_staged(ghexb_plan plan, int mode, int stages, int stage_bytes, int consumers, int ctas_per_sm)
+{
+    return guarded([&] {
+        require(plan != nullptr, "null plan");
+        require(mode <= 2, "staged mode must be 0, 1 or 2");
+        require(stages <= 16, "at most 16 stages");
+        require(stage_bytes <= 0 || (stage_bytes % 128 == 0 && stage_bytes <= 64 * 1024),
+            "stage bytes must be a multiple of 128 and at most 64 KiB");
+        require(consumers <= 8, "at most 8 consumer warps");
+        require(ctas_per_sm <= 4, "at most 4 staged CTAs per SM");
+        const int st = stages > 0 ? stages : plan->stages, sb = stage_bytes > 0 ? stage_bytes : plan->stage_bytes;
+        require(st >= 2, "at least 2 stages");
+        require((size_t)st * sb + 128 <= 227 * 1024, "stages x stage bytes exceed the shared memory of a CTA");
+        if (mode >= 0) plan->staged_mode = mode;
+        plan->stages = st, plan->stage_bytes = sb;
+        if (consumers > 0) plan->stage_consumers = consumers;
+        if (ctas_per_sm > 0) plan->stage_ctas_per_sm = ctas_per_sm;
+        ghexb::retile(*plan);
+        ghexb::check_cuda(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
+    });
+}
+
+int ghexb_plan_staged_status(ghexb_plan plan, unsigned* status)
+{
+    return guarded([&] {
+        require(plan && status, "null argument");
+        *status = 0;
+        if (!plan->d_status) return;
+        ghexb::check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+        ghexb::check_cuda(cudaMemcpy(status, plan->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost), "cudaMemcpy(status)");
+        ghexb::check_cuda(cudaMemset(plan->d_status, 0, sizeof(unsigned)), "cudaMemset(status)");
     });
 }
 

@@ -11,6 +11,7 @@
 // a sign-bit mask; the unstructured gather/scatter (unstructured/user_concepts.hpp:549-581)
 // becomes one index-list descriptor per neighbour pair.
 #include <algorithm>
+#include <array>
 #include <cstring>
 #include <map>
 #include <tuple>
@@ -853,6 +854,8 @@ void check_accessible(const void* p, size_t bytes)
 void upload_plan(ghexb_plan_s& plan)
 {
     for (const auto& f : plan.fields) check_accessible(f.data, (size_t)(field_span(f) * f.esize));
+    plan.field_on_device.clear();
+    for (const auto& f : plan.fields) plan.field_on_device.push_back(accessible_type(f.data) == cudaMemoryTypeDevice);
     // upload index lists, patch device pointers, upload descriptor tables
     upload(plan.d_idx, plan.idx);
     for (size_t i = 0; i < plan.lists.size(); ++i)
@@ -1129,7 +1132,9 @@ int64_t check_tables(ghexb_plan_s& plan)
     for (const auto& r : plan.xp_field) np += check_tiles(plan.xp, r.first, r.second, class_of_x);
     for (const auto& r : plan.xb_box) nb += check_tiles(plan.xb, r.first, r.second, class_of_x);
     for (const auto& r : plan.xb_list) nb += check_tiles(plan.xb, r.first, r.second, class_of_x);
-    if (nf != nb || np != nb) throw error(GHEXB_ERR_INTERNAL, "batched, per-field and per-box tables differ");
+    const int64_t ns = check_staged(plan);
+    checked += ns;
+    if (nf + ns != nb || np != nb) throw error(GHEXB_ERR_INTERNAL, "batched, per-field and per-box tables differ");
     if (plan.gather_ok)
     {
         check_tiles(plan.gt, 0, (int)plan.gt.size(), class_of_g);
@@ -1291,12 +1296,24 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
     copy_async(plan.d_xb, plan.xb, stream);
     copy_async(plan.d_gt, plan.gt, stream);
     copy_async(plan.d_lcols, plan.lcols, stream);
+    ensure(plan.d_smaps, plan.cap_smaps, plan.smaps.size());
+    ensure(plan.d_sitems, plan.cap_sitems, plan.sitems.size());
+    copy_async(plan.d_smaps, plan.smaps, stream);
+    copy_async(plan.d_sitems, plan.sitems, stream);
+    if (!plan.sitems.empty() && !plan.d_status)
+    {
+        check_cuda(cudaMalloc(&plan.d_status, sizeof(unsigned)), "cudaMalloc(staged status)");
+        check_cuda(cudaMemsetAsync(plan.d_status, 0, sizeof(unsigned), stream), "cudaMemsetAsync(staged status)");
+    }
     upload(plan.d_adj_btiles, plan.adj_btiles);
     upload(plan.d_adj_ltiles, plan.adj_ltiles);
 }
 
 void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
 {
+    // ---- staged boxes (batched form): tensor maps and items
+    build_staged(plan);
+    auto staged = [&](int box) { return !plan.box_staged.empty() && plan.box_staged[box]; };
     // ---- forward
     const int B = plan.block;
     auto cap = [&](int unit) { return (uint32_t)(forward_per_thread(plan.per_thread, unit) * B); };
@@ -1413,13 +1430,21 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
         plan.xp_field[lg] = append_range(plan.xp, f);
     }
     // batched: one range, the most DRAM bytes per element (short rows) first, so that the first
-    // wave of CTAs starts on the most expensive tiles
+    // wave of CTAs starts on the most expensive tiles; staged boxes are the staged kernel's, and
+    // a pair moves as a pair only when neither of its boxes is staged
     {
+        auto paired = [&](int i) {
+            if (!plan.use_pairs || plan.box_pair[i] < 0) return false;
+            const auto& pr = plan.pairs[plan.box_pair[i]];
+            return !staged(pr.first) && !staged(pr.second);
+        };
         std::vector<xtile> all;
         for (size_t i = 0; i < plan.boxes.size(); ++i)
-            if (!plan.use_pairs || plan.box_pair[i] < 0) all.insert(all.end(), btiles[i].begin(), btiles[i].end());
+            if (!staged((int)i) && !paired((int)i)) all.insert(all.end(), btiles[i].begin(), btiles[i].end());
         if (plan.use_pairs)
-            for (const auto& v : ptiles) all.insert(all.end(), v.begin(), v.end());
+            for (size_t p = 0; p < ptiles.size(); ++p)
+                if (!staged(plan.pairs[p].first) && !staged(plan.pairs[p].second))
+                    all.insert(all.end(), ptiles[p].begin(), ptiles[p].end());
         for (const auto& v : ltiles) all.insert(all.end(), v.begin(), v.end());
         auto per_elem = [](const xtile& t) { return tile_cost(t) / std::max<uint32_t>(1u, t.count); };
         std::stable_sort(all.begin(), all.end(), [&](const xtile& x, const xtile& y) { return per_elem(x) > per_elem(y); });
@@ -1559,7 +1584,12 @@ void launch_plan(ghexb_plan_s& plan, int form, cudaStream_t stream)
     };
     switch (form)
     {
-        case GHEXB_FORM_BATCHED: run(plan.d_xf, {0, (int)plan.xf.size()}); break;
+        case GHEXB_FORM_BATCHED:
+            launch_staged_plan(plan, stream);
+            run(plan.d_xf, {0, (int)plan.xf.size()});
+            if (!plan.sitems.empty())
+                check_cuda(cudaStreamWaitEvent(stream, plan.join_event, 0), "cudaStreamWaitEvent(join)");
+            break;
         case GHEXB_FORM_PER_FIELD:
             for (const auto& r : plan.xp_field) run(plan.d_xp, r);
             break;
@@ -1654,6 +1684,20 @@ void adjoint_plan(ghexb_plan_s& plan, cudaStream_t stream)
     check_cuda(cudaGraphLaunch(plan.adj_exec, stream), "cudaGraphLaunch");
 }
 
+namespace
+{
+// stream-ordered rewrite of the descriptor tables the phased adjoint kernels read
+void put_descriptors(ghexb_plan_s& plan, cudaStream_t stream)
+{
+    auto put = [&](void* dst, const void* src, size_t bytes) {
+        if (bytes) check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync(rebind)");
+    };
+    put(plan.d_boxes, plan.boxes.data(), plan.boxes.size() * sizeof(box_desc));
+    put(plan.d_lists, plan.lists.data(), plan.lists.size() * sizeof(list_desc));
+    put(plan.d_adj_lists, plan.adj_lists.data(), plan.adj_lists.size() * sizeof(list_desc));
+}
+} // namespace
+
 void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stream)
 {
     if (n != (int)plan.fields.size())
@@ -1686,6 +1730,14 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
         plan.adj_lists[i].src = plan.fields[plan.adj_src_slot[i]].data + plan.adj_src_off[i];
         plan.adj_lists[i].dst = plan.fields[plan.adj_dst_slot[i]].data + plan.adj_dst_off[i];
     }
+    if (plan.staged_mode > 0)
+    {
+        // tensor maps hold addresses, and which boxes a map can load depends on the alignment of
+        // the new memory: the tables are rebuilt (and the graph recaptured on its next launch)
+        put_descriptors(plan, stream);
+        retile(plan, stream);
+        return;
+    }
     // stream-ordered rewrite of the tables; from pageable memory the copies return once staged.
     // The tile tables keep their size and device address, so a captured graph stays valid.
     build_tiles(plan, plan.d_idx);
@@ -1694,12 +1746,7 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
     copy_async(plan.d_xb, plan.xb, stream);
     copy_async(plan.d_gt, plan.gt, stream);
     copy_async(plan.d_lcols, plan.lcols, stream);
-    auto put = [&](void* dst, const void* src, size_t bytes) {
-        if (bytes) check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync(rebind)");
-    };
-    put(plan.d_boxes, plan.boxes.data(), plan.boxes.size() * sizeof(box_desc));
-    put(plan.d_lists, plan.lists.data(), plan.lists.size() * sizeof(list_desc));
-    put(plan.d_adj_lists, plan.adj_lists.data(), plan.adj_lists.size() * sizeof(list_desc));
+    put_descriptors(plan, stream);
 }
 
 void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
@@ -1709,12 +1756,19 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
     {
         int k, block;
         bool pairs;
+        int mode, stages, stage_bytes, consumers, ctas;
     };
+    const cand start{plan.per_thread, plan.block, plan.use_pairs, plan.staged_mode, plan.stages, plan.stage_bytes,
+        plan.stage_consumers, plan.stage_ctas_per_sm};
+    // the element kernel alone first; then, with its best shape, the staged form beside it
     std::vector<cand> cands;
     for (int k : {4, 8, 16})
         for (int block : {128, 256, 512})
             for (bool pairs : {false, true})
-                if (!pairs || !plan.pairs.empty()) cands.push_back({k, block, pairs});
+                if (!pairs || !plan.pairs.empty()) cands.push_back({k, block, pairs, 0, start.stages, start.stage_bytes,
+                                                       start.consumers, start.ctas});
+    const bool stageable = !plan.boxes.empty();
+    const size_t n_element = cands.size();
 
     // every timed launch starts with a cold L2: read a buffer of twice the L2 size first
     int l2 = 0;
@@ -1730,7 +1784,13 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
             if (e) cudaEventDestroy(e);
     };
     float best = 1e30f;
-    cand bestc{plan.per_thread, plan.block, plan.use_pairs};
+    cand bestc = start;
+    auto apply = [&](const cand& c) {
+        plan.per_thread = c.k, plan.block = c.block, plan.use_pairs = c.pairs;
+        plan.staged_mode = c.mode, plan.stages = c.stages, plan.stage_bytes = c.stage_bytes;
+        plan.stage_consumers = c.consumers, plan.stage_ctas_per_sm = c.ctas;
+        retile(plan, stream);
+    };
     try
     {
         check_cuda(cudaMalloc(&flush, flush_bytes), "cudaMalloc(l2 flush)");
@@ -1738,10 +1798,20 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         check_cuda(cudaMalloc(&sink, sizeof(unsigned)), "cudaMalloc(l2 flush sink)");
         for (auto& e : ev) check_cuda(cudaEventCreate(&e), "cudaEventCreate");
         const int fgrid = (plan.ctx ? plan.ctx->num_sms : 148) * 8;
-        for (const auto& c : cands)
+        for (size_t ci = 0; ci < cands.size(); ++ci)
         {
-            plan.per_thread = c.k, plan.block = c.block, plan.use_pairs = c.pairs;
-            retile(plan, stream);
+            if (ci == n_element && stageable)
+            {
+                // the staged form beside the best element-kernel shape
+                const cand e = bestc;
+                for (int mode : {1, 2})
+                    for (const auto& sh : std::vector<std::array<int, 4>>{{8, 16384, 4, 1}, {6, 16384, 8, 1}, {4, 16384, 4, 2},
+                             {12, 8192, 4, 1}})
+                        cands.push_back({e.k, e.block, e.pairs, mode, sh[0], sh[1], sh[2], sh[3]});
+            }
+            const cand& c = cands[ci];
+            apply(c);
+            if (c.mode > 0 && plan.sitems.empty()) continue; // nothing to stage
             for (int w = 0; w < 3; ++w) launch_plan(plan, GHEXB_FORM_BATCHED, stream); // warm-up
             // the launches queued back to back, each after a cold-L2 read outside its events, as
             // an application's exchanges follow its other kernels; the mean time per launch
@@ -1760,6 +1830,18 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
                 check_cuda(cudaEventElapsedTime(&ms, ev[2 * r], ev[2 * r + 1]), "cudaEventElapsedTime");
                 total += ms;
             }
+            // a staged candidate whose waits gave up is not a result
+            if (c.mode > 0 && plan.d_status)
+            {
+                unsigned st = 0;
+                check_cuda(cudaMemcpyAsync(&st, plan.d_status, sizeof st, cudaMemcpyDeviceToHost, stream), "cudaMemcpyAsync(status)");
+                check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+                if (st)
+                {
+                    check_cuda(cudaMemsetAsync(plan.d_status, 0, sizeof st, stream), "cudaMemsetAsync(status)");
+                    continue;
+                }
+            }
             if (total < best) best = total, bestc = c;
         }
     }
@@ -1769,8 +1851,7 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         throw;
     }
     cleanup();
-    plan.per_thread = bestc.k, plan.block = bestc.block, plan.use_pairs = bestc.pairs;
-    retile(plan, stream);
+    apply(bestc);
     check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
 }
 } // namespace ghexb
@@ -1779,6 +1860,11 @@ ghexb_plan_s::~ghexb_plan_s()
 {
     ghexb::release_graph(*this);
     if (cap_stream) cudaStreamDestroy(cap_stream);
+    if (side_stream) cudaStreamDestroy(side_stream);
+    if (fork_event) cudaEventDestroy(fork_event);
+    if (join_event) cudaEventDestroy(join_event);
+    for (void* p : {(void*)d_smaps, (void*)d_sitems, (void*)d_status})
+        if (p) cudaFree(p);
     for (void* p : {(void*)d_boxes, (void*)d_lists, (void*)d_adj_lists, (void*)d_idx, (void*)d_xf, (void*)d_xp,
              (void*)d_xb, (void*)d_gt, (void*)d_lcols, (void*)d_adj_btiles, (void*)d_adj_ltiles, (void*)d_counters})
         if (p) cudaFree(p);

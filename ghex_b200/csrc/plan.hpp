@@ -10,6 +10,7 @@
 
 #include "core.hpp"
 #include "exchange.hpp"
+#include "staged.hpp"
 
 struct ghexb_plan_s
 {
@@ -102,6 +103,34 @@ struct ghexb_plan_s
     int block = 256;
     bool use_pairs = true; // batched and per-field tables move x-face pairs as segments
 
+    // Staged form of box descriptors (staged.hpp), batched form only: the boxes marked in
+    // box_staged are loaded through tensor maps by the staged kernel, which runs beside the
+    // element kernel (its tiles are then the other boxes, the pairs of unstaged boxes and the
+    // lists). staged_mode 0: none; 1: boxes of rows of at most 64 bytes and boxes whose source
+    // rows run along the destination's second axis; 2: every box a tensor map can load.
+    int staged_mode = 0;
+    int stage_bytes = 16384, stages = 8, stage_consumers = 4, stage_ctas_per_sm = 1;
+    std::vector<char> box_staged;
+    std::vector<char> field_on_device; // per field: device memory (set when the plan is uploaded)
+    bool encode_maps = true;           // false for host-only checks: geometry without tensor maps
+    struct smap_info // host copy of a tensor map's geometry, for the replay check
+    {
+        const char* base;
+        int64_t dims[3], strides[2]; // elements; byte strides of dimensions 1 and 2
+        int es, w, h, d;             // element size, load box
+        int slot;                    // source field slot
+    };
+    std::vector<CUtensorMap> smaps;
+    std::vector<smap_info> smap_host;
+    std::vector<ghexb::sitem> sitems;
+    std::vector<int> sitem_box; // per item: its box descriptor
+    CUtensorMap* d_smaps = nullptr;
+    ghexb::sitem* d_sitems = nullptr;
+    unsigned* d_status = nullptr;
+    size_t cap_smaps = 0, cap_sitems = 0;
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t fork_event = nullptr, join_event = nullptr;
+
     // graphs of the batched form and of the adjoint, captured on first use
     cudaStream_t cap_stream = nullptr;
     cudaGraph_t graph = nullptr;
@@ -145,6 +174,15 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats);
 // recomputes the descriptor pointers and rewrites the device tables on `stream`.
 void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stream);
 void check_cuda(cudaError_t e, const char* what);
+// Host-only: decides which boxes the staged kernel takes (plan.staged_mode) and builds their
+// tensor maps and items (staged_plan.cu).
+void build_staged(ghexb_plan_s& plan);
+// Host replay of every staged item's element: the load coordinates stay inside the map, the
+// source and destination inside their fields, and the items move exactly their boxes' elements.
+// Returns the elements checked.
+int64_t check_staged(const ghexb_plan_s& plan);
+// The staged kernel of the batched form on a side stream forked from and joined to `stream`.
+void launch_staged_plan(ghexb_plan_s& plan, cudaStream_t stream);
 // Host-only: the least DRAM traffic of one exchange with a cold cache at the given sector size:
 // every sector holding a source element is read, every sector holding a destination element is
 // written back, and a sector written in part that holds no source element is read first.

@@ -69,7 +69,16 @@ typedef struct ghexb_plan_info_t
     int32_t pairs;             /* pairs of x-face boxes whose rows interleave in memory */
     int32_t use_pairs;         /* current tuning: 1 if the batched and per-field forms move those
                                   pairs as contiguous row-boundary segments */
-    int32_t reserved;
+    int32_t staged_mode;       /* current tuning: boxes the batched form loads through tensor maps
+                                  (0 none, 1 rows of at most 64 bytes and transposed edges, 2 all
+                                  it can) */
+    int32_t staged_boxes;      /* boxes the staged kernel takes */
+    int32_t staged_items;      /* its work items (one tensor-map load each) */
+    int32_t staged_maps;       /* its tensor maps */
+    int32_t stages;            /* current tuning: shared-memory stages per staged CTA */
+    int32_t stage_bytes;       /* current tuning: bytes per stage */
+    int32_t stage_consumers;   /* current tuning: consumer warps per staged CTA */
+    int32_t stage_ctas_per_sm; /* current tuning: staged CTAs per SM */
 } ghexb_plan_info_t;
 
 /* ---- errors / version ----------------------------------------------------------------- */
@@ -222,7 +231,9 @@ int ghexb_plan_create_ipr(ghexb_context ctx, const ghexb_field* fields, int n, g
 int ghexb_plan_destroy(ghexb_plan plan);
 /* Host-only validation, no device needed: builds the plan's tables and replays the address
  * computation of every element the forward and adjoint kernels touch, failing with
- * GHEXB_ERR_RANGE if one falls outside its field's memory span. */
+ * GHEXB_ERR_RANGE if one falls outside its field's memory span. The staged form is replayed in
+ * every mode at two stage sizes (its loads inside their tensor maps, every staged box's elements
+ * moved once); elements_checked counts the element kernel's form. */
 int ghexb_plan_check(ghexb_context ctx, const ghexb_field* fields, int n, int64_t* elements_checked);
 int ghexb_plan_get_info(ghexb_plan plan, ghexb_plan_info_t* info);
 /* Host-only, no device needed: the least DRAM traffic of one exchange of these fields from a
@@ -238,6 +249,19 @@ int ghexb_plan_dram_floor(ghexb_context ctx, const ghexb_field* fields, int n, i
  * use_pairs: 1 moves the x-face pairs as contiguous segments, 0 as separate boxes, < 0 keeps.
  * Invalidates the captured graph. */
 int ghexb_plan_set_tuning(ghexb_plan plan, int elems_per_thread, int block, int use_pairs);
+/* Staged form of the batched exchange (no GHEX counterpart): the boxes selected by `mode` (0
+ * none, 1 rows of at most 64 bytes and edges whose source rows run along the destination's second
+ * axis, 2 every box a tensor map can load) are moved by a second kernel that loads their source
+ * regions into shared memory through tensor maps (cp.async.bulk.tensor) and writes the halos from
+ * there, beside the element kernel; `stages` (2..16) stages of `stage_bytes` (a multiple of 128)
+ * per CTA, `consumers` (1..8) writing warps per CTA, `ctas_per_sm` CTAs per SM. Values <= 0 keep
+ * the current one (mode < 0 keeps). Fields in host memory stay on the element kernel.
+ * Invalidates the captured graph. */
+int ghexb_plan_set_staged(ghexb_plan plan, int mode, int stages, int stage_bytes, int consumers, int ctas_per_sm);
+/* Status word of the staged kernel since the last call, then cleared: 0 when every wait of the
+ * kernel ended in time; bit 0 a load, bit 1 a write that gave up waiting (its halos are then
+ * incomplete). Synchronises the device. */
+int ghexb_plan_staged_status(ghexb_plan plan, unsigned* status);
 /* One forward exchange in the given form, stream-ordered. */
 int ghexb_plan_launch(ghexb_plan plan, int form, void* stream);
 /* The batched form captured once into a CUDA graph and replayed on `stream`. */
