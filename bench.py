@@ -64,10 +64,16 @@ def parse():
     ap.add_argument("--no-configs", action="store_true", help="skip the other workloads")
     ap.add_argument("--baseline-seconds", type=float, default=10.0)
     ap.add_argument("--calibrate", action="store_true",
-                    help="time torch's own strided copies of the exchange's access patterns (rows of n elements at a "
-                         "row stride) and a contiguous copy, cold L2, and print one JSON line")
+                    help="time a plain row-copy kernel on the exchange's access pattern (rows of n elements at a row "
+                         "stride) and contiguous copies, cold L2, and print one JSON line")
+    ap.add_argument("--calibrate-host", action="store_true",
+                    help="the same row pattern in pinned host memory (the e2e form's access over the host "
+                         "interconnect) and host<->device copies")
     ap.add_argument("--profile", choices=["batched", "per_field", "adjoint"], default=None,
                     help="only run `--steps` launches of one form after `--warmup` (for ncu captures)")
+    ap.add_argument("--tuning", default=None,
+                    help="with --profile: the tuning to launch at, as printed in the bench line's "
+                         "roofline.traffic_tuning (e.g. k8.b128.p0.s1.st8x16384.c4.g1); default: the autotuner's")
     return ap.parse_args()
 
 
@@ -81,15 +87,66 @@ def peaks() -> tuple[float, str]:
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic(cfg: str):
-    """DRAM bytes per launch of the exchange kernel from the committed ncu summary, if any."""
+TUNING_KEYS = ("elems_per_thread", "block", "grid", "pairs", "use_pairs", "staged_mode", "staged_boxes", "staged_items",
+               "stages", "stage_bytes", "stage_consumers", "stage_ctas_per_sm")
+
+
+def tuning_key(info: dict) -> str:
+    """The tuning that decides a launch's kernels and their shapes, as a short string (the key of
+    profiles/traffic.json)."""
+    k = f"k{info['elems_per_thread']}.b{info['block']}.p{info['use_pairs']}.s{info['staged_mode']}"
+    if info["staged_mode"]:
+        k += f".st{info['stages']}x{info['stage_bytes']}.c{info['stage_consumers']}.g{info['stage_ctas_per_sm']}"
+    return k
+
+
+def apply_tuning(plan, key: str) -> None:
+    """Sets a plan to the tuning named by tuning_key()."""
+    parts = {}
+    for tok in key.split("."):
+        if tok.startswith("st"):
+            a, b = tok[2:].split("x")
+            parts["stages"], parts["stage_bytes"] = int(a), int(b)
+        else:
+            parts[tok[0]] = int(tok[1:])
+    plan.set_tuning(parts["k"], parts["b"], parts["p"])
+    plan.set_staged(parts["s"], parts.get("stages", 0), parts.get("stage_bytes", 0), parts.get("c", 0), parts.get("g", 0))
+    if tuning_key(plan.info()) != key:
+        raise ValueError(f"tuning {key} not applied: {tuning_key(plan.info())}")
+
+
+def ncu_traffic(cfg: str, key: str):
+    """DRAM bytes per launch of the batched form (all its kernels) from the committed ncu summary,
+    captured at this tuning; None when no capture of this tuning is committed."""
     p = ROOT / "profiles" / "traffic.json"
     if p.exists():
         try:
-            return json.loads(p.read_text()).get(cfg)
+            entry = json.loads(p.read_text()).get(cfg, {}).get(key)
+            return entry if isinstance(entry, dict) else None
         except Exception:
             return None
     return None
+
+
+def roofline_block(alg: float, ms: float, peak: float, peak_kind: str, plan, cfg: str, info: dict) -> dict:
+    """Achieved algorithmic GB/s against the measured HBM copy bandwidth; beside it the DRAM floor
+    of the exchange (the sectors it cannot avoid, 32-byte granularity) and, where an ncu capture of
+    this tuning is committed, the measured DRAM traffic per launch."""
+    achieved = alg / (ms * 1e-3) / 1e9
+    out = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+           "peak_source": peak_kind}
+    fl = plan.dram_floor(32)
+    out["floor"] = {"sector_bytes": 32, "bytes": fl["total"], "read": fl["read"], "write": fl["write"],
+                    "alg_over_floor": alg / fl["total"],
+                    "frac_on_floor": fl["total"] / (ms * 1e-3) / 1e9 / peak}
+    key = tuning_key(info)
+    tr = ncu_traffic(cfg, key)
+    out["traffic"] = tr["dram_bytes"] if tr else None
+    out["traffic_tuning"] = key
+    if tr:
+        out["dram_frac"] = tr["dram_bytes"] / (ms * 1e-3) / 1e9 / peak
+        out["traffic_capture"] = tr.get("capture")
+    return out
 
 
 # ------------------------------------------------------------------------------------------
@@ -586,13 +643,19 @@ def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline
     s = timer.stream.cuda_stream
     tuning = plan.autotune(repeats=20, stream=s) if autotune else plan.info()
     ms_b = timer(lambda: plan.graph_launch(s), steps, warmup)
+    ms_warm = timer(lambda: plan.graph_launch(s), steps, warmup, mode="warm")
+    ms_wb = timer(lambda: plan.graph_launch(s), steps, warmup, mode="writeback")
     ms_f = timer(lambda: plan.launch(plan.PER_FIELD, s), max(10, steps // 2), warmup)
     out = {"workload": case.w.name, "algorithmic_bytes": case.alg, "dtype": case.dtype,
            "batched": {"ms": ms_b, "GB/s": case.alg / ms_b / 1e6, "exchanges_per_s": 1e3 / ms_b,
                        "roofline_frac": case.alg / ms_b / 1e6 / peak},
+           "l2": {"cold_ms": ms_b, "warm_ms": ms_warm, "cold_with_writeback_ms": ms_wb},
+           "roofline": roofline_block(case.alg, ms_b, peak, "measured", plan, cfg, plan.info()),
            "per_field": {"ms": ms_f, "GB/s": case.alg / ms_f / 1e6, "exchanges_per_s": 1e3 / ms_f},
            "batched_vs_per_field": ms_f / ms_b,
-           "tuning": {k: tuning[k] for k in ("elems_per_thread", "block", "grid", "pairs", "use_pairs")}}
+           "tuning": {k: tuning[k] for k in TUNING_KEYS}}
+    if plan.info()["staged_mode"]:
+        out["staged_status"] = plan.staged_status()
     if cfg in ("cfg4", "cfg4_f32"):
         ms_a = timer(lambda: plan.adjoint(s), steps, warmup)
         out["adjoint"] = {"ms": ms_a, "vs_forward": ms_a / ms_b, "launches": plan.info()["adjoint_launches"]}
@@ -696,35 +759,51 @@ def measure_staged(dev, timer, peak, steps, warmup, autotune=True, baseline=True
 
 
 def calibrate(args):
-    """The access-pattern roofline: how fast a library copy kernel (torch's strided copy_) moves
-    rows of n float64 elements spaced one x-row of a halo field apart (stride 139 elements, as in
-    the x faces of the 400x300x96 workload), against a contiguous copy of the same bytes. Every
-    timed copy starts with a cold L2."""
+    """Access-pattern calibration: how fast a plain kernel (ghexb_calibrate_rows: the exchange
+    kernel's lane mapping without its work records) moves rows of n float64 elements spaced one
+    x-row of a halo field apart (stride 139 elements, 96 x 3000 rows, as the x faces of the
+    400x300x96 workload), cold L2 (device) or from pinned host memory over the host interconnect
+    (--calibrate-host), beside contiguous copies of the same bytes. Prints one JSON line."""
+    import ctypes as C
     import torch
+    from ghex_b200 import _capi
     dev = torch.device("cuda", 0)
     stream = torch.cuda.Stream(device=dev)
     l2 = torch.cuda.get_device_properties(dev).L2_cache_size
     flush = torch.ones(max(2 * l2, 64 << 20) // 4, dtype=torch.float32, device=dev)
     timer = Timer(stream, flush, 1, dev)
-    warm = Timer(stream, None, 1, dev)
-    out = {"calibration": "torch copy_ of views, CUDA events; cold: after an L2 flush, warm: the rows' lines "
-                          "resident in L2 from the previous copy", "rows": {}}
-    a = torch.zeros(96, 3000, 139, dtype=torch.float64, device=dev)
-    b = torch.zeros_like(a)
-    for n in (1, 3, 8, 32, 128):
-        src, dst = a[:, :, 3:3 + n], b[:, :, 0:n]
-        rows = src.shape[0] * src.shape[1]
-        ms = timer(lambda: dst.copy_(src), 20, 3)
+    host = args.calibrate_host
+    where = "pinned host memory, mapped for the device" if host else "device memory, cold L2"
+    out = {"calibration": f"ghexb_calibrate_rows, rows of n float64 spaced 139 elements apart, {where}; CUDA events, "
+                          "mean of the timed launches", "rows": {}}
+    shape = (96, 3000, 139)
+    if host:
+        a = torch.zeros(shape, dtype=torch.float64, pin_memory=True)
+        b = torch.zeros(shape, dtype=torch.float64, pin_memory=True)
+    else:
+        a = torch.zeros(shape, dtype=torch.float64, device=dev)
+        b = torch.zeros_like(a)
+    rows = shape[0] * shape[1]
+    for n in ((1, 3, 6, 12) if host else (1, 3, 8, 32, 128)):
+        def launch(n=n):
+            _capi.call("ghexb_calibrate_rows", C.c_void_p(a.data_ptr() + 3 * 8), C.c_void_p(b.data_ptr()), rows, n,
+                       shape[2], shape[2], 8, C.c_void_p(stream.cuda_stream))
+        ms = timer(launch, 5 if host else 20, 2 if host else 3)
         out["rows"][f"n={n}"] = {"rows": rows, "us": ms * 1e3, "rows_per_ns": rows / (ms * 1e6),
                                  "useful_GB/s": 2 * rows * n * 8 / (ms * 1e-3) / 1e9}
-        if n <= 8:
-            ms = warm(lambda: dst.copy_(src), 20, 3)
-            out["rows"][f"n={n}"]["warm_rows_per_ns"] = rows / (ms * 1e6)
-    for mb in (8, 35, 70):
-        x = torch.ones(mb * (1 << 20) // 8, dtype=torch.float64, device=dev)
-        y = torch.empty_like(x)
-        ms = timer(lambda: y.copy_(x), 20, 3)
-        out[f"contiguous_{mb}MB"] = {"us": ms * 1e3, "GB/s (read+write)": 2 * x.numel() * 8 / (ms * 1e-3) / 1e9}
+    if host:
+        x = torch.ones(64 << 20 >> 3, dtype=torch.float64, pin_memory=True)
+        y = torch.empty(64 << 20 >> 3, dtype=torch.float64, device=dev)
+        ms = timer(lambda: y.copy_(x, non_blocking=True), 5, 2)
+        out["h2d_64MB"] = {"us": ms * 1e3, "GB/s": x.numel() * 8 / (ms * 1e-3) / 1e9}
+        ms = timer(lambda: x.copy_(y, non_blocking=True), 5, 2)
+        out["d2h_64MB"] = {"us": ms * 1e3, "GB/s": x.numel() * 8 / (ms * 1e-3) / 1e9}
+    else:
+        for mb in (8, 35, 70):
+            x = torch.ones(mb * (1 << 20) // 8, dtype=torch.float64, device=dev)
+            y = torch.empty_like(x)
+            ms = timer(lambda: y.copy_(x), 20, 3)
+            out[f"contiguous_{mb}MB"] = {"us": ms * 1e3, "GB/s (read+write)": 2 * x.numel() * 8 / (ms * 1e-3) / 1e9}
     print(json.dumps(out), flush=True)
 
 
@@ -733,7 +812,7 @@ def main():
     if args.impl == "reference":
         run_reference(args)
         return
-    if args.calibrate:
+    if args.calibrate or args.calibrate_host:
         calibrate(args)
         return
     import torch
@@ -751,13 +830,17 @@ def main():
     case = Case(args.config, dev, local)
     plan = case.plan
     if args.profile:
+        if args.tuning:
+            apply_tuning(plan, args.tuning)
+        else:
+            plan.autotune(repeats=20)
         launch = {"batched": lambda: plan.launch(plan.BATCHED), "per_field": lambda: plan.launch(plan.PER_FIELD),
                   "adjoint": lambda: plan.adjoint()}[args.profile]
         for _ in range(args.warmup + args.steps):
             launch()
         torch.cuda.synchronize()
         print(json.dumps({"profile": args.profile, "config": case.w.name, "launches": args.warmup + args.steps,
-                          "plan": plan.info()}), flush=True)
+                          "tuning": tuning_key(plan.info()), "plan": plan.info()}), flush=True)
         return
     alg = case.alg
     stream = torch.cuda.Stream(device=dev)
@@ -767,13 +850,18 @@ def main():
     peak, peak_kind = peaks()
     s = stream.cuda_stream
     tuning = plan.info() if args.no_autotune else plan.autotune(repeats=20, stream=s)
-    info = plan.info()
 
     sampler = ClockSampler(dev.index)
     with sampler:
         ms_batched = timer(lambda: plan.graph_launch(s), args.steps, max(3, args.warmup))
     clocks = sampler.summary()
-    launches = args.steps  # one kernel per graph launch
+    info = plan.info()
+    # kernels per graph launch: the element kernel, and the staged kernel beside it when it has items
+    kernels = (1 if info["num_tiles"] > 0 else 0) + (1 if info["staged_items"] > 0 else 0)
+    launches = args.steps * kernels
+    staged_status = plan.staged_status() if info["staged_mode"] else 0
+    ms_warm = timer(lambda: plan.graph_launch(s), args.steps, max(3, args.warmup), mode="warm")
+    ms_wb = timer(lambda: plan.graph_launch(s), args.steps, max(3, args.warmup), mode="writeback")
     k_small = max(10, min(args.steps, 200))
     ms_field = timer(lambda: plan.launch(plan.PER_FIELD, s), k_small, max(3, args.warmup))
     ms_box = timer(lambda: plan.launch(plan.PER_BOX, s), max(5, k_small // 4), 3)
@@ -781,7 +869,6 @@ def main():
     e2e, h2d, d2h, e2e_ok = e2e_host_ms(case, max(10, min(args.steps, 200)), max(3, args.warmup), world, dev)
 
     achieved = alg / (ms_batched * 1e-3) / 1e9
-    traffic = ncu_traffic(args.config)
     n_logical = len({f[0] for f in case.fields})
     line = {
         "metric": METRIC, "value": world * achieved, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
@@ -792,15 +879,17 @@ def main():
                    "l2": "cold: a read of an unrelated buffer of twice the L2 size before every timed exchange, "
                          "outside its events",
                    "parallelism": f"replicas x{world}",
-                   "tuning": {k: tuning[k] for k in ("elems_per_thread", "block", "grid", "pairs", "use_pairs")}},
+                   "tuning": {k: tuning[k] for k in TUNING_KEYS}},
         "exchanges_per_s": world * 1e3 / ms_batched,
         "per_field": {"ms_per_step": ms_field, "GB/s": world * alg / (ms_field * 1e-3) / 1e9,
                       "exchanges_per_s": world * 1e3 / ms_field, "launches_per_exchange": n_logical},
         "per_box": {"ms_per_step": ms_box, "GB/s": world * alg / (ms_box * 1e-3) / 1e9,
                     "exchanges_per_s": world * 1e3 / ms_box, "launches_per_exchange": info["num_descriptors"]},
         "batched_vs_per_field": ms_field / ms_batched,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_kind, "traffic": traffic},
+        "roofline": roofline_block(alg, ms_batched, peak, peak_kind, plan, args.config, info),
+        "l2": {"cold_ms": ms_batched, "warm_ms": ms_warm, "cold_with_writeback_ms": ms_wb,
+               "warm": "steps back to back, no flush", "cold_with_writeback": "the events also span the flush after "
+               "the exchange, minus a flush after a flush: the exchange plus the write-back of what it dirtied"},
         "e2e": {"value": world * alg / (e2e * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e, "bitexact": e2e_ok,
                 "form": "fields in pinned host memory, co.exchange(...).wait() per step: the exchange kernel reads "
@@ -809,10 +898,11 @@ def main():
                               "h2d_bytes_per_step": copy_bytes, "d2h_bytes_per_step": copy_bytes,
                               "form": "every field copied to the device, exchanged there and copied back"}},
         "gpu_launches": launches,
+        "kernels_per_exchange": kernels,
         "clocks": clocks,
     }
-    if traffic:
-        line["roofline"]["dram_frac"] = traffic / (ms_batched * 1e-3) / 1e9 / peak
+    if info["staged_mode"]:
+        line["staged_status"] = staged_status
     if rank == 0 and world == 1 and not args.no_baseline:
         case.reset()
         plan.launch(plan.BATCHED, s)

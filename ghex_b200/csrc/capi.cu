@@ -766,6 +766,22 @@ int ghexb_plan_autotune(ghexb_plan plan, void* stream, int repeats, ghexb_plan_i
     });
 }
 
+int ghexb_calibrate_rows(const void* src, void* dst, int64_t rows, int n, int64_t src_stride, int64_t dst_stride,
+    int elem_bytes, void* stream)
+{
+    return guarded([&] {
+        require(src && dst, "null argument");
+        require(rows >= 1 && rows < (int64_t(1) << 32) && n >= 1 && n <= 256, "rows or row length out of range");
+        require(elem_bytes == 4 || elem_bytes == 8, "elements of 4 or 8 bytes");
+        require(src_stride >= n && dst_stride >= n, "row strides shorter than the rows");
+        ghexb::check_accessible(src, (size_t)((rows - 1) * src_stride + n) * elem_bytes);
+        ghexb::check_accessible(dst, (size_t)((rows - 1) * dst_stride + n) * elem_bytes);
+        ghexb::check_cuda(ghexb::launch_row_copy(src, dst, (uint32_t)rows, (uint32_t)n, src_stride, dst_stride, elem_bytes,
+                              static_cast<cudaStream_t>(stream)),
+            "row copy launch");
+    });
+}
+
 int ghexb_stencil7(int dtype, int n, const void* const* in, void* const* out, const int64_t* extents,
                    const int64_t* strides, int halo, double alpha, int adjoint, void* stream)
 {

@@ -225,7 +225,52 @@ __global__ void __launch_bounds__(256) l2_flush_kernel(const uint4* __restrict__
     if (acc == 0x9e3779b9u) *sink = acc;
 }
 
+// Calibration copy of short rows: dst[r*dst_stride + i] = src[r*src_stride + i] for r < rows, i < n;
+// consecutive threads take consecutive elements, each thread 8 elements (all loads before any
+// store), as the exchange kernel moves the rows of a box, without its tile records.
+template<typename T>
+__global__ void __launch_bounds__(256) row_copy_kernel(const T* __restrict__ src, T* __restrict__ dst, uint32_t rows,
+    uint32_t n, int64_t src_stride, int64_t dst_stride)
+{
+    constexpr int K = 8;
+    const uint64_t total = (uint64_t)rows * n;
+    T v[K];
+    int64_t o[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+    {
+        const uint64_t e = ((uint64_t)blockIdx.x * K + k) * blockDim.x + threadIdx.x;
+        o[k] = -1;
+        if (e < total)
+        {
+            const uint64_t r = e / n, i = e - r * n;
+            v[k] = __ldcg(src + r * src_stride + i);
+            o[k] = (int64_t)(r * dst_stride + i);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if (o[k] >= 0) __stcg(dst + o[k], v[k]);
+}
+
 } // namespace
+
+cudaError_t launch_row_copy(const void* src, void* dst, uint32_t rows, uint32_t n, int64_t src_stride,
+    int64_t dst_stride, int es, cudaStream_t stream)
+{
+    const uint64_t total = (uint64_t)rows * n;
+    if (total == 0) return cudaSuccess;
+    const unsigned grid = (unsigned)((total + 8 * 256 - 1) / (8 * 256));
+    if (es == 8)
+        row_copy_kernel<<<grid, 256, 0, stream>>>(static_cast<const unsigned long long*>(src),
+            static_cast<unsigned long long*>(dst), rows, n, src_stride, dst_stride);
+    else if (es == 4)
+        row_copy_kernel<<<grid, 256, 0, stream>>>(static_cast<const unsigned*>(src), static_cast<unsigned*>(dst), rows, n,
+            src_stride, dst_stride);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
 
 cudaError_t launch_l2_flush(const uint4* buf, size_t n16, unsigned* sink, int grid, cudaStream_t stream)
 {

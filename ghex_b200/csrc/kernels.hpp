@@ -20,4 +20,8 @@ cudaError_t launch_list_adjoint(const list_desc* lists, const tile* tiles, int n
 // `sink` receives a value only when the data sum to a sentinel that a zero-filled buffer never
 // produces, which keeps the loads alive.
 cudaError_t launch_l2_flush(const uint4* buf, size_t n16, unsigned* sink, int grid, cudaStream_t stream);
+
+// Calibration copy of `rows` rows of n elements of es (4 or 8) bytes at the given element strides.
+cudaError_t launch_row_copy(const void* src, void* dst, uint32_t rows, uint32_t n, int64_t src_stride,
+    int64_t dst_stride, int es, cudaStream_t stream);
 } // namespace ghexb

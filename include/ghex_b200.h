@@ -294,6 +294,14 @@ int ghexb_plan_autotune(ghexb_plan plan, void* stream, int repeats, ghexb_plan_i
  * overlap on the GPU race on it. */
 int ghexb_exchange_noalloc(ghexb_context ctx, const ghexb_field* fields, int n, void* stream);
 
+/* ---- calibration (no GHEX counterpart): copies `rows` rows of n elements (4 or 8 bytes) at the
+ * given element strides, dst[r*dst_stride + i] = src[r*src_stride + i], with the lane mapping of
+ * the exchange kernel's box tiles (consecutive threads take consecutive elements, 8 loads in flight
+ * per thread) but no work records: the rate at which a plain kernel moves such rows, from device
+ * or from mapped host memory, against which the exchange of the same rows is compared. */
+int ghexb_calibrate_rows(const void* src, void* dst, int64_t rows, int n, int64_t src_stride, int64_t dst_stride,
+    int elem_bytes, void* stream);
+
 /* ---- the compute step of the differentiable-exchange program. No counterpart in GHEX, which
  * has no stencil: this is the 7-point update x <- x + alpha * L(x) on the interior of each of n
  * 3-D domains (output halo set to 0), or with adjoint != 0 its transpose (gradient of the
