@@ -64,10 +64,22 @@ template<> __device__ __forceinline__ uint8_t ld_stream(const uint8_t* p)
     return __ldcg(reinterpret_cast<const unsigned char*>(p));
 }
 
+// CTAs start roughly in block order, about a thousand at a time: the record of the CTA that
+// starts a wave later is brought into L2 now, so that after the first wave a CTA's first round
+// trip is an L2 hit rather than a DRAM access (the tables are read once per exchange, cold after
+// other work has run).
+constexpr unsigned k_record_prefetch = 1024;
+
 // Loads this CTA's record (W 16-byte words) into shared memory.
 template<int W, typename R>
 __device__ __forceinline__ void load_record(R& t, const R* __restrict__ tiles)
 {
+    if (threadIdx.x == 32 && blockIdx.x + k_record_prefetch < gridDim.x)
+    {
+        const char* next = reinterpret_cast<const char*>(tiles + blockIdx.x + k_record_prefetch);
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(next));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(next + sizeof(R) - 1));
+    }
     if (threadIdx.x < W)
         reinterpret_cast<uint4*>(&t)[threadIdx.x] = __ldg(reinterpret_cast<const uint4*>(tiles + blockIdx.x) + threadIdx.x);
     __syncthreads();

@@ -34,14 +34,71 @@ namespace
 {
 constexpr int64_t k_i32max = 0x7fffffffLL;
 
+// Host-to-device copies of a plan's tables, stream-ordered, through the plan's page-locked
+// staging buffers: put() queues a copy; commit() takes the next buffer of the ring, waits until
+// the copies of its previous use have left it, packs the queued tables into it and issues the
+// copies on `stream`.
+class host_stager
+{
+  public:
+    host_stager(ghexb_plan_s& plan, cudaStream_t stream)
+    : m_plan(plan)
+    , m_stream(stream)
+    {
+    }
+    template<typename T>
+    void put(T* dptr, const std::vector<T>& v)
+    {
+        if (!v.empty()) m_q.push_back({dptr, v.data(), v.size() * sizeof(T)});
+    }
+    void commit()
+    {
+        size_t total = 0;
+        for (const auto& c : m_q) total += (c.bytes + 255) / 256 * 256;
+        if (total == 0) return;
+        auto& B = m_plan.h_stage[m_plan.h_stage_next];
+        m_plan.h_stage_next = (m_plan.h_stage_next + 1) % 4;
+        if (B.done) check_cuda(cudaEventSynchronize(B.done), "cudaEventSynchronize(staging)");
+        else
+            check_cuda(cudaEventCreateWithFlags(&B.done, cudaEventDisableTiming), "cudaEventCreate(staging)");
+        if (total > B.cap)
+        {
+            if (B.ptr) cudaFreeHost(B.ptr), B.ptr = nullptr, B.cap = 0;
+            check_cuda(cudaMallocHost(&B.ptr, total), "cudaMallocHost(plan staging)");
+            B.cap = total;
+        }
+        char* buf = static_cast<char*>(B.ptr);
+        size_t off = 0;
+        for (const auto& c : m_q)
+        {
+            std::memcpy(buf + off, c.src, c.bytes);
+            check_cuda(cudaMemcpyAsync(c.dst, buf + off, c.bytes, cudaMemcpyHostToDevice, m_stream),
+                "cudaMemcpyAsync(plan table)");
+            off += (c.bytes + 255) / 256 * 256;
+        }
+        check_cuda(cudaEventRecord(B.done, m_stream), "cudaEventRecord(staging)");
+        m_q.clear();
+    }
+
+  private:
+    struct copy
+    {
+        void* dst;
+        const void* src;
+        size_t bytes;
+    };
+    ghexb_plan_s& m_plan;
+    cudaStream_t m_stream;
+    std::vector<copy> m_q;
+};
+
 template<typename T>
-void upload(T*& dptr, const std::vector<T>& v)
+void upload(T*& dptr, const std::vector<T>& v, host_stager& st)
 {
     if (dptr) cudaFree(dptr), dptr = nullptr;
     if (v.empty()) return;
     check_cuda(cudaMalloc(&dptr, v.size() * sizeof(T)), "cudaMalloc(plan table)");
-    check_cuda(cudaMemcpy(dptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice),
-        "cudaMemcpy(plan table)");
+    st.put(dptr, v);
 }
 
 // One axis of a box: extent, first source/destination coordinates in field memory and the
@@ -857,7 +914,8 @@ void upload_plan(ghexb_plan_s& plan)
     plan.field_on_device.clear();
     for (const auto& f : plan.fields) plan.field_on_device.push_back(accessible_type(f.data) == cudaMemoryTypeDevice);
     // upload index lists, patch device pointers, upload descriptor tables
-    upload(plan.d_idx, plan.idx);
+    host_stager st(plan, nullptr);
+    upload(plan.d_idx, plan.idx, st);
     for (size_t i = 0; i < plan.lists.size(); ++i)
     {
         plan.lists[i].sidx = plan.d_idx + plan.list_idx_off[i];
@@ -868,11 +926,13 @@ void upload_plan(ghexb_plan_s& plan)
         plan.adj_lists[i].sidx = plan.d_idx + plan.adj_idx_off[i];
         plan.adj_lists[i].didx = plan.d_idx + plan.adj_didx_off[i];
     }
-    upload(plan.d_boxes, plan.boxes);
-    upload(plan.d_lists, plan.lists);
+    upload(plan.d_boxes, plan.boxes, st);
+    upload(plan.d_lists, plan.lists, st);
     // two scheduler counters per phased adjoint kernel
-    upload(plan.d_counters, std::vector<unsigned>(4, 0u));
-    upload(plan.d_adj_lists, plan.adj_lists);
+    const std::vector<unsigned> zeros(4, 0u);
+    upload(plan.d_counters, zeros, st);
+    upload(plan.d_adj_lists, plan.adj_lists, st);
+    st.commit();
     check_cuda(cudaStreamCreateWithFlags(&plan.cap_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     retile(plan);
     check_cuda(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
@@ -1273,13 +1333,6 @@ bool ensure(T*& dptr, size_t& cap, size_t n)
     return true;
 }
 
-template<typename T>
-void copy_async(T* dptr, const std::vector<T>& v, cudaStream_t stream)
-{
-    if (!v.empty())
-        check_cuda(cudaMemcpyAsync(dptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream),
-            "cudaMemcpyAsync(plan tiles)");
-}
 } // namespace
 
 void retile(ghexb_plan_s& plan, cudaStream_t stream)
@@ -1291,22 +1344,24 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
     ensure(plan.d_xb, plan.cap_xb, plan.xb.size());
     ensure(plan.d_gt, plan.cap_gt, plan.gt.size());
     ensure(plan.d_lcols, plan.cap_lcols, plan.lcols.size());
-    copy_async(plan.d_xf, plan.xf, stream);
-    copy_async(plan.d_xp, plan.xp, stream);
-    copy_async(plan.d_xb, plan.xb, stream);
-    copy_async(plan.d_gt, plan.gt, stream);
-    copy_async(plan.d_lcols, plan.lcols, stream);
     ensure(plan.d_smaps, plan.cap_smaps, plan.smaps.size());
     ensure(plan.d_sitems, plan.cap_sitems, plan.sitems.size());
-    copy_async(plan.d_smaps, plan.smaps, stream);
-    copy_async(plan.d_sitems, plan.sitems, stream);
+    host_stager st(plan, stream);
+    st.put(plan.d_xf, plan.xf);
+    st.put(plan.d_xp, plan.xp);
+    st.put(plan.d_xb, plan.xb);
+    st.put(plan.d_gt, plan.gt);
+    st.put(plan.d_lcols, plan.lcols);
+    st.put(plan.d_smaps, plan.smaps);
+    st.put(plan.d_sitems, plan.sitems);
     if (!plan.sitems.empty() && !plan.d_status)
     {
         check_cuda(cudaMalloc(&plan.d_status, sizeof(unsigned)), "cudaMalloc(staged status)");
         check_cuda(cudaMemsetAsync(plan.d_status, 0, sizeof(unsigned), stream), "cudaMemsetAsync(staged status)");
     }
-    upload(plan.d_adj_btiles, plan.adj_btiles);
-    upload(plan.d_adj_ltiles, plan.adj_ltiles);
+    upload(plan.d_adj_btiles, plan.adj_btiles, st);
+    upload(plan.d_adj_ltiles, plan.adj_ltiles, st);
+    st.commit();
 }
 
 void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
@@ -1689,12 +1744,11 @@ namespace
 // stream-ordered rewrite of the descriptor tables the phased adjoint kernels read
 void put_descriptors(ghexb_plan_s& plan, cudaStream_t stream)
 {
-    auto put = [&](void* dst, const void* src, size_t bytes) {
-        if (bytes) check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync(rebind)");
-    };
-    put(plan.d_boxes, plan.boxes.data(), plan.boxes.size() * sizeof(box_desc));
-    put(plan.d_lists, plan.lists.data(), plan.lists.size() * sizeof(list_desc));
-    put(plan.d_adj_lists, plan.adj_lists.data(), plan.adj_lists.size() * sizeof(list_desc));
+    host_stager st(plan, stream);
+    st.put(plan.d_boxes, plan.boxes);
+    st.put(plan.d_lists, plan.lists);
+    st.put(plan.d_adj_lists, plan.adj_lists);
+    st.commit();
 }
 } // namespace
 
@@ -1738,15 +1792,19 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
         retile(plan, stream);
         return;
     }
-    // stream-ordered rewrite of the tables; from pageable memory the copies return once staged.
-    // The tile tables keep their size and device address, so a captured graph stays valid.
+    // stream-ordered rewrite of the tables. The tile tables keep their size and device address,
+    // so a captured graph stays valid.
     build_tiles(plan, plan.d_idx);
-    copy_async(plan.d_xf, plan.xf, stream);
-    copy_async(plan.d_xp, plan.xp, stream);
-    copy_async(plan.d_xb, plan.xb, stream);
-    copy_async(plan.d_gt, plan.gt, stream);
-    copy_async(plan.d_lcols, plan.lcols, stream);
-    put_descriptors(plan, stream);
+    host_stager st(plan, stream);
+    st.put(plan.d_xf, plan.xf);
+    st.put(plan.d_xp, plan.xp);
+    st.put(plan.d_xb, plan.xb);
+    st.put(plan.d_gt, plan.gt);
+    st.put(plan.d_lcols, plan.lcols);
+    st.put(plan.d_boxes, plan.boxes);
+    st.put(plan.d_lists, plan.lists);
+    st.put(plan.d_adj_lists, plan.adj_lists);
+    st.commit();
 }
 
 void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
@@ -1861,6 +1919,11 @@ ghexb_plan_s::~ghexb_plan_s()
     ghexb::release_graph(*this);
     if (cap_stream) cudaStreamDestroy(cap_stream);
     if (side_stream) cudaStreamDestroy(side_stream);
+    for (auto& b : h_stage)
+    {
+        if (b.done) cudaEventSynchronize(b.done), cudaEventDestroy(b.done);
+        if (b.ptr) cudaFreeHost(b.ptr);
+    }
     if (fork_event) cudaEventDestroy(fork_event);
     if (join_event) cudaEventDestroy(join_event);
     for (void* p : {(void*)d_smaps, (void*)d_sitems, (void*)d_status})

@@ -130,6 +130,18 @@ struct ghexb_plan_s
     size_t cap_smaps = 0, cap_sitems = 0;
     cudaStream_t side_stream = nullptr;
     cudaEvent_t fork_event = nullptr, join_event = nullptr;
+    // Page-locked staging of the table uploads (plan.cu host_stager): copies never read the
+    // library's pageable heap memory, which may share pages with host fields that the page
+    // registry has locked (a copy whose source straddles a locked range is refused by CUDA).
+    // A ring of four buffers, each reused once the copies out of its previous use are done.
+    struct stage_buffer
+    {
+        void* ptr = nullptr;
+        size_t cap = 0;
+        cudaEvent_t done = nullptr;
+    };
+    stage_buffer h_stage[4];
+    int h_stage_next = 0;
 
     // graphs of the batched form and of the adjoint, captured on first use
     cudaStream_t cap_stream = nullptr;
