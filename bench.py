@@ -593,19 +593,25 @@ def e2e_ms(case, stream, steps, world, dev):
     return max_over_ranks(e0.elapsed_time(e1) / steps, world, dev), h2d
 
 
-def e2e_host_ms(case, steps, warmup, world, dev):
+def e2e_host_ms(case, steps, warmup, world, dev, alloc="library"):
     """Public API end to end on host fields: the fields live in pinned host memory and every step
     is `co.exchange(...).wait()` on them; the exchange kernel reads the source cells from host
     memory and writes the halo cells into it over the host interconnect, and wait() returns when
     the halos are in host memory. Returns (ms per step, bytes read from host, bytes written to
     host, bit-exact against the device-resident exchange)."""
     import torch
+    from ghex_b200 import host_empty
     host = []
     for f in case.fields:
         ts = []
         for a in f[1]:
             src = torch.from_numpy(a)
-            t = torch.empty_strided(tuple(src.shape), tuple(src.stride()), dtype=src.dtype, pin_memory=True)
+            if alloc == "library":
+                # page-locked, mapped host memory from the library (cudaHostAlloc)
+                t = torch.from_numpy(host_empty(a.shape, a.dtype, order="F" if a.flags["F_CONTIGUOUS"] else "C"))
+            else:
+                t = torch.empty_strided(tuple(src.shape), tuple(src.stride()), dtype=src.dtype, pin_memory=True)
+            assert t.stride() == src.stride()
             t.copy_(src)
             ts.append(t)
         host.append(ts)
@@ -710,7 +716,7 @@ def measure_program(dev, timer, dtype, steps, warmup, baseline=True) -> dict:
     res = {"workload": w.name + f", {nsteps} x (exchange, 7-point update), loss = sum of squares, forward + backward",
            "dtype": np.dtype(dtype).name.replace("float", "f"),
            "forward_backward_ms": ms_fb, "forward_ms": ms_f, "inner_steps": nsteps,
-           "forward_backward_ms_per_inner_step": ms_fb / nsteps}
+           "forward_backward_ms_per_inner_step": ms_fb / nsteps, "plan_pool": dx.pool_stats()}
     if baseline:
         from oracle import regular as O
         from oracle import stencil as S
@@ -773,13 +779,19 @@ def calibrate(args):
     flush = torch.ones(max(2 * l2, 64 << 20) // 4, dtype=torch.float32, device=dev)
     timer = Timer(stream, flush, 1, dev)
     host = args.calibrate_host
-    where = "pinned host memory, mapped for the device" if host else "device memory, cold L2"
+    where = ("host memory from ghex_b200.host_empty (cudaHostAlloc, mapped; torch pin_memory beside it)" if host
+             else "device memory, cold L2")
     out = {"calibration": f"ghexb_calibrate_rows, rows of n float64 spaced 139 elements apart, {where}; CUDA events, "
                           "mean of the timed launches", "rows": {}}
     shape = (96, 3000, 139)
     if host:
-        a = torch.zeros(shape, dtype=torch.float64, pin_memory=True)
-        b = torch.zeros(shape, dtype=torch.float64, pin_memory=True)
+        from ghex_b200 import host_empty
+        a = torch.from_numpy(host_empty(shape, np.float64, order="C"))
+        b = torch.from_numpy(host_empty(shape, np.float64, order="C"))
+        a.zero_()
+        b.zero_()
+        ta = torch.zeros(shape, dtype=torch.float64, pin_memory=True)
+        tb = torch.zeros(shape, dtype=torch.float64, pin_memory=True)
     else:
         a = torch.zeros(shape, dtype=torch.float64, device=dev)
         b = torch.zeros_like(a)
@@ -791,6 +803,12 @@ def calibrate(args):
         ms = timer(launch, 5 if host else 20, 2 if host else 3)
         out["rows"][f"n={n}"] = {"rows": rows, "us": ms * 1e3, "rows_per_ns": rows / (ms * 1e6),
                                  "useful_GB/s": 2 * rows * n * 8 / (ms * 1e-3) / 1e9}
+        if host:
+            def launch_t(n=n):
+                _capi.call("ghexb_calibrate_rows", C.c_void_p(ta.data_ptr() + 3 * 8), C.c_void_p(tb.data_ptr()), rows, n,
+                           shape[2], shape[2], 8, C.c_void_p(stream.cuda_stream))
+            ms = timer(launch_t, 3, 1)
+            out["rows"][f"n={n}"]["torch_pinned_rows_per_ns"] = rows / (ms * 1e6)
     if host:
         x = torch.ones(64 << 20 >> 3, dtype=torch.float64, pin_memory=True)
         y = torch.empty(64 << 20 >> 3, dtype=torch.float64, device=dev)
@@ -867,6 +885,8 @@ def main():
     ms_box = timer(lambda: plan.launch(plan.PER_BOX, s), max(5, k_small // 4), 3)
     e2e_copy, copy_bytes = e2e_ms(case, stream, max(3, min(args.steps, 20)), world, dev)
     e2e, h2d, d2h, e2e_ok = e2e_host_ms(case, max(10, min(args.steps, 200)), max(3, args.warmup), world, dev)
+    e2e_torch, _, _, e2e_torch_ok = e2e_host_ms(case, max(10, min(args.steps, 200)), max(3, args.warmup), world, dev,
+                                                alloc="torch")
 
     achieved = alg / (ms_batched * 1e-3) / 1e9
     n_logical = len({f[0] for f in case.fields})
@@ -892,8 +912,11 @@ def main():
                "the exchange, minus a flush after a flush: the exchange plus the write-back of what it dirtied"},
         "e2e": {"value": world * alg / (e2e * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e, "bitexact": e2e_ok,
-                "form": "fields in pinned host memory, co.exchange(...).wait() per step: the exchange kernel reads "
-                        "the source cells from host memory and writes the halo cells into it",
+                "form": "fields in page-locked host memory from ghex_b200.host_empty (cudaHostAlloc, mapped), "
+                        "co.exchange(...).wait() per step: the exchange kernel reads the source cells from host memory "
+                        "and writes the halo cells into it",
+                "torch_pinned": {"value": world * alg / (e2e_torch * 1e-3) / 1e9, "ms_per_step": e2e_torch,
+                                 "bitexact": e2e_torch_ok, "form": "the same, fields in torch pin_memory tensors"},
                 "full_copy": {"value": world * alg / (e2e_copy * 1e-3) / 1e9, "ms_per_step": e2e_copy,
                               "h2d_bytes_per_step": copy_bytes, "d2h_bytes_per_step": copy_bytes,
                               "form": "every field copied to the device, exchanged there and copied back"}},

@@ -18,7 +18,8 @@ The shared library is loaded on first use of the API (not by `python -m ghex_b20
 __version__ = "0.1.0"
 
 _CORE_NAMES = ("Architecture", "make_context", "make_communication_object", "make_exchange_plan",
-               "make_bulk_communication_object", "BulkCommunicationObject", "GenericBulkCommunicationObject")
+               "make_bulk_communication_object", "BulkCommunicationObject", "GenericBulkCommunicationObject",
+               "host_empty", "dram_floor")
 
 
 def __getattr__(name):

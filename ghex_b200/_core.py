@@ -576,6 +576,31 @@ class ExchangePlan:
         self._h = None
 
 
+class _HostBlock:
+    """Page-locked host memory from ghexb_host_alloc, freed with the last array that uses it."""
+
+    def __init__(self, nbytes: int):
+        p = C.c_void_p()
+        call("ghexb_host_alloc", max(1, int(nbytes)), C.byref(p))
+        self.ptr, self.nbytes = p.value, int(nbytes)
+
+    def __del__(self, _release=_capi.release):
+        _release("ghexb_host_free", getattr(self, "ptr", None))
+
+
+def host_empty(shape, dtype, order: str = "F"):
+    """A numpy array in page-locked host memory mapped for the device (cudaHostAlloc, mapped and
+    portable): a host field the exchange kernels read and write in place over the host
+    interconnect. The memory lives as long as the array (or any view of it)."""
+    import numpy as np
+    dt = np.dtype(dtype)
+    n = int(np.prod(shape)) if len(shape) else 1
+    block = _HostBlock(n * dt.itemsize)
+    buf = (C.c_char * max(1, n * dt.itemsize)).from_address(block.ptr)
+    buf._owner = block
+    return np.frombuffer(buf, dtype=dt, count=n).reshape(shape, order=order)
+
+
 def dram_floor(ctx: context, buffer_infos: Sequence[BufferInfo], sector_bytes: int = 32) -> dict:
     """The least DRAM traffic of one exchange of these fields from a cold cache, with
     `sector_bytes` as the DRAM access granularity: sectors holding halo sources are read, sectors

@@ -40,21 +40,28 @@ class _PlanPool:
     def __init__(self, ctx: context, bis: Sequence[BufferInfo], size: int):
         self.ctx, self.bis, self.size = ctx, list(bis), size
         self.plans: "OrderedDict[tuple, ExchangePlan]" = OrderedDict()
+        self.hits = self.rebinds = self.created = 0
 
     def get(self, tensors: Sequence[torch.Tensor], stream) -> ExchangePlan:
         key = tuple(t.data_ptr() for t in tensors)
         plan = self.plans.get(key)
         if plan is not None:
             self.plans.move_to_end(key)
+            self.hits += 1
             return plan
         if len(self.plans) < self.size:
             plan = ExchangePlan(self.ctx, self.bis)
+            self.created += 1
         else:
             _, plan = self.plans.popitem(last=False)
         if plan.bound_pointers() != key:
             plan.rebind(tensors, stream=stream, keep=False)
+            self.rebinds += 1
         self.plans[key] = plan
         return plan
+
+    def stats(self) -> dict:
+        return {"plans": len(self.plans), "hits": self.hits, "rebinds": self.rebinds, "created": self.created}
 
 
 class DifferentiableExchange:
@@ -79,6 +86,11 @@ class DifferentiableExchange:
 
     def __len__(self) -> int:
         return len(self._layout)
+
+    def pool_stats(self) -> dict:
+        """Plan-pool use of the forward exchanges and of the adjoints: lookups that found a plan
+        bound to the tensors (hits) and rebinds of a plan to new memory."""
+        return {"forward": self._fwd.stats(), "adjoint": self._bwd.stats()}
 
     def check(self, tensors: Sequence[torch.Tensor]) -> None:
         if len(tensors) != len(self._layout):

@@ -5,6 +5,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 
@@ -455,33 +456,106 @@ int ghexb_field_destroy(ghexb_field f)
 }
 
 // ---- host memory for fields --------------------------------------------------------------------
+namespace
+{
+// Ranges registered by ghexb_host_register under the pointer it was given: one range normally,
+// several when part of the requested range was page-locked already by other code.
+std::mutex g_host_mutex;
+std::map<void*, std::vector<void*>> g_host_runs;
+
+bool host_locked(const void* p)
+{
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess)
+    {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+} // namespace
+
 int ghexb_host_register(void* ptr, size_t bytes, int* owned)
 {
     return guarded([&] {
         require(ptr && bytes > 0 && owned, "null argument");
         cudaPointerAttributes a{};
         ghexb::check_cuda(cudaPointerGetAttributes(&a, ptr), "cudaPointerGetAttributes");
-        if (a.type == cudaMemoryTypeHost)
+        std::vector<void*> runs;
+        // the whole range at once, unless its first page is page-locked already (a pinned
+        // allocation, or a registration of other code)
+        const cudaError_t e = a.type == cudaMemoryTypeHost
+                                  ? cudaErrorHostMemoryAlreadyRegistered
+                                  : cudaHostRegister(ptr, bytes, cudaHostRegisterMapped | cudaHostRegisterPortable);
+        if (e == cudaSuccess)
+            runs.push_back(ptr);
+        else if (e == cudaErrorHostMemoryAlreadyRegistered)
         {
-            // page-locked already (a pinned allocation, or a registration of other code): every
-            // page must be, at its own address
-            *owned = 0;
-            ghexb::check_accessible(ptr, bytes);
-            return;
+            // part of the range is locked by other code: lock each maximal run of pages that is
+            // not, page by page
+            (void)cudaGetLastError();
+            const size_t page = 4096;
+            char* c = static_cast<char*>(ptr);
+            char* end = c + bytes;
+            try
+            {
+                while (c < end)
+                {
+                    char* next = std::min(end, reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(c) / page + 1) * page));
+                    if (host_locked(c))
+                    {
+                        c = next;
+                        continue;
+                    }
+                    char* q = next;
+                    while (q < end && !host_locked(q))
+                        q = std::min(end, reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(q) / page + 1) * page));
+                    ghexb::check_cuda(cudaHostRegister(c, (size_t)(q - c), cudaHostRegisterMapped | cudaHostRegisterPortable),
+                        "cudaHostRegister");
+                    runs.push_back(c);
+                    c = q;
+                }
+            }
+            catch (...)
+            {
+                for (void* r : runs) (void)cudaHostUnregister(r);
+                throw;
+            }
         }
-        ghexb::check_cuda(cudaHostRegister(ptr, bytes, cudaHostRegisterMapped | cudaHostRegisterPortable),
-            "cudaHostRegister");
-        *owned = 1;
+        else
+            ghexb::check_cuda(e, "cudaHostRegister");
         try
         {
-            ghexb::check_accessible(ptr);
-            ghexb::check_accessible(static_cast<char*>(ptr) + bytes - 1);
+            ghexb::check_accessible(ptr, bytes);
         }
         catch (...)
         {
-            (void)cudaHostUnregister(ptr);
+            for (void* r : runs) (void)cudaHostUnregister(r);
             throw;
         }
+        *owned = runs.empty() ? 0 : 1;
+        if (!runs.empty())
+        {
+            std::lock_guard<std::mutex> lock(g_host_mutex);
+            g_host_runs[ptr] = std::move(runs);
+        }
+    });
+}
+
+int ghexb_host_alloc(size_t bytes, void** out)
+{
+    return guarded([&] {
+        require(out != nullptr && bytes > 0, "null argument or empty allocation");
+        *out = nullptr;
+        ghexb::check_cuda(cudaHostAlloc(out, bytes, cudaHostAllocMapped | cudaHostAllocPortable), "cudaHostAlloc");
+    });
+}
+
+int ghexb_host_free(void* ptr)
+{
+    return guarded([&] {
+        require(ptr != nullptr, "null argument");
+        ghexb::check_cuda(cudaFreeHost(ptr), "cudaFreeHost");
     });
 }
 
@@ -489,7 +563,17 @@ int ghexb_host_unregister(void* ptr)
 {
     return guarded([&] {
         require(ptr != nullptr, "null argument");
-        ghexb::check_cuda(cudaHostUnregister(ptr), "cudaHostUnregister");
+        std::vector<void*> runs{ptr};
+        {
+            std::lock_guard<std::mutex> lock(g_host_mutex);
+            auto it = g_host_runs.find(ptr);
+            if (it != g_host_runs.end())
+            {
+                runs = it->second;
+                g_host_runs.erase(it);
+            }
+        }
+        for (void* r : runs) ghexb::check_cuda(cudaHostUnregister(r), "cudaHostUnregister");
     });
 }
 

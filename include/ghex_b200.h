@@ -192,11 +192,17 @@ int ghexb_field_destroy(ghexb_field f);
  * (cudaHostAlloc) as it is, ordinary pageable memory after ghexb_host_register, which page-locks
  * [ptr, ptr + bytes) and maps it for the device (cudaHostRegister, mapped and portable). The
  * exchange kernels then read and write such fields in place over the host interconnect. *owned is
- * 1 when the call registered the range (undo with ghexb_host_unregister(ptr)) and 0 when the range
- * was page-locked already (every page is then checked). Fails with GHEXB_ERR_INVALID when the
+ * 1 when the call registered pages of the range (undo with ghexb_host_unregister(ptr)) and 0 when
+ * the whole range was page-locked already; pages locked by other code inside the range are left
+ * to it, the others registered, and every page is checked. Fails with GHEXB_ERR_INVALID when the
  * device cannot address the memory at its host address. Plans check every page of a host field
  * and refuse memory that the device cannot address, before any launch. */
 int ghexb_host_register(void* ptr, size_t bytes, int* owned);
+/* Page-locked host memory mapped for every device (cudaHostAlloc, mapped and portable), for fields
+ * that live in host memory: the device reads and writes it over the host interconnect at its host
+ * address. Free with ghexb_host_free. */
+int ghexb_host_alloc(size_t bytes, void** out);
+int ghexb_host_free(void* ptr);
 int ghexb_host_unregister(void* ptr);
 
 /* ---- communication object: replaces make_communication_object<Pattern>(ctx)

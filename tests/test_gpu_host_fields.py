@@ -159,3 +159,32 @@ def test_device_array_with_cpu_arch_refused(cuda):
     with pytest.raises(TypeError, match="host array"):
         R.make_field_descriptor(dm, run.dev[specs[0].name][0], w.offsets(specs[0]), w.extents(d, specs[0]),
                                 arch=Architecture.CPU)
+
+
+def test_library_host_memory_fields(cuda):
+    """Fields in page-locked host memory from ghex_b200.host_empty (cudaHostAlloc, mapped): the
+    exchange runs on them in place, bit-exact, and the memory is released with the arrays."""
+    from ghex_b200 import host_empty
+    w = W.config1(shape=(40, 30, 12))
+    run = RegularRun(w, cuda)
+    expected = run.oracle()
+    host = {}
+    for name, arrays in run.host.items():
+        hs = []
+        for a in arrays:
+            h = host_empty(a.shape, a.dtype, order="F")
+            h[...] = a
+            hs.append(h)
+        host[name] = hs
+    bis = []
+    for halos, specs in w.halo_groups().items():
+        pat = run.patterns[halos]
+        for spec in specs:
+            for dm, d, h in zip(pat.domains, w.domains, host[spec.name]):
+                bis.append(pat(R.make_field_descriptor(dm, h, w.offsets(spec), w.extents(d, spec),
+                                                       arch=Architecture.CPU)))
+    co = R.make_communication_object(run.ctx)
+    for _ in range(2):
+        co.exchange(bis).wait()
+        for name, hs in host.items():
+            assert sum(bits_equal(h, e) for h, e in zip(hs, expected[name])) == 0
