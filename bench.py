@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--calibrate", action="store_true",
                     help="time a plain row-copy kernel on the exchange's access pattern (rows of n elements at a row "
                          "stride) and contiguous copies, cold L2, and print one JSON line")
+    ap.add_argument("--staged-ab", action="store_true",
+                    help="time the staged (tensor-map) form against the element kernel on cfg1, cfg3 and cfg4")
     ap.add_argument("--calibrate-host", action="store_true",
                     help="the same row pattern in pinned host memory (the e2e form's access over the host "
                          "interconnect) and host<->device copies")
@@ -139,6 +141,14 @@ def roofline_block(alg: float, ms: float, peak: float, peak_kind: str, plan, cfg
     out["floor"] = {"sector_bytes": 32, "bytes": fl["total"], "read": fl["read"], "write": fl["write"],
                     "alg_over_floor": alg / fl["total"],
                     "frac_on_floor": fl["total"] / (ms * 1e-3) / 1e9 / peak}
+    # B200 fetches 128-byte lines from DRAM for these scattered reads whatever the L2 fetch
+    # granularity limit says (ncu dram__bytes_read matches a 128-byte line model), and writes
+    # back 32-byte sectors: the floor the hardware imposes
+    fl128 = plan.dram_floor(128)
+    hw = fl128["read"] + fl["write"]
+    out["floor_hw"] = {"read_line_bytes": 128, "write_sector_bytes": 32, "bytes": hw, "read": fl128["read"],
+                       "write": fl["write"], "alg_over_floor": alg / hw,
+                       "frac_on_floor": hw / (ms * 1e-3) / 1e9 / peak}
     key = tuning_key(info)
     tr = ncu_traffic(cfg, key)
     out["traffic"] = tr["dram_bytes"] if tr else None
@@ -797,18 +807,21 @@ def calibrate(args):
         b = torch.zeros_like(a)
     rows = shape[0] * shape[1]
     for n in ((1, 3, 6, 12) if host else (1, 3, 8, 32, 128)):
-        def launch(n=n):
-            _capi.call("ghexb_calibrate_rows", C.c_void_p(a.data_ptr() + 3 * 8), C.c_void_p(b.data_ptr()), rows, n,
-                       shape[2], shape[2], 8, C.c_void_p(stream.cuda_stream))
+        def launch(n=n, mode=0, x=a, y=b):
+            _capi.call("ghexb_calibrate_rows", C.c_void_p(x.data_ptr() + 3 * 8), C.c_void_p(y.data_ptr()), rows, n,
+                       shape[2], shape[2], 8, mode, C.c_void_p(stream.cuda_stream))
         ms = timer(launch, 5 if host else 20, 2 if host else 3)
-        out["rows"][f"n={n}"] = {"rows": rows, "us": ms * 1e3, "rows_per_ns": rows / (ms * 1e6),
-                                 "useful_GB/s": 2 * rows * n * 8 / (ms * 1e-3) / 1e9}
+        r = out["rows"][f"n={n}"] = {"rows": rows, "us": ms * 1e3, "rows_per_ns": rows / (ms * 1e6),
+                                     "useful_GB/s": 2 * rows * n * 8 / (ms * 1e-3) / 1e9}
         if host:
-            def launch_t(n=n):
-                _capi.call("ghexb_calibrate_rows", C.c_void_p(ta.data_ptr() + 3 * 8), C.c_void_p(tb.data_ptr()), rows, n,
-                           shape[2], shape[2], 8, C.c_void_p(stream.cuda_stream))
-            ms = timer(launch_t, 3, 1)
-            out["rows"][f"n={n}"]["torch_pinned_rows_per_ns"] = rows / (ms * 1e6)
+            ms = timer(lambda: launch(n, 0, ta, tb), 3, 1)
+            r["torch_pinned_rows_per_ns"] = rows / (ms * 1e6)
+        else:
+            # the halves of a copy, and the copy with the write-back of its rows inside the timing
+            r["read_only_rows_per_ns"] = rows / (timer(lambda: launch(n, 1), 20, 3) * 1e6)
+            r["write_only_rows_per_ns"] = rows / (timer(lambda: launch(n, 2), 20, 3) * 1e6)
+            r["write_only_with_writeback_rows_per_ns"] = rows / (timer(lambda: launch(n, 2), 20, 3, mode="writeback") * 1e6)
+            r["copy_with_writeback_rows_per_ns"] = rows / (timer(launch, 20, 3, mode="writeback") * 1e6)
     if host:
         x = torch.ones(64 << 20 >> 3, dtype=torch.float64, pin_memory=True)
         y = torch.empty(64 << 20 >> 3, dtype=torch.float64, device=dev)
@@ -825,6 +838,37 @@ def calibrate(args):
     print(json.dumps(out), flush=True)
 
 
+def staged_ab(args):
+    """The staged form (tensor-map loads into shared memory) against the element kernel, per
+    workload: cold-L2 time of the batched graph at the element kernel's autotuned shape, then with
+    the staged kernel beside it in modes 1 and 2 at several pipeline shapes. One JSON line."""
+    import torch
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    l2 = torch.cuda.get_device_properties(dev).L2_cache_size
+    flush = torch.ones(max(2 * l2, 64 << 20) // 4, dtype=torch.float32, device=dev)
+    timer = Timer(stream, flush, 1, dev)
+    s = stream.cuda_stream
+    out = {"staged_ab": "cold-L2 CUDA-event time of the batched graph, mean of 40 launches", "configs": {}}
+    for cfg in ("cfg1", "cfg3", "cfg4"):
+        case = Case(cfg, dev, 0)
+        plan = case.plan
+        plan.autotune(repeats=20, stream=s)
+        plan.set_staged(0)
+        rows = []
+        for mode, shape in ((0, (8, 16384, 4, 1)), (1, (8, 16384, 4, 1)), (1, (4, 16384, 4, 2)), (2, (8, 16384, 4, 1)),
+                            (2, (6, 16384, 8, 1)), (2, (4, 16384, 4, 2))):
+            plan.set_staged(mode, *shape)
+            ms = timer(lambda: plan.graph_launch(s), 40, 5)
+            info = plan.info()
+            rows.append({"tuning": tuning_key(info), "us": ms * 1e3, "staged_boxes": info["staged_boxes"],
+                         "staged_items": info["staged_items"], "element_tiles": info["num_tiles"],
+                         "status": plan.staged_status()})
+        out["configs"][cfg] = rows
+        del case, plan
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -832,6 +876,9 @@ def main():
         return
     if args.calibrate or args.calibrate_host:
         calibrate(args)
+        return
+    if args.staged_ab:
+        staged_ab(args)
         return
     import torch
     import torch.distributed as dist

@@ -119,8 +119,9 @@ SIGNATURES = {
     "ghexb_plan_get_info": [_vp, C.POINTER(PlanInfo)],
     "ghexb_plan_set_staged": [_vp, _i, _i, _i, _i, _i],
     "ghexb_host_alloc": [C.c_size_t, C.POINTER(_vp)],
+    "ghexb_host_is_mapped": [_vp, C.c_size_t, _pi],
     "ghexb_host_free": [_vp],
-    "ghexb_calibrate_rows": [_vp, _vp, C.c_int64, _i, C.c_int64, C.c_int64, _i, _vp],
+    "ghexb_calibrate_rows": [_vp, _vp, C.c_int64, _i, C.c_int64, C.c_int64, _i, _i, _vp],
     "ghexb_plan_staged_status": [_vp, C.POINTER(C.c_uint)],
     "ghexb_plan_dram_floor": [_vp, C.POINTER(_vp), _i, _i, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
     "ghexb_plan_set_tuning": [_vp, _i, _i, _i],

@@ -174,6 +174,13 @@ class _HostRegistration:
                 return
             lo += min(0, (n - 1) * st)
             hi += max(0, (n - 1) * st)
+        # memory that is page-locked and mapped already (pinned allocations: torch pin_memory,
+        # ghex_b200.host_empty, cudaHostAlloc) needs no registration of ours
+        mapped = C.c_int()
+        call("ghexb_host_is_mapped", C.c_void_p(lo), hi + info["itemsize"] - lo, C.byref(mapped))
+        if mapped.value:
+            self.held = []
+            return
         self.held = _host_pages.acquire(lo, hi + info["itemsize"])
 
     def __del__(self, _pages=_host_pages):

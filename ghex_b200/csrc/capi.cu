@@ -542,6 +542,24 @@ int ghexb_host_register(void* ptr, size_t bytes, int* owned)
     });
 }
 
+int ghexb_host_is_mapped(const void* ptr, size_t bytes, int* mapped)
+{
+    return guarded([&] {
+        require(ptr && bytes > 0 && mapped, "null argument");
+        *mapped = 0;
+        try
+        {
+            ghexb::check_accessible(ptr, bytes);
+        }
+        catch (const ghexb::error&)
+        {
+            (void)cudaGetLastError();
+            return;
+        }
+        *mapped = 1;
+    });
+}
+
 int ghexb_host_alloc(size_t bytes, void** out)
 {
     return guarded([&] {
@@ -851,17 +869,18 @@ int ghexb_plan_autotune(ghexb_plan plan, void* stream, int repeats, ghexb_plan_i
 }
 
 int ghexb_calibrate_rows(const void* src, void* dst, int64_t rows, int n, int64_t src_stride, int64_t dst_stride,
-    int elem_bytes, void* stream)
+    int elem_bytes, int mode, void* stream)
 {
     return guarded([&] {
         require(src && dst, "null argument");
+        require(mode >= 0 && mode <= 2, "mode 0 (copy), 1 (read only) or 2 (write only)");
         require(rows >= 1 && rows < (int64_t(1) << 32) && n >= 1 && n <= 256, "rows or row length out of range");
         require(elem_bytes == 4 || elem_bytes == 8, "elements of 4 or 8 bytes");
         require(src_stride >= n && dst_stride >= n, "row strides shorter than the rows");
         ghexb::check_accessible(src, (size_t)((rows - 1) * src_stride + n) * elem_bytes);
         ghexb::check_accessible(dst, (size_t)((rows - 1) * dst_stride + n) * elem_bytes);
         ghexb::check_cuda(ghexb::launch_row_copy(src, dst, (uint32_t)rows, (uint32_t)n, src_stride, dst_stride, elem_bytes,
-                              static_cast<cudaStream_t>(stream)),
+                              mode, static_cast<cudaStream_t>(stream)),
             "row copy launch");
     });
 }

@@ -228,7 +228,9 @@ __global__ void __launch_bounds__(256) l2_flush_kernel(const uint4* __restrict__
 // Calibration copy of short rows: dst[r*dst_stride + i] = src[r*src_stride + i] for r < rows, i < n;
 // consecutive threads take consecutive elements, each thread 8 elements (all loads before any
 // store), as the exchange kernel moves the rows of a box, without its tile records.
-template<typename T>
+// MODE 0 copies, 1 only reads (a value reaches dst only in the impossible case that the rows sum
+// to a sentinel), 2 only writes (each element its own index).
+template<typename T, int MODE>
 __global__ void __launch_bounds__(256) row_copy_kernel(const T* __restrict__ src, T* __restrict__ dst, uint32_t rows,
     uint32_t n, int64_t src_stride, int64_t dst_stride)
 {
@@ -241,35 +243,54 @@ __global__ void __launch_bounds__(256) row_copy_kernel(const T* __restrict__ src
     {
         const uint64_t e = ((uint64_t)blockIdx.x * K + k) * blockDim.x + threadIdx.x;
         o[k] = -1;
+        v[k] = (T)e;
         if (e < total)
         {
             const uint64_t r = e / n, i = e - r * n;
-            v[k] = __ldcg(src + r * src_stride + i);
+            if (MODE != 2) v[k] = __ldcg(src + r * src_stride + i);
             o[k] = (int64_t)(r * dst_stride + i);
         }
+    }
+    if (MODE == 1)
+    {
+        T acc = 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc ^= o[k] >= 0 ? v[k] : T(0);
+        if (acc == (T)0x5bd1e995u && o[0] >= 0) dst[o[0]] = acc;
+        return;
     }
 #pragma unroll
     for (int k = 0; k < K; ++k)
         if (o[k] >= 0) __stcg(dst + o[k], v[k]);
 }
 
+template<typename T>
+cudaError_t row_copy(const void* src, void* dst, uint32_t rows, uint32_t n, int64_t ss, int64_t ds, int mode,
+    unsigned grid, cudaStream_t stream)
+{
+    const T* s = static_cast<const T*>(src);
+    T* d = static_cast<T*>(dst);
+    switch (mode)
+    {
+        case 0: row_copy_kernel<T, 0><<<grid, 256, 0, stream>>>(s, d, rows, n, ss, ds); break;
+        case 1: row_copy_kernel<T, 1><<<grid, 256, 0, stream>>>(s, d, rows, n, ss, ds); break;
+        case 2: row_copy_kernel<T, 2><<<grid, 256, 0, stream>>>(s, d, rows, n, ss, ds); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 } // namespace
 
 cudaError_t launch_row_copy(const void* src, void* dst, uint32_t rows, uint32_t n, int64_t src_stride,
-    int64_t dst_stride, int es, cudaStream_t stream)
+    int64_t dst_stride, int es, int mode, cudaStream_t stream)
 {
     const uint64_t total = (uint64_t)rows * n;
     if (total == 0) return cudaSuccess;
     const unsigned grid = (unsigned)((total + 8 * 256 - 1) / (8 * 256));
-    if (es == 8)
-        row_copy_kernel<<<grid, 256, 0, stream>>>(static_cast<const unsigned long long*>(src),
-            static_cast<unsigned long long*>(dst), rows, n, src_stride, dst_stride);
-    else if (es == 4)
-        row_copy_kernel<<<grid, 256, 0, stream>>>(static_cast<const unsigned*>(src), static_cast<unsigned*>(dst), rows, n,
-            src_stride, dst_stride);
-    else
-        return cudaErrorInvalidValue;
-    return cudaGetLastError();
+    if (es == 8) return row_copy<unsigned long long>(src, dst, rows, n, src_stride, dst_stride, mode, grid, stream);
+    if (es == 4) return row_copy<unsigned>(src, dst, rows, n, src_stride, dst_stride, mode, grid, stream);
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_l2_flush(const uint4* buf, size_t n16, unsigned* sink, int grid, cudaStream_t stream)

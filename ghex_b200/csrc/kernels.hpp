@@ -21,7 +21,8 @@ cudaError_t launch_list_adjoint(const list_desc* lists, const tile* tiles, int n
 // produces, which keeps the loads alive.
 cudaError_t launch_l2_flush(const uint4* buf, size_t n16, unsigned* sink, int grid, cudaStream_t stream);
 
-// Calibration copy of `rows` rows of n elements of es (4 or 8) bytes at the given element strides.
+// Calibration copy of `rows` rows of n elements of es (4 or 8) bytes at the given element strides;
+// mode 0 copies, 1 only reads the source rows, 2 only writes the destination rows.
 cudaError_t launch_row_copy(const void* src, void* dst, uint32_t rows, uint32_t n, int64_t src_stride,
-    int64_t dst_stride, int es, cudaStream_t stream);
+    int64_t dst_stride, int es, int mode, cudaStream_t stream);
 } // namespace ghexb

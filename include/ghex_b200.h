@@ -198,6 +198,10 @@ int ghexb_field_destroy(ghexb_field f);
  * device cannot address the memory at its host address. Plans check every page of a host field
  * and refuse memory that the device cannot address, before any launch. */
 int ghexb_host_register(void* ptr, size_t bytes, int* owned);
+/* *mapped = 1 when every byte of [ptr, ptr + bytes) is device memory, or host memory page-locked
+ * and mapped for the device at its own address (pinned allocations, earlier registrations):
+ * such a field needs no ghexb_host_register. */
+int ghexb_host_is_mapped(const void* ptr, size_t bytes, int* mapped);
 /* Page-locked host memory mapped for every device (cudaHostAlloc, mapped and portable), for fields
  * that live in host memory: the device reads and writes it over the host interconnect at its host
  * address. Free with ghexb_host_free. */
@@ -304,9 +308,10 @@ int ghexb_exchange_noalloc(ghexb_context ctx, const ghexb_field* fields, int n, 
  * given element strides, dst[r*dst_stride + i] = src[r*src_stride + i], with the lane mapping of
  * the exchange kernel's box tiles (consecutive threads take consecutive elements, 8 loads in flight
  * per thread) but no work records: the rate at which a plain kernel moves such rows, from device
- * or from mapped host memory, against which the exchange of the same rows is compared. */
+ * or from mapped host memory, against which the exchange of the same rows is compared. mode 0
+ * copies, 1 only reads the source rows, 2 only writes the destination rows. */
 int ghexb_calibrate_rows(const void* src, void* dst, int64_t rows, int n, int64_t src_stride, int64_t dst_stride,
-    int elem_bytes, void* stream);
+    int elem_bytes, int mode, void* stream);
 
 /* ---- the compute step of the differentiable-exchange program. No counterpart in GHEX, which
  * has no stencil: this is the 7-point update x <- x + alpha * L(x) on the interior of each of n
