@@ -189,10 +189,22 @@ __device__ __forceinline__ void pair_elements(const xtile& t)
         if (ok[k]) st_global(dst + doff[k], v[k]);
 }
 
+// The index lists of the list tiles: the first CTAs bring them into L2 at the start of the launch,
+// 4 KB each (one 128-byte line per lane of their last warp), so that the CTAs of later waves find
+// their indices in L2 when their records arrive.
+__device__ __forceinline__ void prefetch_lists(const char* __restrict__ lists, uint32_t bytes)
+{
+    if (bytes == 0 || threadIdx.x < blockDim.x - 32) return;
+    const uint64_t off = (uint64_t)blockIdx.x * 4096 + (threadIdx.x - (blockDim.x - 32)) * 128;
+    if (off < bytes) asm volatile("prefetch.global.L2 [%0];" ::"l"(lists + off));
+}
+
 template<int K>
-__global__ void __launch_bounds__(k_max_block, K >= 16 ? 1 : 2) exchange_kernel(const xtile* __restrict__ tiles)
+__global__ void __launch_bounds__(k_max_block, K >= 16 ? 1 : 2) exchange_kernel(const xtile* __restrict__ tiles,
+    const char* __restrict__ lists, uint32_t list_bytes)
 {
     __shared__ xtile t;
+    prefetch_lists(lists, list_bytes);
     load_record<k_xtile_words>(t, tiles);
     switch (t.cls)
     {
@@ -354,16 +366,19 @@ __global__ void __launch_bounds__(k_gather_block, 3) list_gather_kernel(const gt
 
 } // namespace
 
-cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cudaStream_t stream)
+cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cudaStream_t stream, const void* lists,
+    size_t list_bytes)
 {
     if (ntiles <= 0) return cudaSuccess;
     if (block < 32 || block > k_max_block || block % 32) return cudaErrorInvalidValue;
     const int grid = ntiles;
+    const char* pl = static_cast<const char*>(lists);
+    const uint32_t pb = lists ? (uint32_t)std::min<size_t>(list_bytes, 0xffffffffu) : 0u;
     switch (k)
     {
-        case 4: exchange_kernel<4><<<grid, block, 0, stream>>>(tiles); break;
-        case 8: exchange_kernel<8><<<grid, block, 0, stream>>>(tiles); break;
-        case 16: exchange_kernel<16><<<grid, block, 0, stream>>>(tiles); break;
+        case 4: exchange_kernel<4><<<grid, block, 0, stream>>>(tiles, pl, pb); break;
+        case 8: exchange_kernel<8><<<grid, block, 0, stream>>>(tiles, pl, pb); break;
+        case 16: exchange_kernel<16><<<grid, block, 0, stream>>>(tiles, pl, pb); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

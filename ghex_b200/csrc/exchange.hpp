@@ -66,7 +66,10 @@ constexpr int k_gather_classes = 4 * k_max_images;
 
 // Forward exchange of tiles[0, ntiles), one CTA per tile: a tile holds at most
 // forward_per_thread(k, unit) * block elements; k is 4, 8 or 16.
-cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cudaStream_t stream);
+// `lists` (list_bytes long): the index lists the list tiles read, brought into L2 by the first
+// CTAs of the launch; nullptr when there are none.
+cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cudaStream_t stream,
+    const void* lists = nullptr, size_t list_bytes = 0);
 // Adjoint in gather form of tiles[0, ntiles), one CTA per tile: a tile holds at most
 // gather_per_thread(nimg) * k_gather_block elements. launch_gather takes box cells,
 // launch_list_gather unstructured owner groups with `cols`, their column table.

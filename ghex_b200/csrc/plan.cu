@@ -1635,7 +1635,9 @@ void launch_plan(ghexb_plan_s& plan, int form, cudaStream_t stream)
 {
     auto run = [&](const xtile* base, std::pair<int, int> r) {
         if (r.second <= 0) return;
-        check_cuda(launch_exchange(base + r.first, r.second, plan.per_thread, plan.block, stream), "exchange kernel launch");
+        check_cuda(launch_exchange(base + r.first, r.second, plan.per_thread, plan.block, stream, plan.d_idx,
+                       plan.idx.size() * sizeof(int32_t)),
+            "exchange kernel launch");
     };
     switch (form)
     {
@@ -1858,15 +1860,6 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         const int fgrid = (plan.ctx ? plan.ctx->num_sms : 148) * 8;
         for (size_t ci = 0; ci < cands.size(); ++ci)
         {
-            if (ci == n_element && stageable)
-            {
-                // the staged form beside the best element-kernel shape
-                const cand e = bestc;
-                for (int mode : {1, 2})
-                    for (const auto& sh : std::vector<std::array<int, 4>>{{8, 16384, 4, 1}, {6, 16384, 8, 1}, {4, 16384, 4, 2},
-                             {12, 8192, 4, 1}})
-                        cands.push_back({e.k, e.block, e.pairs, mode, sh[0], sh[1], sh[2], sh[3]});
-            }
             const cand& c = cands[ci];
             apply(c);
             if (c.mode > 0 && plan.sitems.empty()) continue; // nothing to stage
@@ -1901,6 +1894,15 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
                 }
             }
             if (total < best) best = total, bestc = c;
+            if (ci + 1 == n_element && stageable)
+            {
+                // the staged form beside the best element-kernel shape
+                const cand e = bestc;
+                for (int mode : {1, 2})
+                    for (const auto& sh : std::vector<std::array<int, 4>>{{8, 16384, 4, 1}, {6, 16384, 8, 1}, {4, 16384, 4, 2},
+                             {12, 8192, 4, 1}})
+                        cands.push_back({e.k, e.block, e.pairs, mode, sh[0], sh[1], sh[2], sh[3]});
+            }
         }
     }
     catch (...)
