@@ -74,8 +74,10 @@ def parse():
     ap.add_argument("--profile", choices=["batched", "per_field", "adjoint"], default=None,
                     help="only run `--steps` launches of one form after `--warmup` (for ncu captures)")
     ap.add_argument("--tuning", default=None,
-                    help="with --profile: the tuning to launch at, as printed in the bench line's "
-                         "roofline.traffic_tuning (e.g. k8.b128.p0.s1.st8x16384.c4.g1); default: the autotuner's")
+                    help="the tuning of the headline workload's plan, as printed in the bench line's "
+                         "roofline.traffic_tuning (e.g. k8.b128.p0.s1.st8x16384.c4.g1), instead of the autotuner's "
+                         "choice (for --profile runs and ncu launch lists, whose serialised timing would mislead the "
+                         "autotuner)")
     return ap.parse_args()
 
 
@@ -914,7 +916,11 @@ def main():
     timer = Timer(stream, flush, world, dev)
     peak, peak_kind = peaks()
     s = stream.cuda_stream
-    tuning = plan.info() if args.no_autotune else plan.autotune(repeats=20, stream=s)
+    if args.tuning:
+        apply_tuning(plan, args.tuning)
+        tuning = plan.info()
+    else:
+        tuning = plan.info() if args.no_autotune else plan.autotune(repeats=20, stream=s)
 
     sampler = ClockSampler(dev.index)
     with sampler:

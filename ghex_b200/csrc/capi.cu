@@ -717,6 +717,7 @@ int ghexb_plan_check(ghexb_context ctx, const ghexb_field* fields, int n, int64_
             }
         plan.staged_mode = 0;
         *elements_checked = ghexb::check_tables(plan);
+        ghexb::check_relocation(plan);
     });
 }
 

@@ -119,8 +119,10 @@ __device__ __forceinline__ void box_elements(const xtile& t)
         }
 }
 
+// blk: the tile's index block in shared memory (the indices of columns t.u0, t.u0 + 1, ...), or
+// nullptr when the tile reads its indices from the lists
 template<int K, typename T>
-__device__ __forceinline__ void list_elements(const xtile& t)
+__device__ __forceinline__ void list_elements(const xtile& t, const int32_t* blk)
 {
     const T* __restrict__ src = reinterpret_cast<const T*>(t.src);
     T* __restrict__ dst = reinterpret_cast<T*>(t.dst);
@@ -136,8 +138,17 @@ __device__ __forceinline__ void list_elements(const xtile& t)
             const uint32_t g = t.e0 + e;
             const uint32_t col = fdiv(g, t.m0, t.l0);
             const int32_t lev = (int32_t)(g - col * t.n0);
-            so[k] = __ldg(t.sidx + col) * t.s0 + lev * t.s1;
-            doff[k] = __ldg(t.didx + col) * t.d0 + lev * t.d1;
+            if (blk)
+            {
+                const uint32_t c = col - (uint32_t)t.u0;
+                so[k] = blk[c] * t.s0 + lev * t.s1;
+                doff[k] = blk[k_block_columns + c] * t.d0 + lev * t.d1;
+            }
+            else
+            {
+                so[k] = __ldg(t.sidx + col) * t.s0 + lev * t.s1;
+                doff[k] = __ldg(t.didx + col) * t.d0 + lev * t.d1;
+            }
         }
     }
     T v[K];
@@ -201,11 +212,17 @@ __device__ __forceinline__ void prefetch_lists(const char* __restrict__ lists, u
 
 template<int K>
 __global__ void __launch_bounds__(k_max_block, K >= 16 ? 1 : 2) exchange_kernel(const xtile* __restrict__ tiles,
-    const char* __restrict__ lists, uint32_t list_bytes)
+    const char* __restrict__ lists, uint32_t list_bytes, const int32_t* __restrict__ blocks)
 {
     __shared__ xtile t;
+    __shared__ __align__(16) int32_t blk_s[k_block_ints];
     prefetch_lists(lists, list_bytes);
+    // the tile's index block, in the same round trip as its record (threads 7..22: 16 words)
+    if (blocks && threadIdx.x >= k_xtile_words && threadIdx.x < k_xtile_words + k_block_ints / 4)
+        reinterpret_cast<int4*>(blk_s)[threadIdx.x - k_xtile_words] =
+            __ldg(reinterpret_cast<const int4*>(blocks + (size_t)blockIdx.x * k_block_ints) + (threadIdx.x - k_xtile_words));
     load_record<k_xtile_words>(t, tiles);
+    const int32_t* blk = blocks && t.pad[0] ? blk_s : nullptr;
     switch (t.cls)
     {
 #define GHEXB_CASE(C, F)                                                                                               \
@@ -216,11 +233,11 @@ __global__ void __launch_bounds__(k_max_block, K >= 16 ? 1 : 2) exchange_kernel(
         GHEXB_CASE(k_box4_neg, (box_elements<K, uint32_t, true>))
         GHEXB_CASE(k_box2, (box_elements<K, uint16_t, false>))
         GHEXB_CASE(k_box1, (box_elements<K, uint8_t, false>))
-        GHEXB_CASE(k_list16, (list_elements<forward_per_thread(K, 16), uint4>))
-        GHEXB_CASE(k_list8, (list_elements<K, unsigned long long>))
-        GHEXB_CASE(k_list4, (list_elements<K, uint32_t>))
-        GHEXB_CASE(k_list2, (list_elements<K, uint16_t>))
-        GHEXB_CASE(k_list1, (list_elements<K, uint8_t>))
+        case k_list16: list_elements<forward_per_thread(K, 16), uint4>(t, blk); break;
+        case k_list8: list_elements<K, unsigned long long>(t, blk); break;
+        case k_list4: list_elements<K, uint32_t>(t, blk); break;
+        case k_list2: list_elements<K, uint16_t>(t, blk); break;
+        case k_list1: list_elements<K, uint8_t>(t, blk); break;
         GHEXB_CASE(k_pair8, (pair_elements<K, unsigned long long>))
         GHEXB_CASE(k_pair4, (pair_elements<K, uint32_t>))
 #undef GHEXB_CASE
@@ -367,7 +384,7 @@ __global__ void __launch_bounds__(k_gather_block, 3) list_gather_kernel(const gt
 } // namespace
 
 cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cudaStream_t stream, const void* lists,
-    size_t list_bytes)
+    size_t list_bytes, const int32_t* blocks)
 {
     if (ntiles <= 0) return cudaSuccess;
     if (block < 32 || block > k_max_block || block % 32) return cudaErrorInvalidValue;
@@ -376,9 +393,9 @@ cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cu
     const uint32_t pb = lists ? (uint32_t)std::min<size_t>(list_bytes, 0xffffffffu) : 0u;
     switch (k)
     {
-        case 4: exchange_kernel<4><<<grid, block, 0, stream>>>(tiles, pl, pb); break;
-        case 8: exchange_kernel<8><<<grid, block, 0, stream>>>(tiles, pl, pb); break;
-        case 16: exchange_kernel<16><<<grid, block, 0, stream>>>(tiles, pl, pb); break;
+        case 4: exchange_kernel<4><<<grid, block, 0, stream>>>(tiles, pl, pb, blocks); break;
+        case 8: exchange_kernel<8><<<grid, block, 0, stream>>>(tiles, pl, pb, blocks); break;
+        case 16: exchange_kernel<16><<<grid, block, 0, stream>>>(tiles, pl, pb, blocks); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -66,10 +66,17 @@ constexpr int k_gather_classes = 4 * k_max_images;
 
 // Forward exchange of tiles[0, ntiles), one CTA per tile: a tile holds at most
 // forward_per_thread(k, unit) * block elements; k is 4, 8 or 16.
+// Index block of a list tile: the source indices of its (at most k_block_columns) columns, then
+// their destination indices.
+constexpr int k_block_columns = 32;
+constexpr int k_block_ints = 2 * k_block_columns;
+
 // `lists` (list_bytes long): the index lists the list tiles read, brought into L2 by the first
-// CTAs of the launch; nullptr when there are none.
+// CTAs of the launch; nullptr when there are none. `blocks`: k_block_ints ints per tile, the
+// index blocks of the flagged list tiles (xtile pad[0] = 1), or nullptr (the tiles then read
+// their indices through sidx / didx).
 cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cudaStream_t stream,
-    const void* lists = nullptr, size_t list_bytes = 0);
+    const void* lists = nullptr, size_t list_bytes = 0, const int32_t* blocks = nullptr);
 // Adjoint in gather form of tiles[0, ntiles), one CTA per tile: a tile holds at most
 // gather_per_thread(nimg) * k_gather_block elements. launch_gather takes box cells,
 // launch_list_gather unstructured owner groups with `cols`, their column table.

@@ -1088,6 +1088,106 @@ void dram_floor(const ghexb_plan_s& plan, int sector, int64_t& read_bytes, int64
     write_bytes = written * sector;
 }
 
+namespace
+{
+// Moves the pointers of a plan's tile tables from the fields' old memory to their new memory:
+// every pointer that lies in an old field's span moves by that field's displacement. Every table
+// pointer that the kernels dereference addresses an element of a field (tile records, gather
+// cells, the column table) or the index lists, which do not move. Not applicable (ok == false)
+// when two old spans overlap.
+struct relocator
+{
+    struct span
+    {
+        uintptr_t lo, hi;
+        intptr_t delta;
+    };
+    std::vector<span> spans; // sorted by lo
+    bool ok = true;
+
+    relocator(const std::vector<ghexb_field_s>& fields, void* const* data)
+    {
+        for (size_t i = 0; i < fields.size(); ++i)
+        {
+            const uintptr_t lo = reinterpret_cast<uintptr_t>(fields[i].data);
+            spans.push_back({lo, lo + field_bytes(fields[i]), reinterpret_cast<intptr_t>(data[i]) - (intptr_t)lo});
+        }
+        std::sort(spans.begin(), spans.end(), [](const span& a, const span& b) { return a.lo < b.lo; });
+        for (size_t i = 1; i < spans.size(); ++i)
+            if (spans[i].lo < spans[i - 1].hi) ok = false;
+    }
+    template<typename P>
+    void operator()(P*& p) const
+    {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+        auto it = std::upper_bound(spans.begin(), spans.end(), a, [](uintptr_t v, const span& s) { return v < s.lo; });
+        if (it == spans.begin()) return;
+        --it;
+        if (a < it->hi) p = reinterpret_cast<P*>(a + it->delta);
+    }
+    void operator()(uint64_t& v) const
+    {
+        char* p = reinterpret_cast<char*>(v);
+        (*this)(p);
+        v = reinterpret_cast<uint64_t>(p);
+    }
+};
+
+void relocate_tiles(ghexb_plan_s& plan, const relocator& R)
+{
+    for (auto* tab : {&plan.xf, &plan.xp, &plan.xb, &plan.xpair})
+        for (auto& t : *tab)
+        {
+            R(t.src), R(t.dst);
+            if (t.src2) R(t.src2);
+        }
+    for (auto& g : plan.gt)
+    {
+        if (g.own) R(g.own);
+        for (int k = 0; k < k_max_images; ++k)
+            if (g.img[k].ptr) R(g.img[k].ptr);
+    }
+    for (auto& c : plan.lcols) R(c);
+}
+
+} // namespace
+
+void check_relocation(ghexb_plan_s& plan)
+{
+    // the tables built for the fields at a second address, against the current tables moved there
+    build_tiles(plan, plan.idx.data());
+    std::vector<void*> moved;
+    for (size_t i = 0; i < plan.fields.size(); ++i) moved.push_back(plan.fields[i].data + (int64_t)4096 * (int64_t)(i + 1) * 3);
+    const relocator R(plan.fields, moved.data());
+    if (!R.ok) return;
+    ghexb_plan_s copy;
+    copy.xf = plan.xf, copy.xp = plan.xp, copy.xb = plan.xb, copy.xpair = plan.xpair, copy.gt = plan.gt, copy.lcols = plan.lcols;
+    relocate_tiles(copy, R);
+    const auto old_data = plan.fields;
+    const auto old_boxes = plan.boxes;
+    const auto old_lists = plan.lists;
+    for (size_t i = 0; i < plan.fields.size(); ++i) plan.fields[i].data = static_cast<char*>(moved[i]);
+    for (size_t i = 0; i < plan.boxes.size(); ++i)
+    {
+        plan.boxes[i].src = plan.fields[plan.box_src_slot[i]].data + plan.box_src_off[i];
+        plan.boxes[i].dst = plan.fields[plan.box_dst_slot[i]].data + plan.box_dst_off[i];
+    }
+    for (size_t i = 0; i < plan.lists.size(); ++i)
+    {
+        plan.lists[i].src = plan.fields[plan.list_src_slot[i]].data + plan.list_src_off[i];
+        plan.lists[i].dst = plan.fields[plan.list_dst_slot[i]].data + plan.list_dst_off[i];
+    }
+    build_tiles(plan, plan.idx.data());
+    auto same = [](const auto& a, const auto& b) {
+        return a.size() == b.size() && (a.empty() || std::memcmp(a.data(), b.data(), a.size() * sizeof(a[0])) == 0);
+    };
+    const bool equal = same(copy.xf, plan.xf) && same(copy.xp, plan.xp) && same(copy.xb, plan.xb) &&
+                       same(copy.xpair, plan.xpair) && same(copy.gt, plan.gt) && same(copy.lcols, plan.lcols);
+    plan.fields = old_data, plan.boxes = old_boxes, plan.lists = old_lists;
+    build_tiles(plan, plan.idx.data());
+    if (!equal) throw error(GHEXB_ERR_INTERNAL, "moved tile tables differ from the tables built at the new address");
+}
+
 int64_t check_tables(ghexb_plan_s& plan)
 {
     build_tiles(plan, plan.idx.data());
@@ -1192,6 +1292,27 @@ int64_t check_tables(ghexb_plan_s& plan)
     for (const auto& r : plan.xp_field) np += check_tiles(plan.xp, r.first, r.second, class_of_x);
     for (const auto& r : plan.xb_box) nb += check_tiles(plan.xb, r.first, r.second, class_of_x);
     for (const auto& r : plan.xb_list) nb += check_tiles(plan.xb, r.first, r.second, class_of_x);
+    // index blocks: a flagged list tile finds every column's indices in its block, as the lists hold them
+    auto check_blocks = [&](const std::vector<xtile>& tiles, const std::vector<int32_t>& blocks) {
+        for (size_t p = 0; p < tiles.size(); ++p)
+        {
+            const xtile& t = tiles[p];
+            if (!t.pad[0]) continue;
+            if (t.kind != 1 || blocks.size() < (p + 1) * k_block_ints)
+                throw error(GHEXB_ERR_INTERNAL, "index block of a tile that has none");
+            for (uint32_t e = 0; e < t.count; ++e)
+            {
+                const uint32_t col = fast_div{t.n0, t.m0, t.l0}.div(t.e0 + e);
+                const uint32_t c = col - (uint32_t)t.u0;
+                if (c >= (uint32_t)k_block_columns || blocks[p * k_block_ints + c] != t.sidx[col] ||
+                    blocks[p * k_block_ints + k_block_columns + c] != t.didx[col])
+                    throw error(GHEXB_ERR_INTERNAL, "index block differs from the lists");
+            }
+        }
+    };
+    check_blocks(plan.xf, plan.xf_blk);
+    check_blocks(plan.xp, plan.xp_blk);
+    check_blocks(plan.xb, plan.xb_blk);
     const int64_t ns = check_staged(plan);
     checked += ns;
     if (nf + ns != nb || np != nb) throw error(GHEXB_ERR_INTERNAL, "batched, per-field and per-box tables differ");
@@ -1346,7 +1467,13 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
     ensure(plan.d_lcols, plan.cap_lcols, plan.lcols.size());
     ensure(plan.d_smaps, plan.cap_smaps, plan.smaps.size());
     ensure(plan.d_sitems, plan.cap_sitems, plan.sitems.size());
+    ensure(plan.d_xf_blk, plan.cap_xf_blk, plan.xf_blk.size());
+    ensure(plan.d_xp_blk, plan.cap_xp_blk, plan.xp_blk.size());
+    ensure(plan.d_xb_blk, plan.cap_xb_blk, plan.xb_blk.size());
     host_stager st(plan, stream);
+    st.put(plan.d_xf_blk, plan.xf_blk);
+    st.put(plan.d_xp_blk, plan.xp_blk);
+    st.put(plan.d_xb_blk, plan.xb_blk);
     st.put(plan.d_xf, plan.xf);
     st.put(plan.d_xp, plan.xp);
     st.put(plan.d_xb, plan.xb);
@@ -1362,6 +1489,32 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
     upload(plan.d_adj_btiles, plan.adj_btiles, st);
     upload(plan.d_adj_ltiles, plan.adj_ltiles, st);
     st.commit();
+}
+
+// Index blocks of a tile table: for every list tile whose columns number at most
+// k_block_columns, the source then destination indices of its columns (k_block_ints per tile, at
+// the tile's position), which the kernel loads beside the tile record; the tile is flagged
+// (pad[0] = 1). Empty when the plan has no lists.
+void build_index_blocks(ghexb_plan_s& plan, std::vector<xtile>& tiles, std::vector<int32_t>& blocks, const int32_t* idx)
+{
+    blocks.clear();
+    if (plan.lists.empty() || !idx) return;
+    blocks.assign(tiles.size() * k_block_ints, 0);
+    for (size_t p = 0; p < tiles.size(); ++p)
+    {
+        xtile& t = tiles[p];
+        t.pad[0] = 0;
+        if (t.kind != 1 || t.count == 0) continue;
+        const uint32_t first = t.e0 / t.n0, last = (t.e0 + t.count - 1) / t.n0;
+        if ((uint32_t)t.u0 != first || last - first + 1 > (uint32_t)k_block_columns) continue;
+        const int64_t so = t.sidx - idx, dof = t.didx - idx; // offsets of the lists in plan.idx
+        for (uint32_t c = first; c <= last; ++c)
+        {
+            blocks[p * k_block_ints + (c - first)] = plan.idx[so + c];
+            blocks[p * k_block_ints + k_block_columns + (c - first)] = plan.idx[dof + c];
+        }
+        t.pad[0] = 1;
+    }
 }
 
 void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
@@ -1402,7 +1555,11 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
     auto list_tiles = [&](int i, std::vector<xtile>& out) {
         const auto& l = plan.lists[i];
         const fast_div f0 = fast_div::make((uint32_t)l.levels);
-        const uint32_t n = (uint32_t)((int64_t)l.count * l.levels), c = row_cap((int)l.unit, l.levels);
+        const uint32_t n = (uint32_t)((int64_t)l.count * l.levels);
+        uint32_t c = row_cap((int)l.unit, l.levels);
+        // whole columns, at most k_block_columns of them, when a tile holds at least one: the
+        // tile's index block (below) then covers its columns
+        if ((uint32_t)l.levels <= c) c = std::min<uint32_t>(c / l.levels, k_block_columns) * (uint32_t)l.levels;
         for (uint32_t e0 = 0; e0 < n; e0 += c)
         {
             xtile t{};
@@ -1415,6 +1572,7 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
             t.n1 = 1, t.m1 = 1, t.l1 = 0;
             t.unit = (uint8_t)l.unit;
             t.kind = 1;
+            t.u0 = (int32_t)(e0 / (uint32_t)l.levels); // first column of the tile
             out.push_back(t);
         }
     };
@@ -1506,6 +1664,9 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
         plan.xf.clear();
         append_range(plan.xf, all);
     }
+    build_index_blocks(plan, plan.xf, plan.xf_blk, idx);
+    build_index_blocks(plan, plan.xp, plan.xp_blk, idx);
+    build_index_blocks(plan, plan.xb, plan.xb_blk, idx);
 
     // ---- box adjoint, gather form
     plan.gt.clear();
@@ -1633,26 +1794,26 @@ void release_graph(ghexb_plan_s& plan)
 
 void launch_plan(ghexb_plan_s& plan, int form, cudaStream_t stream)
 {
-    auto run = [&](const xtile* base, std::pair<int, int> r) {
+    auto run = [&](const xtile* base, const int32_t* blocks, std::pair<int, int> r) {
         if (r.second <= 0) return;
         check_cuda(launch_exchange(base + r.first, r.second, plan.per_thread, plan.block, stream, plan.d_idx,
-                       plan.idx.size() * sizeof(int32_t)),
+                       plan.idx.size() * sizeof(int32_t), blocks ? blocks + (size_t)r.first * k_block_ints : nullptr),
             "exchange kernel launch");
     };
     switch (form)
     {
         case GHEXB_FORM_BATCHED:
             launch_staged_plan(plan, stream);
-            run(plan.d_xf, {0, (int)plan.xf.size()});
+            run(plan.d_xf, plan.xf_blk.empty() ? nullptr : plan.d_xf_blk, {0, (int)plan.xf.size()});
             if (!plan.sitems.empty())
                 check_cuda(cudaStreamWaitEvent(stream, plan.join_event, 0), "cudaStreamWaitEvent(join)");
             break;
         case GHEXB_FORM_PER_FIELD:
-            for (const auto& r : plan.xp_field) run(plan.d_xp, r);
+            for (const auto& r : plan.xp_field) run(plan.d_xp, plan.xp_blk.empty() ? nullptr : plan.d_xp_blk, r);
             break;
         case GHEXB_FORM_PER_BOX:
-            for (const auto& r : plan.xb_box) run(plan.d_xb, r);
-            for (const auto& r : plan.xb_list) run(plan.d_xb, r);
+            for (const auto& r : plan.xb_box) run(plan.d_xb, plan.xb_blk.empty() ? nullptr : plan.d_xb_blk, r);
+            for (const auto& r : plan.xb_list) run(plan.d_xb, plan.xb_blk.empty() ? nullptr : plan.d_xb_blk, r);
             break;
         default: throw error(GHEXB_ERR_INVALID, "unknown exchange form " + std::to_string(form));
     }
@@ -1770,6 +1931,7 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
                                            reinterpret_cast<uintptr_t>(data[plan.list_dst_slot[i]]) % 16))
             throw error(GHEXB_ERR_INVALID, "rebind: 16-byte column alignment of the plan is not met by the new memory");
     for (int i = 0; i < n; ++i) check_accessible(data[i], (size_t)(field_span(plan.fields[i]) * plan.fields[i].esize));
+    const relocator R(plan.fields, data);
     for (int i = 0; i < n; ++i) plan.fields[i].data = static_cast<char*>(data[i]);
     for (size_t i = 0; i < plan.boxes.size(); ++i)
     {
@@ -1795,9 +1957,16 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
         return;
     }
     // stream-ordered rewrite of the tables. The tile tables keep their size and device address,
-    // so a captured graph stays valid.
-    build_tiles(plan, plan.d_idx);
+    // so a captured graph stays valid. Their pointers move with the fields (the same tables as a
+    // rebuild gives: ghexb_plan_check compares the two), else they are rebuilt.
+    if (R.ok)
+        relocate_tiles(plan, R);
+    else
+        build_tiles(plan, plan.d_idx);
     host_stager st(plan, stream);
+    st.put(plan.d_xf_blk, plan.xf_blk);
+    st.put(plan.d_xp_blk, plan.xp_blk);
+    st.put(plan.d_xb_blk, plan.xb_blk);
     st.put(plan.d_xf, plan.xf);
     st.put(plan.d_xp, plan.xp);
     st.put(plan.d_xb, plan.xb);
@@ -1928,7 +2097,7 @@ ghexb_plan_s::~ghexb_plan_s()
     }
     if (fork_event) cudaEventDestroy(fork_event);
     if (join_event) cudaEventDestroy(join_event);
-    for (void* p : {(void*)d_smaps, (void*)d_sitems, (void*)d_status})
+    for (void* p : {(void*)d_smaps, (void*)d_sitems, (void*)d_status, (void*)d_xf_blk, (void*)d_xp_blk, (void*)d_xb_blk})
         if (p) cudaFree(p);
     for (void* p : {(void*)d_boxes, (void*)d_lists, (void*)d_adj_lists, (void*)d_idx, (void*)d_xf, (void*)d_xp,
              (void*)d_xb, (void*)d_gt, (void*)d_lcols, (void*)d_adj_btiles, (void*)d_adj_ltiles, (void*)d_counters})

@@ -40,6 +40,12 @@ struct ghexb_plan_s
     // DRAM bytes per element first), xp the per-field form's (grouped by logical field) and xb
     // the per-box form's (grouped by descriptor).
     std::vector<ghexb::xtile> xf, xp, xb;
+    // Index blocks of the list tiles, one per tile of xf, xp and xb (exchange.hpp
+    // k_block_ints each): the indices of the tile's columns, loaded beside its record. Empty
+    // when the plan has no lists.
+    std::vector<int32_t> xf_blk, xp_blk, xb_blk;
+    int32_t *d_xf_blk = nullptr, *d_xp_blk = nullptr, *d_xb_blk = nullptr;
+    size_t cap_xf_blk = 0, cap_xp_blk = 0, cap_xb_blk = 0;
     // x-face boxes whose rows interleave (A's row r ends where B's row r + 1 begins): the
     // batched and per-field tables move each pair as one set of contiguous segments
     std::vector<std::pair<int, int>> pairs; // (A, B) box indices
@@ -172,6 +178,8 @@ void build_plan(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* fie
 // Replays on the host the address computation of every element the forward and adjoint kernels
 // touch and checks it against the memory span of its field; returns the number of elements.
 int64_t check_tables(ghexb_plan_s& plan);
+// Host-only: the tile tables moved to other field memory by a rebind equal the tables built there.
+void check_relocation(ghexb_plan_s& plan);
 // Host-only: forward tiles of the current tuning and the adjoint tiles, addressing the fields'
 // current data; list tiles point into `idx` (the device copy of plan.idx, or any copy of it).
 void build_tiles(ghexb_plan_s& plan, const int32_t* idx);
