@@ -1,5 +1,6 @@
 // extern "C" entry points of libghex_b200.so (declared in include/ghex_b200.h).
 #include <cuda_runtime.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <cstring>
@@ -494,7 +495,7 @@ int ghexb_host_register(void* ptr, size_t bytes, int* owned)
             // part of the range is locked by other code: lock each maximal run of pages that is
             // not, page by page
             (void)cudaGetLastError();
-            const size_t page = 4096;
+            const size_t page = (size_t)sysconf(_SC_PAGESIZE);
             char* c = static_cast<char*>(ptr);
             char* end = c + bytes;
             try
