@@ -69,7 +69,7 @@ class DifferentiableExchange:
     arrays. Calling it with tensors of the same layouts (shape, strides, dtype, device) as the
     fields the buffer_infos were made from exchanges those tensors in place."""
 
-    def __init__(self, ctx: context, buffer_infos: Sequence[BufferInfo], *, graph: bool = True, pool: int = 32):
+    def __init__(self, ctx: context, buffer_infos: Sequence[BufferInfo], *, graph: bool = True, pool: int = 8):
         self.context = ctx
         self._bis = _flatten(tuple(buffer_infos))
         templates = [a for bi in self._bis for a in bi.arrays()]

@@ -1489,6 +1489,7 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
     upload(plan.d_adj_btiles, plan.adj_btiles, st);
     upload(plan.d_adj_ltiles, plan.adj_ltiles, st);
     st.commit();
+    plan.forms_stale = false;
 }
 
 // Index blocks of a tile table: for every list tile whose columns number at most
@@ -1794,6 +1795,14 @@ void release_graph(ghexb_plan_s& plan)
 
 void launch_plan(ghexb_plan_s& plan, int form, cudaStream_t stream)
 {
+    if (plan.forms_stale && (form == GHEXB_FORM_PER_FIELD || form == GHEXB_FORM_PER_BOX))
+    {
+        host_stager st(plan, stream);
+        st.put(plan.d_xp, plan.xp);
+        st.put(plan.d_xb, plan.xb);
+        st.commit();
+        plan.forms_stale = false;
+    }
     auto run = [&](const xtile* base, const int32_t* blocks, std::pair<int, int> r) {
         if (r.second <= 0) return;
         check_cuda(launch_exchange(base + r.first, r.second, plan.per_thread, plan.block, stream, plan.d_idx,
@@ -1959,17 +1968,25 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
     // stream-ordered rewrite of the tables. The tile tables keep their size and device address,
     // so a captured graph stays valid. Their pointers move with the fields (the same tables as a
     // rebuild gives: ghexb_plan_check compares the two), else they are rebuilt.
-    if (R.ok)
-        relocate_tiles(plan, R);
-    else
-        build_tiles(plan, plan.d_idx);
+    // Moved tables keep their index blocks (indices do not move), and the per-field and per-box
+    // tables are uploaded when one of those forms is launched next (forms_stale).
     host_stager st(plan, stream);
-    st.put(plan.d_xf_blk, plan.xf_blk);
-    st.put(plan.d_xp_blk, plan.xp_blk);
-    st.put(plan.d_xb_blk, plan.xb_blk);
+    if (R.ok)
+    {
+        relocate_tiles(plan, R);
+        plan.forms_stale = true;
+    }
+    else
+    {
+        build_tiles(plan, plan.d_idx);
+        st.put(plan.d_xf_blk, plan.xf_blk);
+        st.put(plan.d_xp_blk, plan.xp_blk);
+        st.put(plan.d_xb_blk, plan.xb_blk);
+        st.put(plan.d_xp, plan.xp);
+        st.put(plan.d_xb, plan.xb);
+        plan.forms_stale = false;
+    }
     st.put(plan.d_xf, plan.xf);
-    st.put(plan.d_xp, plan.xp);
-    st.put(plan.d_xb, plan.xb);
     st.put(plan.d_gt, plan.gt);
     st.put(plan.d_lcols, plan.lcols);
     st.put(plan.d_boxes, plan.boxes);

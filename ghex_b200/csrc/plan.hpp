@@ -44,6 +44,7 @@ struct ghexb_plan_s
     // k_block_ints each): the indices of the tile's columns, loaded beside its record. Empty
     // when the plan has no lists.
     std::vector<int32_t> xf_blk, xp_blk, xb_blk;
+    bool forms_stale = false; // xp and xb moved on the host by a rebind, not yet on the device
     int32_t *d_xf_blk = nullptr, *d_xp_blk = nullptr, *d_xb_blk = nullptr;
     size_t cap_xf_blk = 0, cap_xp_blk = 0, cap_xb_blk = 0;
     // x-face boxes whose rows interleave (A's row r ends where B's row r + 1 begins): the
