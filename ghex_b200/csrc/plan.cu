@@ -1682,7 +1682,11 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
             for (int k = 0; k < g.nimg && contiguous; ++k) contiguous = g.img[k].t[0] == 1 || g.img[k].t[0] == -1;
             const int64_t w = (contiguous ? g.n[0] : 1) * (int64_t)g.esize;
             const int64_t full = (int64_t)gather_per_thread(g.nimg) * k_gather_block;
-            const uint32_t gc = (uint32_t)std::max<int64_t>(k_gather_block, std::min<int64_t>(full, full * w / (w + 32)));
+            int64_t sized = std::max<int64_t>(k_gather_block, std::min<int64_t>(full, full * w / (w + 32)));
+            // tuning: halved (gather_scale -1) or grown towards a full tile (1: x2, 2: x4)
+            if (plan.gather_scale < 0) sized = std::max<int64_t>(k_gather_block / 2, sized / 2);
+            else if (plan.gather_scale > 0) sized = std::min<int64_t>(full, sized << plan.gather_scale);
+            const uint32_t gc = (uint32_t)sized;
             const auto& of = plan.fields[g.own_slot];
             const fast_div f0 = fast_div::make((uint32_t)g.n[0]), f1 = fast_div::make((uint32_t)g.n[1]);
             const uint32_t n = (uint32_t)((int64_t)g.n[0] * g.n[1] * g.n[2]);
@@ -1995,6 +1999,67 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
     st.commit();
 }
 
+// The size of the adjoint's gather tiles of short rows (gather_scale -1, 0, 1, 2), timed like the
+// forward candidates: each adjoint after a cold-L2 read outside its events, the mean per launch.
+// The adjoint runs in place on the fields: the values it leaves are not an exchange's.
+void autotune_adjoint(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
+{
+    int l2 = 0;
+    check_cuda(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, plan.ctx->device), "cudaDeviceGetAttribute");
+    const size_t flush_bytes = std::max<size_t>(2 * (size_t)l2, 64u << 20);
+    uint4* flush = nullptr;
+    unsigned* sink = nullptr;
+    std::vector<cudaEvent_t> ev(2 * (size_t)repeats, nullptr);
+    auto cleanup = [&]() {
+        if (flush) cudaFree(flush);
+        if (sink) cudaFree(sink);
+        for (auto e : ev)
+            if (e) cudaEventDestroy(e);
+    };
+    const int start = plan.gather_scale;
+    int best_scale = start;
+    float best = 1e30f;
+    try
+    {
+        check_cuda(cudaMalloc(&flush, flush_bytes), "cudaMalloc(l2 flush)");
+        check_cuda(cudaMemsetAsync(flush, 0, flush_bytes, stream), "cudaMemsetAsync(l2 flush)");
+        check_cuda(cudaMalloc(&sink, sizeof(unsigned)), "cudaMalloc(l2 flush sink)");
+        for (auto& e : ev) check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+        const int fgrid = (plan.ctx ? plan.ctx->num_sms : 148) * 8;
+        for (int scale : {-1, 0, 1, 2})
+        {
+            plan.gather_scale = scale;
+            retile(plan, stream);
+            for (int w = 0; w < 3; ++w) adjoint_plan(plan, stream);
+            for (int r = 0; r < repeats; ++r)
+            {
+                check_cuda(launch_l2_flush(flush, flush_bytes / 16, sink, fgrid, stream), "l2 flush");
+                check_cuda(cudaEventRecord(ev[2 * r], stream), "cudaEventRecord");
+                adjoint_plan(plan, stream);
+                check_cuda(cudaEventRecord(ev[2 * r + 1], stream), "cudaEventRecord");
+            }
+            check_cuda(cudaEventSynchronize(ev[2 * repeats - 1]), "cudaEventSynchronize");
+            float total = 0.f;
+            for (int r = 0; r < repeats; ++r)
+            {
+                float ms = 0.f;
+                check_cuda(cudaEventElapsedTime(&ms, ev[2 * r], ev[2 * r + 1]), "cudaEventElapsedTime");
+                total += ms;
+            }
+            if (total < best) best = total, best_scale = scale;
+        }
+    }
+    catch (...)
+    {
+        cleanup();
+        plan.gather_scale = start;
+        throw;
+    }
+    cleanup();
+    plan.gather_scale = best_scale;
+    retile(plan, stream);
+}
+
 void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
 {
     if (repeats < 1) repeats = 10;
@@ -2098,6 +2163,7 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
     }
     cleanup();
     apply(bestc);
+    if (plan.adjoint_ok && plan.gather_ok) autotune_adjoint(plan, stream, repeats);
     check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
 }
 } // namespace ghexb

@@ -109,6 +109,9 @@ struct ghexb_plan_s
     int per_thread = 8;
     int block = 256;
     bool use_pairs = true; // batched and per-field tables move x-face pairs as segments
+    // adjoint gather tiles of short rows: -1 half the size, 0 sized by row length, 1 and 2 that
+    // size doubled or quadrupled (never beyond a full tile); chosen by the autotuner
+    int gather_scale = 0;
 
     // Staged form of box descriptors (staged.hpp), batched form only: the boxes marked in
     // box_staged are loaded through tensor maps by the staged kernel, which runs beside the
