@@ -75,7 +75,8 @@ def parse():
                     help="only run `--steps` launches of one form after `--warmup` (for ncu captures)")
     ap.add_argument("--tuning", default=None,
                     help="the tuning of the headline workload's plan, as printed in the bench line's "
-                         "roofline.traffic_tuning (e.g. k8.b128.p0.s1.st8x16384.c4.g1), instead of the autotuner's "
+                         "roofline.traffic_tuning (e.g. k8.b128.p0.s1.st8x16384.c4.g1; a trailing .a<-1..2> sets the adjoint's "
+                         "gather-tile scale), instead of the autotuner's "
                          "choice (for --profile runs and ncu launch lists, whose serialised timing would mislead the "
                          "autotuner)")
     return ap.parse_args()
@@ -105,17 +106,23 @@ def tuning_key(info: dict) -> str:
 
 
 def apply_tuning(plan, key: str) -> None:
-    """Sets a plan to the tuning named by tuning_key()."""
+    """Sets a plan to the tuning named by tuning_key(), optionally followed by `.a<scale>`, the
+    adjoint's gather-tile scale (-1 to 2)."""
     parts = {}
+    forward = []
     for tok in key.split("."):
         if tok.startswith("st"):
             a, b = tok[2:].split("x")
             parts["stages"], parts["stage_bytes"] = int(a), int(b)
         else:
             parts[tok[0]] = int(tok[1:])
+        if not tok.startswith("a"):
+            forward.append(tok)
     plan.set_tuning(parts["k"], parts["b"], parts["p"])
     plan.set_staged(parts["s"], parts.get("stages", 0), parts.get("stage_bytes", 0), parts.get("c", 0), parts.get("g", 0))
-    if tuning_key(plan.info()) != key:
+    if "a" in parts:
+        plan.set_adjoint_tuning(parts["a"])
+    if tuning_key(plan.info()) != ".".join(forward):
         raise ValueError(f"tuning {key} not applied: {tuning_key(plan.info())}")
 
 
@@ -676,7 +683,8 @@ def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline
         out["staged_status"] = plan.staged_status()
     if cfg in ("cfg4", "cfg4_f32"):
         ms_a = timer(lambda: plan.adjoint(s), steps, warmup)
-        out["adjoint"] = {"ms": ms_a, "vs_forward": ms_a / ms_b, "launches": plan.info()["adjoint_launches"]}
+        out["adjoint"] = {"ms": ms_a, "vs_forward": ms_a / ms_b, "launches": plan.info()["adjoint_launches"],
+                          "gather_scale": plan.info()["gather_scale"]}
     if baseline:
         case.reset()
         plan.launch(plan.BATCHED, s)

@@ -74,6 +74,7 @@ class PlanInfo(C.Structure):
         ("stage_bytes", C.c_int32),
         ("stage_consumers", C.c_int32),
         ("stage_ctas_per_sm", C.c_int32),
+        ("gather_scale", C.c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -123,6 +124,7 @@ SIGNATURES = {
     "ghexb_host_free": [_vp],
     "ghexb_calibrate_rows": [_vp, _vp, C.c_int64, _i, C.c_int64, C.c_int64, _i, _i, _vp],
     "ghexb_plan_staged_status": [_vp, C.POINTER(C.c_uint)],
+    "ghexb_plan_set_adjoint_tuning": [_vp, _i],
     "ghexb_plan_dram_floor": [_vp, C.POINTER(_vp), _i, _i, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
     "ghexb_plan_set_tuning": [_vp, _i, _i, _i],
     "ghexb_plan_launch": [_vp, _i, _vp],

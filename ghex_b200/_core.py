@@ -527,6 +527,11 @@ class ExchangePlan:
         rows and transposed edges, 2 every box it can take; and its pipeline shape (0 keeps)."""
         call("ghexb_plan_set_staged", self._h, mode, stages, stage_bytes, consumers, ctas_per_sm)
 
+    def set_adjoint_tuning(self, gather_scale: int = 0) -> None:
+        """Adjoint gather tiles of short rows sized by row length (0), halved (-1), doubled (1) or
+        quadrupled (2)."""
+        call("ghexb_plan_set_adjoint_tuning", self._h, gather_scale)
+
     def staged_status(self) -> int:
         """The staged kernel's status word since the last call (0: every wait ended in time)."""
         v = C.c_uint()

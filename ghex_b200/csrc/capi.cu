@@ -717,6 +717,13 @@ int ghexb_plan_check(ghexb_context ctx, const ghexb_field* fields, int n, int64_
                 (void)ghexb::check_tables(plan);
             }
         plan.staged_mode = 0;
+        // every size of the adjoint's gather tiles
+        for (int scale : {-1, 1, 2})
+        {
+            plan.gather_scale = scale;
+            (void)ghexb::check_tables(plan);
+        }
+        plan.gather_scale = 0;
         *elements_checked = ghexb::check_tables(plan);
         ghexb::check_relocation(plan);
     });
@@ -767,6 +774,7 @@ int ghexb_plan_get_info(ghexb_plan plan, ghexb_plan_info_t* info)
         info->stage_bytes = plan->stage_bytes;
         info->stage_consumers = plan->stage_consumers;
         info->stage_ctas_per_sm = plan->stage_ctas_per_sm;
+        info->gather_scale = plan->gather_scale;
     });
 }
 
@@ -808,6 +816,17 @@ int ghexb_plan_set_staged(ghexb_plan plan, int mode, int stages, int stage_bytes
         plan->stages = st, plan->stage_bytes = sb;
         if (consumers > 0) plan->stage_consumers = consumers;
         if (ctas_per_sm > 0) plan->stage_ctas_per_sm = ctas_per_sm;
+        ghexb::retile(*plan);
+        ghexb::check_cuda(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
+    });
+}
+
+int ghexb_plan_set_adjoint_tuning(ghexb_plan plan, int gather_scale)
+{
+    return guarded([&] {
+        require(plan != nullptr, "null plan");
+        require(gather_scale >= -1 && gather_scale <= 2, "gather scale must be -1, 0, 1 or 2");
+        plan->gather_scale = gather_scale;
         ghexb::retile(*plan);
         ghexb::check_cuda(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
     });

@@ -2001,9 +2001,42 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
 
 // The size of the adjoint's gather tiles of short rows (gather_scale -1, 0, 1, 2), timed like the
 // forward candidates: each adjoint after a cold-L2 read outside its events, the mean per launch.
-// The adjoint runs in place on the fields: the values it leaves are not an exchange's.
+// The adjoint updates the fields in place, so their memory (merged spans) is saved to a device
+// buffer first and restored after; the tuning is skipped, keeping the current size, when a field
+// is in host memory or the device has no room for the copy.
 void autotune_adjoint(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
 {
+    std::vector<std::pair<uintptr_t, uintptr_t>> spans;
+    for (size_t i = 0; i < plan.fields.size(); ++i)
+    {
+        if (i < plan.field_on_device.size() && !plan.field_on_device[i]) return;
+        const uintptr_t lo = reinterpret_cast<uintptr_t>(plan.fields[i].data);
+        spans.push_back({lo, lo + field_bytes(plan.fields[i])});
+    }
+    std::sort(spans.begin(), spans.end());
+    std::vector<std::pair<uintptr_t, uintptr_t>> merged;
+    for (const auto& sp : spans)
+        if (!merged.empty() && sp.first <= merged.back().second) merged.back().second = std::max(merged.back().second, sp.second);
+        else merged.push_back(sp);
+    size_t saved_bytes = 0;
+    for (const auto& m : merged) saved_bytes += (m.second - m.first + 255) & ~(size_t)255;
+    char* saved = nullptr;
+    if (cudaMalloc(&saved, std::max<size_t>(saved_bytes, 1)) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return;
+    }
+    auto copy_fields = [&](bool restore) {
+        size_t off = 0;
+        for (const auto& m : merged)
+        {
+            char* f = reinterpret_cast<char*>(m.first);
+            const size_t n = m.second - m.first;
+            check_cuda(cudaMemcpyAsync(restore ? f : saved + off, restore ? saved + off : f, n, cudaMemcpyDeviceToDevice, stream),
+                       "cudaMemcpyAsync(adjoint tuning copy)");
+            off += (n + 255) & ~(size_t)255;
+        }
+    };
     int l2 = 0;
     check_cuda(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, plan.ctx->device), "cudaDeviceGetAttribute");
     const size_t flush_bytes = std::max<size_t>(2 * (size_t)l2, 64u << 20);
@@ -2021,6 +2054,7 @@ void autotune_adjoint(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
     float best = 1e30f;
     try
     {
+        copy_fields(false);
         check_cuda(cudaMalloc(&flush, flush_bytes), "cudaMalloc(l2 flush)");
         check_cuda(cudaMemsetAsync(flush, 0, flush_bytes, stream), "cudaMemsetAsync(l2 flush)");
         check_cuda(cudaMalloc(&sink, sizeof(unsigned)), "cudaMalloc(l2 flush sink)");
@@ -2051,13 +2085,25 @@ void autotune_adjoint(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
     }
     catch (...)
     {
+        try
+        {
+            copy_fields(true);
+        }
+        catch (...)
+        {
+        }
+        cudaStreamSynchronize(stream);
         cleanup();
+        cudaFree(saved);
         plan.gather_scale = start;
         throw;
     }
     cleanup();
     plan.gather_scale = best_scale;
     retile(plan, stream);
+    copy_fields(true);
+    check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    cudaFree(saved);
 }
 
 void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)

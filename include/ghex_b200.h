@@ -79,6 +79,8 @@ typedef struct ghexb_plan_info_t
     int32_t stage_bytes;       /* current tuning: bytes per stage */
     int32_t stage_consumers;   /* current tuning: consumer warps per staged CTA */
     int32_t stage_ctas_per_sm; /* current tuning: staged CTAs per SM */
+    int32_t gather_scale;      /* current adjoint tuning: gather tiles of short rows halved (-1),
+                                  sized by row length (0), doubled (1) or quadrupled (2) */
 } ghexb_plan_info_t;
 
 /* ---- errors / version ----------------------------------------------------------------- */
@@ -268,6 +270,10 @@ int ghexb_plan_set_tuning(ghexb_plan plan, int elems_per_thread, int block, int 
  * the current one (mode < 0 keeps). Fields in host memory stay on the element kernel.
  * Invalidates the captured graph. */
 int ghexb_plan_set_staged(ghexb_plan plan, int mode, int stages, int stage_bytes, int consumers, int ctas_per_sm);
+/* Adjoint tiles (no GHEX counterpart): the gather form's tiles of short rows are sized by row
+ * length (gather_scale 0), halved (-1), doubled (1) or quadrupled (2), never beyond a full tile.
+ * Invalidates the captured graphs. */
+int ghexb_plan_set_adjoint_tuning(ghexb_plan plan, int gather_scale);
 /* Status word of the staged kernel since the last call, then cleared: 0 when every wait of the
  * kernel ended in time; bit 0 a load, bit 1 a write that gave up waiting (its halos are then
  * incomplete). Synchronises the device. */
@@ -286,7 +292,10 @@ int ghexb_plan_adjoint_launch(ghexb_plan plan, void* stream);
  * whose fields and gradients are new tensors at every step. */
 int ghexb_plan_rebind(ghexb_plan plan, void* const* data, int n, void* stream);
 /* Times the candidate tunings on `stream` with CUDA events and keeps the fastest one; the
- * chosen tuning is returned through `info` when it is not NULL. Runs real exchanges. */
+ * chosen tuning is returned through `info` when it is not NULL. Runs real exchanges. Then, for
+ * float fields in device memory, times the adjoint's gather-tile sizes (ghexb_plan_set_adjoint_
+ * tuning) on the fields, whose memory it saves to a device buffer first and restores after;
+ * without room for that copy the adjoint keeps its tiles. */
 int ghexb_plan_autotune(ghexb_plan plan, void* stream, int repeats, ghexb_plan_info_t* info);
 
 /* ---- batched exchange without device allocation. This entry point has no counterpart in GHEX.

@@ -82,6 +82,21 @@ def test_autotune_then_bitexact(cuda):
     assert run.mismatches(expected) == {}
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_autotune_keeps_fields(cuda, dtype):
+    """The autotuner times exchanges and adjoints on the plan's own fields: after it, every cell
+    (interiors and halos) holds what one exchange of the original values leaves."""
+    shape = (40, 30, 12)
+    w = W.RegularWorkload("tune", shape, (True, True, False), W.regular_decomposition(shape, (2, 2, 1), 3))
+    w.fields = [W.FieldSpec("f", dtype, (2, 2, 1, 1, 1, 1), 4), W.FieldSpec("g", dtype, (1, 1, 1, 1, 0, 0), 9)]
+    run = RegularRun(w, cuda)
+    expected = run.oracle()
+    plan = R.make_exchange_plan(run.ctx, run.bis)
+    info = plan.autotune(repeats=2)
+    assert info["gather_scale"] in (-1, 0, 1, 2)
+    assert run.mismatches(expected) == {}
+
+
 @pytest.mark.parametrize("periodic", [(True, True), (False, True)])
 def test_simple_2d_known_answer(cuda, periodic):
     """test_simple_regular_domain.cpp's check on the device: (x, y) int32 pairs, x fastest."""
@@ -134,10 +149,11 @@ def test_out_of_range_box_is_rejected(cuda):
     assert e.value.code == _capi.ERR_RANGE
 
 
+@pytest.mark.parametrize("gather_scale", [0, -1, 1, 2])
 @pytest.mark.parametrize("cfg", ["cfg0", "cfg1_small", "cfg4_small"])
-def test_adjoint_bitexact(cuda, cfg):
+def test_adjoint_bitexact(cuda, cfg, gather_scale):
     """The device adjoint equals the oracle's fixed-order explicit transpose bit for bit, on random
-    data in every cell (halos included)."""
+    data in every cell (halos included), at every gather-tile size."""
     from oracle import regular as O
     w = {"cfg0": W.config0(), "cfg1_small": W.config1(shape=(50, 40, 12)),
          "cfg4_small": W.config4(shape=(32, 32, 16))}[cfg]
@@ -153,8 +169,9 @@ def test_adjoint_bitexact(cuda, cfg):
             grads[name].append(g)
     torch.cuda.synchronize()
     plan = R.make_exchange_plan(run.ctx, run.bis)
+    plan.set_adjoint_tuning(gather_scale)
     info = plan.info()
-    assert info["adjoint_launches"] == 1 and info["adjoint_cells"] > 0
+    assert info["adjoint_launches"] == 1 and info["adjoint_cells"] > 0 and info["gather_scale"] == gather_scale
     plan.adjoint()
     for halos, specs in w.halo_groups().items():
         doms = [O.Domain(i, f, l) for i, f, l in w.domains]
