@@ -43,6 +43,7 @@ ERR_INTERNAL = 7
 
 F32, F64, I32, I64, U8, U16 = 0, 1, 2, 3, 4, 5
 FORM_BATCHED, FORM_PER_FIELD, FORM_PER_BOX = 0, 1, 2
+IPC_HANDLE_BYTES = 64  # GHEXB_IPC_HANDLE_BYTES
 
 _vp = C.c_void_p
 _i = C.c_int
@@ -125,6 +126,11 @@ SIGNATURES = {
     "ghexb_calibrate_rows": [_vp, _vp, C.c_int64, _i, C.c_int64, C.c_int64, _i, _i, _vp],
     "ghexb_plan_staged_status": [_vp, C.POINTER(C.c_uint)],
     "ghexb_plan_set_adjoint_tuning": [_vp, _i],
+    "ghexb_plan_create_sharded": [_vp, C.POINTER(_vp), _i, C.c_char_p, _i, C.POINTER(_vp)],
+    "ghexb_plan_check_sharded": [_vp, C.POINTER(_vp), _i, C.c_char_p, _i, _pi64],
+    "ghexb_ipc_export": [_vp, C.c_char_p, _pi64],
+    "ghexb_ipc_open": [C.c_char_p, _i64, C.POINTER(_vp)],
+    "ghexb_ipc_close": [C.c_char_p],
     "ghexb_plan_dram_floor": [_vp, C.POINTER(_vp), _i, _i, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
     "ghexb_plan_set_tuning": [_vp, _i, _i, _i],
     "ghexb_plan_launch": [_vp, _i, _vp],

@@ -336,8 +336,13 @@ class FieldDescriptorBase:
     def domain_key(self) -> Any:  # pragma: no cover - abstract
         raise NotImplementedError
 
-    def _wrap(self, pattern: PatternContainer) -> C.c_void_p:  # pragma: no cover - abstract
+    def _spec(self) -> dict:  # pragma: no cover - abstract
+        """Everything but the address that wraps this field's memory (wrap_spec): picklable, so
+        that another process can wrap the same memory once it has mapped it."""
         raise NotImplementedError
+
+    def _wrap(self, pattern: PatternContainer) -> C.c_void_p:
+        return wrap_spec(pattern, self._spec(), self.info["ptr"])
 
     def _bind(self, pattern: PatternContainer) -> C.c_void_p:
         key = id(pattern)
@@ -352,6 +357,22 @@ class FieldDescriptorBase:
         for h in getattr(self, "_handles", {}).values():
             _release("ghexb_field_destroy", h)
         self._handles = {}
+
+
+def wrap_spec(pattern: PatternContainer, spec: dict, ptr: int) -> C.c_void_p:
+    """A field handle for the memory at `ptr` laid out as `spec` (FieldDescriptorBase._spec) and
+    bound to `pattern`."""
+    from ._capi import int_array, int64_array
+    h = C.c_void_p()
+    if spec["kind"] == "list":
+        call("ghexb_field_wrap_unstructured", pattern._h, spec["domain"], spec["dtype"], C.c_void_p(ptr),
+             spec["levels"], int(spec["levels_first"]), spec["outer_stride"], C.byref(h))
+    else:
+        dom = pattern.domain_index(spec["domain"]) if spec["by_index"] else spec["domain"]
+        call("ghexb_field_wrap", pattern._h, dom, spec["dtype"], C.c_void_p(ptr), spec["ndim"],
+             int_array(spec["offsets"]), int_array(spec["extents"]), int_array(spec["layout"]),
+             int64_array(spec["strides"]), spec["ncomp"], int(spec["is_vector"]), C.byref(h))
+    return h
 
 
 def _flatten(args: tuple) -> list[BufferInfo]:

@@ -11,6 +11,7 @@
 #include <string>
 
 #include "exchange.hpp"
+#include "ipc.hpp"
 #include "kernels.hpp"
 #include "plan.hpp"
 #include "stencil.hpp"
@@ -702,30 +703,94 @@ int ghexb_plan_create_ipr(ghexb_context ctx, const ghexb_field* fields, int n, g
     });
 }
 
-int ghexb_plan_check(ghexb_context ctx, const ghexb_field* fields, int n, int64_t* elements_checked)
+int ghexb_plan_create_sharded(ghexb_context ctx, const ghexb_field* fields, int n, const unsigned char* local, int mode,
+    ghexb_plan* out)
 {
     return guarded([&] {
-        require(ctx && fields && elements_checked, "null argument");
-        ghexb_plan_s plan;
-        ghexb::build_tables(plan, ctx, fields, n);
-        // every staged mode at two stage sizes (host geometry only), then the element kernel alone
-        plan.encode_maps = false;
+        require(ctx && fields && local && out, "null argument");
+        require(n > 0, "an exchange needs at least one field");
+        auto plan = std::make_unique<ghexb_plan_s>();
+        plan->shard_mode = mode;
+        plan->shard_local.assign(local, local + n);
+        ghexb::build_plan(*plan, ctx, fields, n);
+        *out = plan.release();
+    });
+}
+
+namespace
+{
+// host replay of every table of a plan (all staged modes and adjoint tile sizes)
+int64_t check_all(ghexb_plan_s& plan)
+{
+    // every staged mode at two stage sizes (host geometry only), then the element kernel alone
+    plan.encode_maps = false;
+    if (plan.shard_mode == 0)
         for (int mode : {1, 2})
             for (int bytes : {16384, 4096})
             {
                 plan.staged_mode = mode, plan.stage_bytes = bytes;
                 (void)ghexb::check_tables(plan);
             }
-        plan.staged_mode = 0;
-        // every size of the adjoint's gather tiles
-        for (int scale : {-1, 1, 2})
-        {
-            plan.gather_scale = scale;
-            (void)ghexb::check_tables(plan);
-        }
-        plan.gather_scale = 0;
-        *elements_checked = ghexb::check_tables(plan);
-        ghexb::check_relocation(plan);
+    plan.staged_mode = 0;
+    // every size of the adjoint's gather tiles
+    for (int scale : {-1, 1, 2})
+    {
+        plan.gather_scale = scale;
+        (void)ghexb::check_tables(plan);
+    }
+    plan.gather_scale = 0;
+    const int64_t n = ghexb::check_tables(plan);
+    if (plan.shard_mode == 0) ghexb::check_relocation(plan);
+    return n;
+}
+} // namespace
+
+int ghexb_plan_check_sharded(ghexb_context ctx, const ghexb_field* fields, int n, const unsigned char* local, int mode,
+    int64_t* elements_checked)
+{
+    return guarded([&] {
+        require(ctx && fields && local && elements_checked, "null argument");
+        require(n > 0, "an exchange needs at least one field");
+        ghexb_plan_s plan;
+        plan.shard_mode = mode;
+        plan.shard_local.assign(local, local + n);
+        ghexb::build_tables(plan, ctx, fields, n);
+        (void)check_all(plan);
+        *elements_checked = plan.halo_elements;
+    });
+}
+
+int ghexb_ipc_export(const void* ptr, unsigned char* handle, int64_t* offset)
+{
+    return guarded([&] {
+        require(ptr && handle && offset, "null argument");
+        ghexb::ipc_export(ptr, handle, offset);
+    });
+}
+
+int ghexb_ipc_open(const unsigned char* handle, int64_t offset, void** ptr)
+{
+    return guarded([&] {
+        require(handle && ptr, "null argument");
+        *ptr = ghexb::ipc_open(handle, offset);
+    });
+}
+
+int ghexb_ipc_close(const unsigned char* handle)
+{
+    return guarded([&] {
+        require(handle != nullptr, "null argument");
+        ghexb::ipc_close(handle);
+    });
+}
+
+int ghexb_plan_check(ghexb_context ctx, const ghexb_field* fields, int n, int64_t* elements_checked)
+{
+    return guarded([&] {
+        require(ctx && fields && elements_checked, "null argument");
+        ghexb_plan_s plan;
+        ghexb::build_tables(plan, ctx, fields, n);
+        *elements_checked = check_all(plan);
     });
 }
 
@@ -812,6 +877,7 @@ int ghexb_plan_set_staged(ghexb_plan plan, int mode, int stages, int stage_bytes
         const int st = stages > 0 ? stages : plan->stages, sb = stage_bytes > 0 ? stage_bytes : plan->stage_bytes;
         require(st >= 2, "at least 2 stages");
         require((size_t)st * sb + 128 <= 227 * 1024, "stages x stage bytes exceed the shared memory of a CTA");
+        require(mode <= 0 || plan->shard_mode == 0, "a sharded plan has no staged form");
         if (mode >= 0) plan->staged_mode = mode;
         plan->stages = st, plan->stage_bytes = sb;
         if (consumers > 0) plan->stage_consumers = consumers;

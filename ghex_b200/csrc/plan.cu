@@ -710,6 +710,23 @@ void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* f
         if (!fields[i]) throw error(GHEXB_ERR_INVALID, "null field handle");
         plan.fields.push_back(*fields[i]);
     }
+    if (plan.shard_mode != 0)
+    {
+        if (plan.shard_mode != 1 && plan.shard_mode != 2) throw error(GHEXB_ERR_INVALID, "sharded mode must be 1 (pull) or 2 (push)");
+        if ((int)plan.shard_local.size() != n) throw error(GHEXB_ERR_INVALID, "one locality flag per field");
+        if (plan.in_place_receive) throw error(GHEXB_ERR_INVALID, "an in-place receive is not sharded");
+        if (plan.shard_mode == 1)
+        {
+            plan.adjoint_ok = false;
+            plan.adjoint_reason = "the pull form of a sharded exchange has no adjoint (its push form has)";
+        }
+    }
+    // descriptors of a sharded plan: those writing (pull) or reading (push) a local field
+    auto kept = [&](int dst_slot, int src_slot) {
+        if (plan.shard_mode == 1) return plan.shard_local[dst_slot] != 0;
+        if (plan.shard_mode == 2) return plan.shard_local[src_slot] != 0;
+        return true;
+    };
     // patterns in order of first appearance; per (pattern, domain) the field slots in order
     std::vector<ghexb_pattern_s*> pats;
     std::vector<std::vector<std::vector<int>>> groups;
@@ -789,7 +806,8 @@ void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* f
                         const auto& dst = plan.fields[Fd[k]];
                         const auto& src = plan.fields[Fe[k]];
                         check_pair(dst, src);
-                        B.list_pair(dst, Fd[k], src, Fe[k], rlids, se->lids, logical_of(pi, (int)k));
+                        const int lg = logical_of(pi, (int)k);
+                        if (kept(Fd[k], Fe[k])) B.list_pair(dst, Fd[k], src, Fe[k], rlids, se->lids, lg);
                     }
                 }
                 continue;
@@ -803,6 +821,7 @@ void build_tables(ghexb_plan_s& plan, ghexb_context_s* ctx, const ghexb_field* f
                     const auto& src = plan.fields[Fe[k]];
                     check_pair(dst, src);
                     const int lg = logical_of(pi, (int)k);
+                    if (!kept(Fd[k], Fe[k])) continue;
                     for (const auto& sp : re.spaces)
                     {
                         if (P.kind == pattern_kind::regular) B.regular_space(P, re.neighbor, dst, Fd[k], src, Fe[k], sp, lg);
@@ -1436,6 +1455,28 @@ int64_t check_tables(ghexb_plan_s& plan)
             }
         checked += (int64_t)l.count * l.levels;
     }
+    // a sharded plan: every forward descriptor writes (pull) or reads (push) a local field, and
+    // every adjoint owner is local
+    if (plan.shard_mode != 0)
+    {
+        const bool pull = plan.shard_mode == 1;
+        auto local = [&](int slot) { return plan.shard_local[slot] != 0; };
+        for (size_t i = 0; i < plan.boxes.size(); ++i)
+            if (!local(pull ? plan.box_dst_slot[i] : plan.box_src_slot[i]))
+                throw error(GHEXB_ERR_INTERNAL, "a sharded plan holds a box of another process");
+        for (size_t i = 0; i < plan.lists.size(); ++i)
+            if (!local(pull ? plan.list_dst_slot[i] : plan.list_src_slot[i]))
+                throw error(GHEXB_ERR_INTERNAL, "a sharded plan holds a list of another process");
+        if (plan.gather_ok)
+            for (const auto& g : plan.cells)
+                if (!local(g.own_slot)) throw error(GHEXB_ERR_INTERNAL, "a sharded adjoint gathers into another process's field");
+        if (plan.list_gather_ok)
+            for (const auto& o : plan.lowners)
+                if (!local(o.slot)) throw error(GHEXB_ERR_INTERNAL, "a sharded adjoint gathers into another process's field");
+        for (size_t i = 0; i < plan.adj_lists.size() && plan.adjoint_ok; ++i)
+            if (!local(plan.adj_src_slot[i]))
+                throw error(GHEXB_ERR_INTERNAL, "a sharded adjoint accumulates into another process's owner");
+    }
     return checked;
 }
 
@@ -1937,6 +1978,7 @@ void put_descriptors(ghexb_plan_s& plan, cudaStream_t stream)
 
 void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stream)
 {
+    if (plan.shard_mode != 0) throw error(GHEXB_ERR_INVALID, "a sharded plan cannot be rebound: build a new one");
     if (n != (int)plan.fields.size())
         throw error(GHEXB_ERR_INVALID, "rebind needs one pointer per field of the plan (" +
                                            std::to_string(plan.fields.size()) + ")");
@@ -2131,7 +2173,7 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
             for (bool pairs : {false, true})
                 if (!pairs || !plan.pairs.empty()) cands.push_back({k, block, pairs, 0, start.stages, start.stage_bytes,
                                                        start.consumers, start.ctas});
-    const bool stageable = !plan.boxes.empty();
+    const bool stageable = !plan.boxes.empty() && plan.shard_mode == 0;
     const size_t n_element = cands.size();
 
     // every timed launch starts with a cold L2: read a buffer of twice the L2 size first
@@ -2216,7 +2258,8 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
     }
     cleanup();
     apply(bestc);
-    if (plan.adjoint_ok && plan.gather_ok) autotune_adjoint(plan, stream, repeats);
+    // (not on a sharded plan: its adjoint zeroes halos in other processes' memory)
+    if (plan.adjoint_ok && plan.gather_ok && plan.shard_mode == 0) autotune_adjoint(plan, stream, repeats);
     check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
 }
 } // namespace ghexb

@@ -19,6 +19,14 @@ struct ghexb_plan_s
     // unstructured in-place receive (unstructured/communication_object_ipr.hpp:127-141): the
     // values received from a neighbour land on consecutive halo rows from its first receive index
     bool in_place_receive = false;
+    // Sharded exchange (one process per GPU): `fields` holds every domain's fields, those of other
+    // processes mapped from their memory, and shard_local[slot] marks this process's own. mode 0:
+    // every descriptor; 1 (pull): the descriptors that write a local field, reading peers'
+    // interiors; 2 (push): those that read a local field, writing peers' halos, whose adjoint
+    // gathers every image of the local owners (the pull form has no adjoint: a remote owner's
+    // images lie in several processes' plans).
+    int shard_mode = 0;
+    std::vector<char> shard_local;
 
     // host tables
     std::vector<ghexb::box_desc> boxes;

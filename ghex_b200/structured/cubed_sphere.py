@@ -12,7 +12,7 @@ import ctypes as C
 from dataclasses import dataclass
 from typing import Any, Sequence, Union
 
-from .._capi import call, int_array, int64_array
+from .._capi import call, int_array
 from .._core import (Architecture, FieldDescriptorBase, PatternContainer, array_info, check_arch, context,
                      make_bulk_communication_object, make_communication_object, make_context, make_exchange_plan)
 from .regular import _layout_order
@@ -109,13 +109,10 @@ class FieldDescriptor(FieldDescriptorBase):
     def domain_id(self):
         return self.domain.domain_id()
 
-    def _wrap(self, pattern: PatternContainer):
-        h = C.c_void_p()
-        call("ghexb_field_wrap", pattern._h, pattern.domain_index(self.domain_key()), self.info["dtype"],
-             C.c_void_p(self.info["ptr"]), 4, int_array(self.offsets), int_array(self.extents),
-             int_array(self.layout), int64_array(self.info["strides"]), self.num_components, int(self.is_vector),
-             C.byref(h))
-        return h
+    def _spec(self) -> dict:
+        return {"kind": "box", "domain": self.domain_key(), "by_index": True, "dtype": self.info["dtype"], "ndim": 4,
+                "offsets": tuple(self.offsets), "extents": tuple(self.extents), "layout": tuple(self.layout),
+                "strides": tuple(self.info["strides"]), "ncomp": self.num_components, "is_vector": bool(self.is_vector)}
 
 
 def make_field_descriptor(domain: DomainDescriptor, field: Any, offsets: Sequence[int], extents: Sequence[int],

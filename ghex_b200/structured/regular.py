@@ -241,12 +241,11 @@ class FieldDescriptor(FieldDescriptorBase):
     def domain_id(self) -> int:
         return self.domain_desc.domain_id()
 
-    def _wrap(self, pattern: PatternContainer):
-        h = C.c_void_p()
-        call("ghexb_field_wrap", pattern._h, self.domain_desc.domain_id(), self.info["dtype"],
-             C.c_void_p(self.info["ptr"]), self.ndim, int_array(self.offsets), int_array(self.extents),
-             int_array(self.layout), int64_array(self.info["strides"]), self.num_components, 0, C.byref(h))
-        return h
+    def _spec(self) -> dict:
+        return {"kind": "box", "domain": self.domain_desc.domain_id(), "by_index": False, "dtype": self.info["dtype"],
+                "ndim": self.ndim, "offsets": tuple(self.offsets), "extents": tuple(self.extents),
+                "layout": tuple(self.layout), "strides": tuple(self.info["strides"]), "ncomp": self.num_components,
+                "is_vector": False}
 
 
 def make_field_descriptor(domain_desc: DomainDescriptor, field: Any, offsets: Sequence[int],

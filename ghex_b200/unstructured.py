@@ -168,11 +168,9 @@ class FieldDescriptor(FieldDescriptorBase):
     def domain_id(self) -> int:
         return self.domain_desc.domain_id()
 
-    def _wrap(self, pattern: PatternContainer):
-        h = C.c_void_p()
-        call("ghexb_field_wrap_unstructured", pattern._h, self.domain_desc.domain_id(), self.info["dtype"],
-             C.c_void_p(self.info["ptr"]), self.levels, int(self.levels_first), self.outer_stride, C.byref(h))
-        return h
+    def _spec(self) -> dict:
+        return {"kind": "list", "domain": self.domain_desc.domain_id(), "dtype": self.info["dtype"],
+                "levels": self.levels, "levels_first": bool(self.levels_first), "outer_stride": self.outer_stride}
 
 
 def make_field_descriptor(domain_desc: DomainDescriptor, field: Any, *,

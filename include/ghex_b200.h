@@ -241,6 +241,37 @@ int ghexb_plan_create(ghexb_context ctx, const ghexb_field* fields, int n, ghexb
 /* The plan of an in-place receive exchange (see ghexb_co_create_ipr). */
 int ghexb_plan_create_ipr(ghexb_context ctx, const ghexb_field* fields, int n, ghexb_plan* out);
 int ghexb_plan_destroy(ghexb_plan plan);
+
+/* ---- sharded exchange, one process per GPU: replaces the remote sends and receives of an
+ * exchange between ranks (communication_object.hpp:433-512 posting oomph messages,
+ * packer.hpp:32-59 packing them). Every process builds the same patterns over all domains;
+ * `fields` holds the fields of every domain, those of other processes wrapped around their
+ * memory mapped into this one (ghexb_ipc_open), and local[i] != 0 marks this process's own.
+ * mode 1 (pull) keeps the descriptors that write a local field: the kernel reads peers'
+ * interiors and fills this process's halos. mode 2 (push) keeps those that read a local field:
+ * the kernel writes this process's interior values into peers' halos; its adjoint gathers every
+ * image of the local owners (the pull form has no adjoint). No descriptor is in two processes'
+ * plans, and together they hold every descriptor of the exchange. The caller orders the
+ * processes: every process's fields must be final before any process launches, and no process
+ * may change its fields until every process's launch is done (a barrier on both sides). The
+ * staged form and rebinding are not available on sharded plans. */
+int ghexb_plan_create_sharded(ghexb_context ctx, const ghexb_field* fields, int n, const unsigned char* local, int mode,
+    ghexb_plan* out);
+/* Host-only replay of a sharded plan's tables (as ghexb_plan_check, and every descriptor and
+ * adjoint owner checked to be this process's); elements_checked is the number of halo elements
+ * its forward kernel writes. */
+int ghexb_plan_check_sharded(ghexb_context ctx, const ghexb_field* fields, int n, const unsigned char* local, int mode,
+    int64_t* elements_checked);
+/* CUDA IPC of field memory (device memory from cudaMalloc, as PyTorch's caching allocator
+ * uses): `handle` (64 bytes) names the allocation holding `ptr`, `offset` the byte of `ptr` in
+ * it. ghexb_ipc_open maps another process's allocation once per process (later openings of the
+ * same handle count references) and returns the address of byte `offset`; ghexb_ipc_close drops
+ * one opening. A process cannot open its own handles. */
+#define GHEXB_IPC_HANDLE_BYTES 64
+int ghexb_ipc_export(const void* ptr, unsigned char* handle, int64_t* offset);
+int ghexb_ipc_open(const unsigned char* handle, int64_t offset, void** ptr);
+int ghexb_ipc_close(const unsigned char* handle);
+
 /* Host-only validation, no device needed: builds the plan's tables and replays the address
  * computation of every element the forward and adjoint kernels touch, failing with
  * GHEXB_ERR_RANGE if one falls outside its field's memory span. The staged form is replayed in
