@@ -92,7 +92,7 @@ def make_context(group: Any = None, device: int | None = None) -> context:
 
 
 class Pattern:
-    """The pattern of every process's domains (the same on every process, domains in rank order);
+    """The pattern of every process's domains (the same on every process, domains in id order);
     binds this process's fields."""
 
     def __init__(self, ctx: context, pattern: _core.PatternContainer, owner: dict, seq: int):
@@ -129,10 +129,16 @@ def make_pattern(ctx: context, halo_gen: Any, *args) -> Pattern:
     domains = [d for part in parts for d in part]
     if not domains:
         raise ValueError("make_pattern needs at least one domain")
+    # domains in the order of their ids, whichever rank holds them: the order of descriptors, and
+    # so of the adjoint's additions into an owner, is then that of a single process given the
+    # domains in id order
+    order = sorted(range(len(domains)), key=lambda k: domains[k].domain_id())
     if isinstance(halo_gen, (list, tuple)):
         if len(halo_gen) != len(local):
             raise ValueError("one halo generator per local domain is needed")
-        halo_gen = [h for part in ctx.all_gather(list(halo_gen)) for h in part]
+        gens = [h for part in ctx.all_gather(list(halo_gen)) for h in part]
+        halo_gen = [gens[k] for k in order]
+    domains = [domains[k] for k in order]
     module = importlib.import_module(type(domains[0]).__module__)
     pattern = module.make_pattern(ctx, halo_gen, *extra, domains)
     owner = {}
