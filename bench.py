@@ -681,7 +681,7 @@ def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline
            "tuning": {k: tuning[k] for k in TUNING_KEYS}}
     if plan.info()["staged_mode"]:
         out["staged_status"] = plan.staged_status()
-    if cfg in ("cfg4", "cfg4_f32"):
+    if cfg in ("cfg2", "cfg3", "cfg4", "cfg4_f32"):
         ms_a = timer(lambda: plan.adjoint(s), steps, warmup)
         out["adjoint"] = {"ms": ms_a, "vs_forward": ms_a / ms_b, "launches": plan.info()["adjoint_launches"],
                           "gather_scale": plan.info()["gather_scale"]}

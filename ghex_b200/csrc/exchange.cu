@@ -295,12 +295,16 @@ __device__ __forceinline__ void gather_elements(const gtile& t)
 // Unstructured owner columns: element e is level e mod n0 of owner e / n0 of the group; the
 // owner's and its images' column addresses come from the column table.
 template<int K, int NI, typename F>
-__device__ __forceinline__ void list_gather_elements(const gtile& t, const uint64_t* __restrict__ cols)
+__device__ __forceinline__ void list_gather_elements(const gtile& t, const uint64_t* __restrict__ cols,
+    const uint64_t* blk)
 {
     F h[K][NI];
     F acc[K];
     F* own[K];
     F* img[K][NI];
+    // the tile's columns from its block in shared memory, else from the column table
+    const uint32_t j0 = blk ? fdiv(t.e0, t.m0, t.l0) : 0u;
+    const uint64_t* base = blk ? blk - (size_t)j0 * (NI + 1) : cols + t.col0;
 #pragma unroll
     for (int k = 0; k < K; ++k)
     {
@@ -310,10 +314,10 @@ __device__ __forceinline__ void list_gather_elements(const gtile& t, const uint6
             const uint32_t g = t.e0 + e;
             const uint32_t j = fdiv(g, t.m0, t.l0);
             const int32_t lev = (int32_t)(g - j * t.n0);
-            const uint64_t* p = cols + t.col0 + (size_t)j * (NI + 1);
-            own[k] = reinterpret_cast<F*>(__ldg(p)) + lev * t.o0;
+            const uint64_t* p = base + (size_t)j * (NI + 1);
+            own[k] = reinterpret_cast<F*>(blk ? p[0] : __ldg(p)) + lev * t.o0;
 #pragma unroll
-            for (int i = 0; i < NI; ++i) img[k][i] = reinterpret_cast<F*>(__ldg(p + 1 + i)) + lev * t.img[0].t0;
+            for (int i = 0; i < NI; ++i) img[k][i] = reinterpret_cast<F*>(blk ? p[1 + i] : __ldg(p + 1 + i)) + lev * t.img[0].t0;
             acc[k] = __ldcg(own[k]);
 #pragma unroll
             for (int i = 0; i < NI; ++i) h[k][i] = __ldcg(img[k][i]);
@@ -358,16 +362,24 @@ __global__ void __launch_bounds__(k_gather_block, 3) gather_kernel(const gtile* 
 
 // The unstructured owner groups have a kernel of their own, so that the box kernel's code (and
 // its instruction-cache footprint) stays that of the box classes.
+static_assert(k_gblock_entries % 2 == 0 && 16 + k_gblock_entries / 2 <= k_gather_block, "column block load lanes");
+
 __global__ void __launch_bounds__(k_gather_block, 3) list_gather_kernel(const gtile* __restrict__ tiles,
-    const uint64_t* __restrict__ cols)
+    const uint64_t* __restrict__ cols, const uint64_t* __restrict__ blocks)
 {
     __shared__ gtile t;
+    __shared__ __align__(16) uint64_t blk_s[k_gblock_entries];
+    // threads 16.. load the tile's column block while threads 0..15 load the record
+    if (blocks && threadIdx.x >= 16 && threadIdx.x < 16 + k_gblock_entries / 2)
+        reinterpret_cast<uint4*>(blk_s)[threadIdx.x - 16] =
+            __ldg(reinterpret_cast<const uint4*>(blocks + (size_t)blockIdx.x * k_gblock_entries) + (threadIdx.x - 16));
     load_record<16>(t, tiles);
+    const uint64_t* blk = blocks && t.pad[0] ? blk_s : nullptr;
     switch (t.cls)
     {
 #define GHEXB_CASE(NI)                                                                                                 \
-    case list_gather_class(8, NI): list_gather_elements<gather_per_thread(NI), NI, double>(t, cols); break;          \
-    case list_gather_class(4, NI): list_gather_elements<gather_per_thread(NI), NI, float>(t, cols); break;
+    case list_gather_class(8, NI): list_gather_elements<gather_per_thread(NI), NI, double>(t, cols, blk); break;     \
+    case list_gather_class(4, NI): list_gather_elements<gather_per_thread(NI), NI, float>(t, cols, blk); break;
         GHEXB_CASE(1)
         GHEXB_CASE(2)
         GHEXB_CASE(3)
@@ -408,10 +420,11 @@ cudaError_t launch_gather(const gtile* tiles, int ntiles, cudaStream_t stream)
     return cudaGetLastError();
 }
 
-cudaError_t launch_list_gather(const gtile* tiles, int ntiles, const uint64_t* cols, cudaStream_t stream)
+cudaError_t launch_list_gather(const gtile* tiles, int ntiles, const uint64_t* cols, const uint64_t* blocks,
+    cudaStream_t stream)
 {
     if (ntiles <= 0) return cudaSuccess;
-    list_gather_kernel<<<ntiles, k_gather_block, 0, stream>>>(tiles, cols);
+    list_gather_kernel<<<ntiles, k_gather_block, 0, stream>>>(tiles, cols, blocks);
     return cudaGetLastError();
 }
 } // namespace ghexb

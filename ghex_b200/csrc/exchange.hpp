@@ -81,5 +81,9 @@ cudaError_t launch_exchange(const xtile* tiles, int ntiles, int k, int block, cu
 // gather_per_thread(nimg) * k_gather_block elements. launch_gather takes box cells,
 // launch_list_gather unstructured owner groups with `cols`, their column table.
 cudaError_t launch_gather(const gtile* tiles, int ntiles, cudaStream_t stream);
-cudaError_t launch_list_gather(const gtile* tiles, int ntiles, const uint64_t* cols, cudaStream_t stream);
+// `blocks` (nullptr: none): k_gblock_entries column-table entries per tile, the tile's slice of
+// `cols`, loaded by its CTA beside the record; used by the tiles whose record flags it (pad[0]).
+constexpr int k_gblock_entries = 96;
+cudaError_t launch_list_gather(const gtile* tiles, int ntiles, const uint64_t* cols, const uint64_t* blocks,
+    cudaStream_t stream);
 } // namespace ghexb

@@ -1167,6 +1167,7 @@ void relocate_tiles(ghexb_plan_s& plan, const relocator& R)
             if (g.img[k].ptr) R(g.img[k].ptr);
     }
     for (auto& c : plan.lcols) R(c);
+    for (auto& c : plan.gblk) R(c);
 }
 
 } // namespace
@@ -1181,6 +1182,7 @@ void check_relocation(ghexb_plan_s& plan)
     if (!R.ok) return;
     ghexb_plan_s copy;
     copy.xf = plan.xf, copy.xp = plan.xp, copy.xb = plan.xb, copy.xpair = plan.xpair, copy.gt = plan.gt, copy.lcols = plan.lcols;
+    copy.gblk = plan.gblk;
     relocate_tiles(copy, R);
     const auto old_data = plan.fields;
     const auto old_boxes = plan.boxes;
@@ -1201,7 +1203,8 @@ void check_relocation(ghexb_plan_s& plan)
         return a.size() == b.size() && (a.empty() || std::memcmp(a.data(), b.data(), a.size() * sizeof(a[0])) == 0);
     };
     const bool equal = same(copy.xf, plan.xf) && same(copy.xp, plan.xp) && same(copy.xb, plan.xb) &&
-                       same(copy.xpair, plan.xpair) && same(copy.gt, plan.gt) && same(copy.lcols, plan.lcols);
+                       same(copy.xpair, plan.xpair) && same(copy.gt, plan.gt) && same(copy.lcols, plan.lcols) &&
+                       same(copy.gblk, plan.gblk);
     plan.fields = old_data, plan.boxes = old_boxes, plan.lists = old_lists;
     build_tiles(plan, plan.idx.data());
     if (!equal) throw error(GHEXB_ERR_INTERNAL, "moved tile tables differ from the tables built at the new address");
@@ -1437,6 +1440,20 @@ int64_t check_tables(ghexb_plan_s& plan)
                     throw error(GHEXB_ERR_INTERNAL, "adjoint tile outside the column table");
             }
         if (covered != levels) throw error(GHEXB_ERR_INTERNAL, "adjoint tiles do not cover every owner level");
+        // column blocks: the flagged tiles' blocks hold their slices of the column table
+        if (plan.gblk.size() != (plan.gt.size() - (size_t)plan.gt_boxes) * k_gblock_entries)
+            throw error(GHEXB_ERR_INTERNAL, "column blocks do not match the gather tiles");
+        for (size_t i = (size_t)plan.gt_boxes; i < plan.gt.size(); ++i)
+        {
+            const auto& t = plan.gt[i];
+            if (!t.pad[0]) continue;
+            const uint64_t per = (uint64_t)t.nimg + 1, j0 = t.e0 / t.n0, j1 = (t.e0 + t.count - 1) / t.n0;
+            if ((j1 - j0 + 1) * per > (uint64_t)k_gblock_entries) throw error(GHEXB_ERR_INTERNAL, "column block overflow");
+            for (uint64_t j = j0; j <= j1; ++j)
+                for (uint64_t c = 0; c < per; ++c)
+                    if (plan.gblk[(i - plan.gt_boxes) * k_gblock_entries + (j - j0) * per + c] != plan.lcols[t.col0 + j * per + c])
+                        throw error(GHEXB_ERR_INTERNAL, "column block differs from the column table");
+        }
         checked += (int64_t)images.size();
     }
     // phased adjoint lists
@@ -1506,6 +1523,7 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
     ensure(plan.d_xb, plan.cap_xb, plan.xb.size());
     ensure(plan.d_gt, plan.cap_gt, plan.gt.size());
     ensure(plan.d_lcols, plan.cap_lcols, plan.lcols.size());
+    ensure(plan.d_gblk, plan.cap_gblk, plan.gblk.size());
     ensure(plan.d_smaps, plan.cap_smaps, plan.smaps.size());
     ensure(plan.d_sitems, plan.cap_sitems, plan.sitems.size());
     ensure(plan.d_xf_blk, plan.cap_xf_blk, plan.xf_blk.size());
@@ -1520,6 +1538,7 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
     st.put(plan.d_xb, plan.xb);
     st.put(plan.d_gt, plan.gt);
     st.put(plan.d_lcols, plan.lcols);
+    st.put(plan.d_gblk, plan.gblk);
     st.put(plan.d_smaps, plan.smaps);
     st.put(plan.d_sitems, plan.sitems);
     if (!plan.sitems.empty() && !plan.d_status)
@@ -1797,6 +1816,20 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
             a = b;
         }
     }
+    // column blocks of the unstructured gather tiles: a tile's slice of the column table, which
+    // its CTA loads beside the record instead of after it (one dependent round trip fewer)
+    plan.gblk.assign((plan.gt.size() - (size_t)plan.gt_boxes) * k_gblock_entries, 0);
+    for (size_t i = (size_t)plan.gt_boxes; i < plan.gt.size(); ++i)
+    {
+        auto& t = plan.gt[i];
+        const uint64_t per = (uint64_t)t.nimg + 1;
+        const uint64_t first = t.col0 + (uint64_t)(t.e0 / t.n0) * per;
+        const uint64_t n = ((uint64_t)(t.e0 + t.count - 1) / t.n0 - t.e0 / t.n0 + 1) * per;
+        t.pad[0] = n <= (uint64_t)k_gblock_entries ? 1 : 0;
+        if (t.pad[0])
+            std::copy(plan.lcols.begin() + (int64_t)first, plan.lcols.begin() + (int64_t)(first + n),
+                plan.gblk.begin() + (int64_t)(i - plan.gt_boxes) * k_gblock_entries);
+    }
 
     // ---- phased adjoint kernels (boxes without a gather form, lists without one)
     auto box_rows = [&](int i) { return (int64_t)plan.boxes[i].n1 * plan.boxes[i].n2; };
@@ -1914,7 +1947,8 @@ namespace
 void adjoint_launches(ghexb_plan_s& plan, cudaStream_t stream)
 {
     check_cuda(launch_gather(plan.d_gt, plan.gt_boxes, stream), "adjoint kernel launch");
-    check_cuda(launch_list_gather(plan.d_gt + plan.gt_boxes, (int)plan.gt.size() - plan.gt_boxes, plan.d_lcols, stream),
+    check_cuda(launch_list_gather(plan.d_gt + plan.gt_boxes, (int)plan.gt.size() - plan.gt_boxes, plan.d_lcols,
+                   plan.gblk.empty() ? nullptr : plan.d_gblk, stream),
         "adjoint kernel launch");
     const int sms = plan.ctx ? plan.ctx->num_sms : 148;
     auto grid = [&](int n) { return std::min(n, 4 * sms); };
@@ -2042,6 +2076,7 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
     st.put(plan.d_xf, plan.xf);
     st.put(plan.d_gt, plan.gt);
     st.put(plan.d_lcols, plan.lcols);
+    st.put(plan.d_gblk, plan.gblk);
     st.put(plan.d_boxes, plan.boxes);
     st.put(plan.d_lists, plan.lists);
     st.put(plan.d_adj_lists, plan.adj_lists);
@@ -2276,7 +2311,8 @@ ghexb_plan_s::~ghexb_plan_s()
     }
     if (fork_event) cudaEventDestroy(fork_event);
     if (join_event) cudaEventDestroy(join_event);
-    for (void* p : {(void*)d_smaps, (void*)d_sitems, (void*)d_status, (void*)d_xf_blk, (void*)d_xp_blk, (void*)d_xb_blk})
+    for (void* p : {(void*)d_smaps, (void*)d_sitems, (void*)d_status, (void*)d_xf_blk, (void*)d_xp_blk, (void*)d_xb_blk,
+             (void*)d_gblk})
         if (p) cudaFree(p);
     for (void* p : {(void*)d_boxes, (void*)d_lists, (void*)d_adj_lists, (void*)d_idx, (void*)d_xf, (void*)d_xp,
              (void*)d_xb, (void*)d_gt, (void*)d_lcols, (void*)d_adj_btiles, (void*)d_adj_ltiles, (void*)d_counters})

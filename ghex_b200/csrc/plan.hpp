@@ -81,6 +81,11 @@ struct ghexb_plan_s
     bool list_gather_ok = false;
     std::vector<list_owner> lowners;
     std::vector<uint64_t> lcols; // column table of the owner groups (addresses of the columns)
+    // per unstructured gather tile (after the gt_boxes box cells): its slice of lcols in a block
+    // of k_gblock_entries, flagged in the tile's pad[0] when the slice fits
+    std::vector<uint64_t> gblk;
+    uint64_t* d_gblk = nullptr;
+    size_t cap_gblk = 0;
     std::vector<ghexb::gtile> gt; // box cells first (gt_boxes of them), then unstructured owner groups
     int gt_boxes = 0;
     // adjoint tiles of the phased kernels (boxes when !gather_ok, lists) grouped by phase
