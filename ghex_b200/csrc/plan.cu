@@ -1971,6 +1971,12 @@ void adjoint_launches(ghexb_plan_s& plan, cudaStream_t stream)
 void adjoint_plan(ghexb_plan_s& plan, cudaStream_t stream)
 {
     if (!plan.adjoint_ok) throw error(GHEXB_ERR_INVALID, plan.adjoint_reason);
+    // one kernel is launched as it is, as the forward's (a one-node graph was never faster)
+    if (plan.adjoint_launches() == 1)
+    {
+        adjoint_launches(plan, stream);
+        return;
+    }
     if (!plan.adj_exec)
     {
         check_cuda(cudaStreamBeginCapture(plan.cap_stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
