@@ -2,7 +2,8 @@
 fields mapped into the other through CUDA IPC. The processes meet at host barriers (gloo) around
 every exchange, so no kernel waits on another process's kernel. Pull and push forms, the push
 form's adjoint, an autotuned plan and the communication object are bit-exact against the oracle's
-single-process exchange."""
+single-process exchange, on a regular grid and on the cubed sphere (vector components negated
+across rotated edges, some of them between the processes)."""
 from __future__ import annotations
 
 import os
@@ -61,6 +62,49 @@ def _oracle_regular(w, grads=None):
                 O.adjoint(pat, doms, arrays, [w.offsets(spec)] * len(doms))
             for i, a in enumerate(arrays):
                 out[(spec.name, i)] = a
+    return out
+
+
+def _cubed(ctx, rank, world, dev):
+    """The cubed sphere at 48 x 48 x 8 per tile, 2 x 2 domains per tile dealt round-robin: a scalar
+    and a vector field (components negated across rotated edges)."""
+    from ghex_b200 import distributed as D
+    from ghex_b200 import workloads as W
+    from ghex_b200.structured import cubed_sphere as CS
+    from gpu_helpers import to_device
+    w = W.config3(edge=48, levels=8, split=2)
+    mine = [i for i in range(len(w.domains)) if i % world == rank]
+    cube = CS.cube(w.edge, w.levels)
+    pat = D.make_pattern(ctx, CS.HaloGenerator(w.halo), [CS.DomainDescriptor(cube, *w.domains[i]) for i in mine])
+    host, tens, bis, keep = [], [], [], [pat]
+    for name, nc, isv, seed in (("s", 1, False, 1), ("v", 2, True, 2)):
+        for i in mine:
+            a = w.domain_array(w.domains[i], nc, seed)
+            t = to_device(a, dev)
+            fd = CS.make_field_descriptor(CS.DomainDescriptor(cube, *w.domains[i]), t, w.offsets(), a.shape[:3], nc, isv)
+            keep.append(fd)
+            host.append((name, i, a))
+            tens.append(t)
+            bis.append(pat(fd))
+    return w, host, tens, bis, keep
+
+
+def _oracle_cubed(w, grads=None):
+    """Single-process oracle over the domains in id order (the order of a distributed pattern)."""
+    from oracle import cubed_sphere as O
+    order = sorted(range(len(w.domains)), key=lambda i: (w.domains[i][0], (w.domains[i][1], w.domains[i][3])))
+    odoms = [O.Domain(t, (x0, x1), (y0, y1), w.levels) for t, x0, x1, y0, y1 in (w.domains[i] for i in order)]
+    pat = O.make_pattern(w.edge, (w.halo,) * 4, odoms)
+    out = {}
+    for name, nc, isv, seed in (("s", 1, False, 1), ("v", 2, True, 2)):
+        if grads is None:
+            arrays = [w.domain_array(w.domains[i], nc, seed) for i in order]
+            O.exchange(pat, odoms, arrays, [w.offsets()] * len(odoms), w.edge, isv)
+        else:
+            arrays = [grads[(name, i)].copy(order="K") for i in order]
+            O.adjoint(pat, odoms, arrays, [w.offsets()] * len(odoms), w.edge, isv)
+        for i, a in zip(order, arrays):
+            out[(name, i)] = a
     return out
 
 
@@ -135,6 +179,27 @@ def _rank(rank: int, world: int, port: int, out):
         pull_again.release()
         push.release()
 
+        # the cubed sphere: pull and push forms, and the push form's adjoint
+        cw, chost, ctens, cbis, ckeep = _cubed(ctx, rank, world, dev)
+        cexp = _oracle_cubed(cw)
+        for mode in ("pull", "push"):
+            _reset(chost, ctens)
+            plan = D.make_sharded_plan(ctx, cbis, mode)
+            plan.exchange()
+            res[f"cubed_{mode}"] = _mismatches(chost, ctens, cexp)
+            if mode == "push":
+                crng = np.random.default_rng(5)
+                # every rank draws every domain's gradient in the same order
+                allg = {}
+                for name, nc, seed in (("s", 1, 1), ("v", 2, 2)):
+                    for i, d in enumerate(cw.domains):
+                        shape = cw.domain_array(d, nc, seed).shape
+                        allg[(name, i)] = np.asfortranarray(crng.standard_normal(shape))
+                _reset(chost, ctens, allg)
+                plan.adjoint()
+                res["cubed_adjoint"] = _mismatches(chost, ctens, _oracle_cubed(cw, allg))
+            plan.release()
+
         _reset(host, tens)
         co = D.make_communication_object(ctx)
         co.exchange(bis).wait()
@@ -175,7 +240,8 @@ def test_sharded_exchange_two_processes_one_gpu(cuda):
     for r in (0, 1):
         res = got[r]
         assert res["pull_halo_elements"] > 0
-        for k in ("pull", "pull_autotuned", "push", "adjoint", "co", "co_cached"):
+        for k in ("pull", "pull_autotuned", "push", "adjoint", "co", "co_cached", "cubed_pull", "cubed_push",
+                  "cubed_adjoint"):
             assert res[k] == 0, (r, k, res[k])
         assert res["pull_adjoint_refused"]
         assert res["co_plans"] == 1
