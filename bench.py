@@ -66,6 +66,10 @@ def parse():
     ap.add_argument("--calibrate", action="store_true",
                     help="time a plain row-copy kernel on the exchange's access pattern (rows of n elements at a row "
                          "stride) and contiguous copies, cold L2, and print one JSON line")
+    ap.add_argument("--sharded", choices=["pull", "push"], default=None,
+                    help="cfg1 sharded over the ranks (one per GPU, domains dealt round-robin): each rank's "
+                         "kernel moves its part of the exchange through the other GPUs' memory, between two "
+                         "NCCL barriers on the exchange's stream (ghex_b200.distributed); total work fixed")
     ap.add_argument("--staged-ab", action="store_true",
                     help="time the staged (tensor-map) form against the element kernel on cfg1, cfg3 and cfg4")
     ap.add_argument("--calibrate-host", action="store_true",
@@ -879,8 +883,107 @@ def staged_ab(args):
     print(json.dumps(out), flush=True)
 
 
+def run_sharded(args) -> None:
+    """cfg1 sharded over the ranks: every rank holds the fields of its domains only; one step is a
+    sharded exchange (NCCL barrier, this rank's kernel, NCCL barrier), timed with CUDA events on the
+    exchange's stream after a cold-L2 read, max over ranks. Without torchrun it runs as one rank
+    (every domain local, the barriers trivial)."""
+    import datetime
+    import socket
+    import torch
+    import torch.distributed as dist
+    from ghex_b200 import distributed as D
+    from ghex_b200.structured import regular as R
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world == 1 and "MASTER_PORT" not in os.environ:
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(sk.getsockname()[1]), RANK="0", WORLD_SIZE="1")
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    w = workload(args.config if args.config in ("cfg0", "cfg1", "cfg4") else "cfg1")
+    mine = [i for i in range(len(w.domains)) if i % world == rank]
+    ctx = D.make_context(device=local)
+    bis, keep, local_fields = [], [], []
+    for halos, specs in w.halo_groups().items():
+        hg = R.HaloGenerator(((0,) * w.dim, tuple(n - 1 for n in w.shape)),
+                             [(halos[2 * k], halos[2 * k + 1]) for k in range(w.dim)], w.periodic)
+        doms = {i: R.DomainDescriptor(i, (f, l)) for i, f, l in w.domains}
+        pat = D.make_pattern(ctx, hg, [doms[i] for i in mine])
+        keep.append(pat)
+        for spec in specs:
+            for i in mine:
+                a = w.domain_array(w.domains[i], spec)
+                t = torch.from_numpy(a).to(dev)
+                fd = R.make_field_descriptor(doms[i], t, w.offsets(spec), w.extents(w.domains[i], spec))
+                keep.append(fd)
+                local_fields.append((spec.name, i, a, t))
+                bis.append(pat(fd))
+    stream = torch.cuda.Stream(device=dev)
+    s = stream.cuda_stream
+    plan = D.make_sharded_plan(ctx, bis, args.sharded)
+    tuning = plan.info() if args.no_autotune else plan.autotune(repeats=10, stream=s)
+    l2 = torch.cuda.get_device_properties(dev).L2_cache_size
+    flush = torch.ones(max(2 * l2, 64 << 20) // 4, dtype=torch.float32, device=dev)
+    timer = Timer(stream, flush, world, dev)
+    sampler = ClockSampler(dev.index)
+    with sampler:
+        ms = timer(lambda: plan.exchange(s), args.steps, max(3, args.warmup))
+    clocks = sampler.summary()
+    # the whole exchange's bytes: every rank's part
+    part = torch.tensor([plan.info()["algorithmic_bytes"]], dtype=torch.float64, device=dev)
+    dist.all_reduce(part)
+    alg = int(part.item())
+    # bit-exact against GHEX's CPU exchange (or the numpy restatement) of every domain
+    for name, i, a, t in local_fields:
+        t.copy_(torch.from_numpy(a))
+    torch.cuda.synchronize()
+    plan.exchange(s)
+    torch.cuda.synchronize()
+    from oracle import regular as O
+    bad = 0
+    for halos, specs in w.halo_groups().items():
+        odoms = [O.Domain(i, f, l) for i, f, l in w.domains]
+        opat = O.make_pattern((0,) * w.dim, tuple(n - 1 for n in w.shape), halos, w.periodic, odoms)
+        for spec in specs:
+            arrays = [w.domain_array(d, spec) for d in w.domains]
+            O.exchange(opat, odoms, arrays, [w.offsets(spec)] * len(odoms))
+            for name, i, a, t in local_fields:
+                if name == spec.name:
+                    e = arrays[i]
+                    u = np.dtype(f"u{e.itemsize}")
+                    bad += int(np.count_nonzero(np.ascontiguousarray(t.cpu().numpy()).view(u) != np.ascontiguousarray(e).view(u)))
+    bad_t = torch.tensor([bad], dtype=torch.float64, device=dev)
+    dist.all_reduce(bad_t)
+    peak, peak_kind = peaks()
+    line = {"metric": METRIC, "value": alg / (ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic (seeded splitmix64 interiors, NaN halos)",
+            "config": {"workload": w.name, "form": f"sharded exchange, {args.sharded} form: NCCL barrier, one kernel "
+                       "per rank through mapped peer memory, NCCL barrier",
+                       "domains": len(w.domains), "algorithmic_bytes_per_exchange": alg,
+                       "l2": "cold: a read of twice the L2 size before every timed exchange, outside its events",
+                       "parallelism": f"sharded x{world}", "tuning": {k: tuning[k] for k in TUNING_KEYS}},
+            "exchanges_per_s": 1e3 / ms, "bitexact": int(bad_t.item()) == 0, "clocks": clocks,
+            "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9 / world, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (ms * 1e-3) / 1e9 / world / peak, "peak_source": peak_kind,
+                         "per": "GPU (the whole exchange's bytes over the GPUs)"}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.release()
+    del keep
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def main():
     args = parse()
+    if args.sharded:
+        run_sharded(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
@@ -955,7 +1058,7 @@ def main():
         "metric": METRIC, "value": world * achieved, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_batched, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": case.dtype, "data": "synthetic (seeded splitmix64 interiors, NaN halos)",
-        "config": {"workload": case.w.name, "form": "batched kernel, CUDA graph", "domains": len(case.w.domains),
+        "config": {"workload": case.w.name, "form": "batched kernel, one launch", "domains": len(case.w.domains),
                    "algorithmic_bytes_per_exchange": alg,
                    "l2": "cold: a read of an unrelated buffer of twice the L2 size before every timed exchange, "
                          "outside its events",
