@@ -99,3 +99,37 @@ def test_ghex_module_names():
                      "make_bulk_communication_object", "make_exchange_plan"):
             assert callable(getattr(mod, name)), (mod.__name__, name)
     assert callable(regular.make_staged_pattern) and callable(unstructured.make_communication_object_ipr)
+
+
+def test_sharded_and_ipc_argument_checks():
+    """Sharded plans and IPC mappings refuse bad arguments before any device call."""
+    import sys
+    sys.path.insert(0, str(Path(__file__).resolve().parent))
+    from test_plan_check import regular_handles
+    from ghex_b200 import workloads as W
+    ctx, keep, handles = regular_handles(W.config0())
+    arr = (C.c_void_p * len(handles))(*handles)
+    n = C.c_int64()
+    local = bytes([1] * len(handles))
+    # mode outside 1 (pull) and 2 (push)
+    assert _capi.lib.ghexb_plan_check_sharded(ctx._h, arr, len(handles), local, 3, C.byref(n)) == _capi.ERR_INVALID
+    assert "pull" in _capi.last_error()
+    # locality flags are required
+    assert _capi.lib.ghexb_plan_check_sharded(ctx._h, arr, len(handles), None, 1, C.byref(n)) == _capi.ERR_INVALID
+    # every field local: the pull and push parts are the whole exchange
+    _capi.call("ghexb_plan_check_sharded", ctx._h, arr, len(handles), local, 1, C.byref(n))
+    pull = n.value
+    _capi.call("ghexb_plan_check_sharded", ctx._h, arr, len(handles), local, 2, C.byref(n))
+    assert n.value == pull == 52288  # the written halo cells of the 64^3, 2x2x2, halo-1 workload
+    # no field local: an empty part
+    _capi.call("ghexb_plan_check_sharded", ctx._h, arr, len(handles), bytes(len(handles)), 1, C.byref(n))
+    assert n.value == 0
+    # a handle never opened here
+    assert _capi.lib.ghexb_ipc_close(bytes(_capi.IPC_HANDLE_BYTES)) == _capi.ERR_INVALID
+    assert "not open" in _capi.last_error()
+    p = C.c_void_p()
+    assert _capi.lib.ghexb_ipc_open(bytes(_capi.IPC_HANDLE_BYTES), -1, C.byref(p)) == _capi.ERR_INVALID
+
+
+def test_adjoint_tuning_range():
+    assert _capi.lib.ghexb_plan_set_adjoint_tuning(None, 0) == _capi.ERR_INVALID
