@@ -1058,7 +1058,7 @@ def main():
         "metric": METRIC, "value": world * achieved, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_batched, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": case.dtype, "data": "synthetic (seeded splitmix64 interiors, NaN halos)",
-        "config": {"workload": case.w.name, "form": "batched kernel, one launch", "domains": len(case.w.domains),
+        "config": {"workload": case.w.name, "form": "batched kernel, CUDA graph", "domains": len(case.w.domains),
                    "algorithmic_bytes_per_exchange": alg,
                    "l2": "cold: a read of an unrelated buffer of twice the L2 size before every timed exchange, "
                          "outside its events",

@@ -1908,13 +1908,6 @@ void launch_plan(ghexb_plan_s& plan, int form, cudaStream_t stream)
 
 void graph_launch_plan(ghexb_plan_s& plan, cudaStream_t stream)
 {
-    // A batched form of one kernel is launched as it is: from a cold L2 a one-node graph was
-    // never faster, and 1.3 us slower on an unstructured plan (12.8 against 14.2 us).
-    if (plan.sitems.empty())
-    {
-        launch_plan(plan, GHEXB_FORM_BATCHED, stream);
-        return;
-    }
     if (!plan.exec)
     {
         check_cuda(cudaStreamBeginCapture(plan.cap_stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
@@ -1971,7 +1964,7 @@ void adjoint_launches(ghexb_plan_s& plan, cudaStream_t stream)
 void adjoint_plan(ghexb_plan_s& plan, cudaStream_t stream)
 {
     if (!plan.adjoint_ok) throw error(GHEXB_ERR_INVALID, plan.adjoint_reason);
-    // one kernel is launched as it is, as the forward's (a one-node graph was never faster)
+    // one kernel is launched as it is (a one-node graph was never faster than the kernel alone)
     if (plan.adjoint_launches() == 1)
     {
         adjoint_launches(plan, stream);

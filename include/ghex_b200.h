@@ -311,9 +311,7 @@ int ghexb_plan_set_adjoint_tuning(ghexb_plan plan, int gather_scale);
 int ghexb_plan_staged_status(ghexb_plan plan, unsigned* status);
 /* One forward exchange in the given form, stream-ordered. */
 int ghexb_plan_launch(ghexb_plan plan, int form, void* stream);
-/* The batched form on `stream`: captured once into a CUDA graph and replayed when it holds more
- * than one launch (the staged kernel beside the element kernel), else its one kernel launched
- * directly. */
+/* The batched form captured once into a CUDA graph and replayed on `stream`. */
 int ghexb_plan_graph_launch(ghexb_plan plan, void* stream);
 /* Adjoint of the exchange: every halo value is added into the interior value it was copied
  * from (negated where the forward negated it), in a fixed order, then the halo is zeroed.
