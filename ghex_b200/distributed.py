@@ -56,6 +56,8 @@ class context(_core.context):
     a gloo group over the same ranks, made collectively here)."""
 
     def __init__(self, group: Any = None, device: int | None = None):
+        # every process of the default group makes its context at the same point: with an NCCL
+        # group the gloo group of the host collectives is made here, collectively
         super().__init__(None, False, device)
         dist = _dist()
         if not dist.is_initialized():
@@ -85,6 +87,17 @@ class context(_core.context):
 
     def host_barrier(self) -> None:
         _dist().barrier(group=self.host_group)
+
+    def agree(self, error: BaseException | None) -> None:
+        """Collective: raises on every process when any process passes an error, so that a
+        failure on one process never leaves the others waiting in a later collective."""
+        errors = self.all_gather(None if error is None else f"{type(error).__name__}: {error}")
+        bad = [(r, e) for r, e in enumerate(errors) if e is not None]
+        if bad:
+            if error is not None:
+                raise error
+            r, e = bad[0]
+            raise RuntimeError(f"rank {r} failed: {e}")
 
 
 def make_context(group: Any = None, device: int | None = None) -> context:
@@ -190,7 +203,13 @@ class _FieldSet:
         self.context = ctx
         self._remote: list[C.c_void_p] = []
         self._opened: list[bytes] = []
-        everyone = ctx.all_gather(_local_meta(ctx, bis, share))
+        meta, err = None, None
+        try:
+            meta = _local_meta(ctx, bis, share)
+        except Exception as e:  # reported to every process below
+            err = e
+        everyone = ctx.all_gather(meta)
+        ctx.agree(err)
         handles, local = [], []
         try:
             for r, part in enumerate(everyone):
@@ -208,9 +227,11 @@ class _FieldSet:
                     self._remote.append(h)
                     handles.append(h)
                     local.append(0)
-        except Exception:
+        except Exception as e:
+            err = e
+        if err is not None:
             self.release()
-            raise
+        ctx.agree(err)
         self.n = len(handles)
         self.handles = (C.c_void_p * self.n)(*handles)
         self.local = bytes(local)
@@ -257,13 +278,22 @@ class ShardedPlan:
         self._arrays = [a for bi in self._bis for a in bi.arrays()]
         self._fields = _FieldSet(ctx, self._bis, share=True)
         h = C.c_void_p()
+        err = None
         try:
             call("ghexb_plan_create_sharded", ctx._h, self._fields.handles, self._fields.n, self._fields.local,
                  self.mode, C.byref(h))
-        except Exception:
+        except Exception as e:  # every process learns of it, then raises
+            err = e
+        if err is not None:
             self._fields.release()
+        else:
+            self._h = h
+        try:
+            ctx.agree(err)
+        except Exception:
+            if err is None:
+                self.release()
             raise
-        self._h = h
         self._token = torch.zeros(1, device=torch.device("cuda", ctx.device)) if ctx.device_barriers else None
         # no process leaves the collective build (and changes its fields) while another still
         # builds: a plan build uploads tables and may autotune

@@ -155,7 +155,22 @@ def _rank(rank: int, world: int, port: int, out):
             refused = False
         except ValueError as e:
             refused = "belongs to rank" in str(e)
-        out.put((rank, res, refused))
+        # a failure on one rank reaches every rank: rank 1 passes a field of a pattern that is not
+        # distributed, and both ranks raise instead of waiting on each other
+        bis, keep, _, _ = regular_case(ctx, rank, world)
+        if rank == 1:
+            plain = R.make_pattern(ctx, hg, [R.DomainDescriptor(i, (f, l)) for i, f, l in w.domains])
+            g, _ = _fake_regular(R, w.domains[1], 1 << 41, spec, w)
+            keep += [plain, g]
+            bis = bis + [plain(g)]
+        try:
+            D.check_sharded(ctx, bis, "pull")
+            failure = None
+        except ValueError as e:
+            failure = ("ValueError", "distributed.make_pattern" in str(e))
+        except RuntimeError as e:
+            failure = ("RuntimeError", "rank 1 failed" in str(e))
+        out.put((rank, res, refused and failure is not None and failure[1], ))
     finally:
         dist.destroy_process_group()
 
@@ -171,6 +186,7 @@ def test_sharded_parts_partition_the_exchange():
     for p in ps:
         p.start()
     res = dict((r, (v, refused)) for r, v, refused in (q.get(timeout=300) for _ in ps))
+    # (refused also holds: a failure on rank 1 raised on both ranks)
     for p in ps:
         p.join(timeout=60)
         assert p.exitcode == 0
