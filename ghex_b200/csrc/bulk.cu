@@ -1,0 +1,54 @@
+// Bulk column kernel (bulk.hpp): one warp per tile; lane 0 arms the tile's mbarrier with the
+// tile's bytes, every lane issues the bulk loads of its columns (lane, lane + 32) into the shared
+// stage, all wait for the barrier (bounded in time), then every lane issues the bulk stores of its
+// columns and waits until the copy engine has read them out of shared memory.
+#include "async_copy.hpp"
+#include "bulk.hpp"
+
+namespace ghexb
+{
+namespace
+{
+__global__ void __launch_bounds__(32) bulk_kernel(const btile* __restrict__ tiles, const int32_t* __restrict__ blocks,
+    unsigned* status)
+{
+    __shared__ __align__(128) unsigned char stage[k_bulk_stage];
+    __shared__ __align__(16) btile t;
+    __shared__ __align__(16) int32_t blk[k_bulk_block_ints];
+    __shared__ __align__(8) uint64_t bar;
+    const unsigned lane = threadIdx.x;
+    // the record (three 16-byte words) and the index block (32 words), one round trip
+    if (lane < 3) reinterpret_cast<uint4*>(&t)[lane] = __ldg(reinterpret_cast<const uint4*>(tiles + blockIdx.x) + lane);
+    reinterpret_cast<int4*>(blk)[lane] = __ldg(reinterpret_cast<const int4*>(blocks + (size_t)blockIdx.x * k_bulk_block_ints) + lane);
+    if (lane == 0)
+    {
+        mbar_init(&bar, 1);
+        mbar_init_fence();
+    }
+    __syncwarp();
+    const uint32_t n = t.ncols, cb = t.col_bytes;
+    if (lane == 0) mbar_expect_tx(&bar, n * cb);
+    __syncwarp();
+    for (uint32_t c = lane; c < n; c += 32) bulk_load(stage + c * cb, t.src + (int64_t)blk[c] * t.s_is, cb, &bar);
+    if (!mbar_wait(&bar, 0))
+    {
+        // the loads did not complete in time: the tile's columns are not stored; the CTA waits
+        // (again bounded) for its loads, which write into its shared memory, before it ends
+        if (lane == 0 && status) atomicOr(status, 1u);
+        (void)mbar_wait(&bar, 0);
+        return;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    for (uint32_t c = lane; c < n; c += 32) bulk_store(t.dst + (int64_t)blk[k_bulk_columns + c] * t.d_is, stage + c * cb, cb);
+    bulk_commit();
+    bulk_wait_read();
+}
+} // namespace
+
+cudaError_t launch_bulk(const btile* tiles, const int32_t* blocks, int ntiles, unsigned* status, cudaStream_t stream)
+{
+    if (ntiles <= 0) return cudaSuccess;
+    bulk_kernel<<<ntiles, 32, 0, stream>>>(tiles, blocks, status);
+    return cudaGetLastError();
+}
+} // namespace ghexb

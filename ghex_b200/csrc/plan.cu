@@ -1168,6 +1168,7 @@ void relocate_tiles(ghexb_plan_s& plan, const relocator& R)
     }
     for (auto& c : plan.lcols) R(c);
     for (auto& c : plan.gblk) R(c);
+    for (auto& t : plan.bt) R(t.src), R(t.dst);
 }
 
 } // namespace
@@ -1182,7 +1183,7 @@ void check_relocation(ghexb_plan_s& plan)
     if (!R.ok) return;
     ghexb_plan_s copy;
     copy.xf = plan.xf, copy.xp = plan.xp, copy.xb = plan.xb, copy.xpair = plan.xpair, copy.gt = plan.gt, copy.lcols = plan.lcols;
-    copy.gblk = plan.gblk;
+    copy.gblk = plan.gblk, copy.bt = plan.bt;
     relocate_tiles(copy, R);
     const auto old_data = plan.fields;
     const auto old_boxes = plan.boxes;
@@ -1204,7 +1205,7 @@ void check_relocation(ghexb_plan_s& plan)
     };
     const bool equal = same(copy.xf, plan.xf) && same(copy.xp, plan.xp) && same(copy.xb, plan.xb) &&
                        same(copy.xpair, plan.xpair) && same(copy.gt, plan.gt) && same(copy.lcols, plan.lcols) &&
-                       same(copy.gblk, plan.gblk);
+                       same(copy.gblk, plan.gblk) && same(copy.bt, plan.bt);
     plan.fields = old_data, plan.boxes = old_boxes, plan.lists = old_lists;
     build_tiles(plan, plan.idx.data());
     if (!equal) throw error(GHEXB_ERR_INTERNAL, "moved tile tables differ from the tables built at the new address");
@@ -1337,7 +1338,45 @@ int64_t check_tables(ghexb_plan_s& plan)
     check_blocks(plan.xb, plan.xb_blk);
     const int64_t ns = check_staged(plan);
     checked += ns;
-    if (nf + ns != nb || np != nb) throw error(GHEXB_ERR_INTERNAL, "batched, per-field and per-box tables differ");
+    // bulk column tiles: every column inside its fields, 16-byte aligned, its indices as the list
+    // holds them; the lists they take have no element tiles in the batched table
+    int64_t nbulk = 0;
+    if (plan.bt_blk.size() != plan.bt.size() * k_bulk_block_ints || plan.bt_list.size() != plan.bt.size())
+        throw error(GHEXB_ERR_INTERNAL, "bulk tiles and their index blocks differ in number");
+    for (size_t u = 0; u < plan.bt.size(); ++u)
+    {
+        const auto& t = plan.bt[u];
+        const int i = plan.bt_list[u];
+        const auto& l = plan.lists[i];
+        const auto& sf = plan.fields[plan.list_src_slot[i]];
+        const auto& df = plan.fields[plan.list_dst_slot[i]];
+        const int64_t sbytes = field_span(sf) * sf.esize, dbytes = field_span(df) * df.esize;
+        if (t.ncols == 0 || t.ncols > (uint32_t)k_bulk_columns || t.col_bytes % 16 || t.col_bytes != (uint32_t)l.levels * 16u ||
+            (int64_t)t.ncols * t.col_bytes > k_bulk_stage || t.src != l.src || t.dst != l.dst)
+            throw error(GHEXB_ERR_INTERNAL, "bulk tile out of shape");
+        const int32_t* S = plan.idx.data() + plan.list_idx_off[i];
+        for (uint32_t c = 0; c < t.ncols; ++c)
+        {
+            const int32_t col = plan.bt_col0[u] + (int32_t)c;
+            if (col >= l.count || plan.bt_blk[u * k_bulk_block_ints + c] != S[col] ||
+                plan.bt_blk[u * k_bulk_block_ints + k_bulk_columns + c] != S[l.count + col])
+                throw error(GHEXB_ERR_INTERNAL, "bulk index block differs from the list");
+            const int64_t so = (t.src - sf.data) + (int64_t)S[col] * t.s_is;
+            const int64_t dof = (t.dst - df.data) + (int64_t)S[l.count + col] * t.d_is;
+            if (so < 0 || so + t.col_bytes > sbytes || dof < 0 || dof + t.col_bytes > dbytes)
+                throw error(GHEXB_ERR_RANGE, "bulk column outside its field's memory");
+            if ((reinterpret_cast<uintptr_t>(sf.data) + (uint64_t)so) % 16 || (reinterpret_cast<uintptr_t>(df.data) + (uint64_t)dof) % 16)
+                throw error(GHEXB_ERR_INTERNAL, "bulk column not 16-byte aligned");
+        }
+        nbulk += (int64_t)t.ncols * l.levels;
+    }
+    for (const auto& t : plan.xf)
+        if (t.kind == 1)
+            for (size_t u = 0; u < plan.bt.size(); ++u)
+                if (t.src == plan.bt[u].src && t.dst == plan.bt[u].dst && t.sidx == plan.idx.data() + plan.list_idx_off[plan.bt_list[u]])
+                    throw error(GHEXB_ERR_INTERNAL, "a list is both in bulk and in element tiles");
+    checked += nbulk;
+    if (nf + ns + nbulk != nb || np != nb) throw error(GHEXB_ERR_INTERNAL, "batched, per-field and per-box tables differ");
     if (plan.gather_ok)
     {
         check_tiles(plan.gt, 0, (int)plan.gt.size(), class_of_g);
@@ -1524,6 +1563,8 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
     ensure(plan.d_gt, plan.cap_gt, plan.gt.size());
     ensure(plan.d_lcols, plan.cap_lcols, plan.lcols.size());
     ensure(plan.d_gblk, plan.cap_gblk, plan.gblk.size());
+    ensure(plan.d_bt, plan.cap_bt, plan.bt.size());
+    ensure(plan.d_bt_blk, plan.cap_bt_blk, plan.bt_blk.size());
     ensure(plan.d_smaps, plan.cap_smaps, plan.smaps.size());
     ensure(plan.d_sitems, plan.cap_sitems, plan.sitems.size());
     ensure(plan.d_xf_blk, plan.cap_xf_blk, plan.xf_blk.size());
@@ -1539,9 +1580,11 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
     st.put(plan.d_gt, plan.gt);
     st.put(plan.d_lcols, plan.lcols);
     st.put(plan.d_gblk, plan.gblk);
+    st.put(plan.d_bt, plan.bt);
+    st.put(plan.d_bt_blk, plan.bt_blk);
     st.put(plan.d_smaps, plan.smaps);
     st.put(plan.d_sitems, plan.sitems);
-    if (!plan.sitems.empty() && !plan.d_status)
+    if ((!plan.sitems.empty() || !plan.bt.empty()) && !plan.d_status)
     {
         check_cuda(cudaMalloc(&plan.d_status, sizeof(unsigned)), "cudaMalloc(staged status)");
         check_cuda(cudaMemsetAsync(plan.d_status, 0, sizeof(unsigned), stream), "cudaMemsetAsync(staged status)");
@@ -1719,7 +1762,41 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
             for (size_t p = 0; p < ptiles.size(); ++p)
                 if (!staged(plan.pairs[p].first) && !staged(plan.pairs[p].second))
                     all.insert(all.end(), ptiles[p].begin(), ptiles[p].end());
-        for (const auto& v : ltiles) all.insert(all.end(), v.begin(), v.end());
+        // lists in 16-byte units between device fields: bulk column tiles, else element tiles
+        plan.bt.clear(), plan.bt_blk.clear(), plan.bt_list.clear(), plan.bt_col0.clear();
+        auto on_device = [&](int slot) { return plan.field_on_device.empty() || plan.field_on_device[slot]; };
+        for (size_t i = 0; i < plan.lists.size(); ++i)
+        {
+            const auto& l = plan.lists[i];
+            const uint32_t cb = (uint32_t)l.levels * 16u;
+            if (!(plan.bulk_lists && l.unit == 16 && cb <= (uint32_t)k_bulk_stage && on_device(plan.list_src_slot[i]) &&
+                    on_device(plan.list_dst_slot[i])))
+            {
+                all.insert(all.end(), ltiles[i].begin(), ltiles[i].end());
+                continue;
+            }
+            const int32_t per = (int32_t)std::min<uint32_t>(k_bulk_columns, (uint32_t)k_bulk_stage / cb);
+            const int32_t* S = plan.idx.data() + plan.list_idx_off[i];
+            const int32_t* D = S + l.count;
+            for (int32_t c0 = 0; c0 < l.count; c0 += per)
+            {
+                btile t{};
+                t.src = l.src, t.dst = l.dst;
+                t.s_is = (int64_t)l.s_is * 16, t.d_is = (int64_t)l.d_is * 16;
+                t.ncols = (uint32_t)std::min(per, l.count - c0);
+                t.col_bytes = cb;
+                const size_t b = plan.bt_blk.size();
+                plan.bt_blk.resize(b + k_bulk_block_ints, 0);
+                for (uint32_t c = 0; c < t.ncols; ++c)
+                {
+                    plan.bt_blk[b + c] = S[c0 + c];
+                    plan.bt_blk[b + k_bulk_columns + c] = D[c0 + c];
+                }
+                plan.bt.push_back(t);
+                plan.bt_list.push_back((int)i);
+                plan.bt_col0.push_back(c0);
+            }
+        }
         auto per_elem = [](const xtile& t) { return tile_cost(t) / std::max<uint32_t>(1u, t.count); };
         std::stable_sort(all.begin(), all.end(), [&](const xtile& x, const xtile& y) { return per_elem(x) > per_elem(y); });
         plan.xf.clear();
@@ -1891,6 +1968,7 @@ void launch_plan(ghexb_plan_s& plan, int form, cudaStream_t stream)
     {
         case GHEXB_FORM_BATCHED:
             launch_staged_plan(plan, stream);
+            check_cuda(launch_bulk(plan.d_bt, plan.d_bt_blk, (int)plan.bt.size(), plan.d_status, stream), "bulk kernel launch");
             run(plan.d_xf, plan.xf_blk.empty() ? nullptr : plan.d_xf_blk, {0, (int)plan.xf.size()});
             if (!plan.sitems.empty())
                 check_cuda(cudaStreamWaitEvent(stream, plan.join_event, 0), "cudaStreamWaitEvent(join)");
@@ -2076,6 +2154,8 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
     st.put(plan.d_gt, plan.gt);
     st.put(plan.d_lcols, plan.lcols);
     st.put(plan.d_gblk, plan.gblk);
+    st.put(plan.d_bt, plan.bt);
+    st.put(plan.d_bt_blk, plan.bt_blk);
     st.put(plan.d_boxes, plan.boxes);
     st.put(plan.d_lists, plan.lists);
     st.put(plan.d_adj_lists, plan.adj_lists);
@@ -2311,7 +2391,7 @@ ghexb_plan_s::~ghexb_plan_s()
     if (fork_event) cudaEventDestroy(fork_event);
     if (join_event) cudaEventDestroy(join_event);
     for (void* p : {(void*)d_smaps, (void*)d_sitems, (void*)d_status, (void*)d_xf_blk, (void*)d_xp_blk, (void*)d_xb_blk,
-             (void*)d_gblk})
+             (void*)d_gblk, (void*)d_bt, (void*)d_bt_blk})
         if (p) cudaFree(p);
     for (void* p : {(void*)d_boxes, (void*)d_lists, (void*)d_adj_lists, (void*)d_idx, (void*)d_xf, (void*)d_xp,
              (void*)d_xb, (void*)d_gt, (void*)d_lcols, (void*)d_adj_btiles, (void*)d_adj_ltiles, (void*)d_counters})

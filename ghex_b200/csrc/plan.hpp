@@ -8,6 +8,7 @@
 #include <utility>
 #include <vector>
 
+#include "bulk.hpp"
 #include "core.hpp"
 #include "exchange.hpp"
 #include "staged.hpp"
@@ -52,6 +53,17 @@ struct ghexb_plan_s
     // k_block_ints each): the indices of the tile's columns, loaded beside its record. Empty
     // when the plan has no lists.
     std::vector<int32_t> xf_blk, xp_blk, xb_blk;
+    // Bulk column tiles of the batched form (bulk.hpp): the list descriptors in 16-byte units
+    // between device fields, when bulk_lists is set, move by the copy engine instead of the element
+    // kernel. bt_blk holds each tile's index block; bt_list and bt_col0 (host only) its list and
+    // first column.
+    bool bulk_lists = true;
+    std::vector<ghexb::btile> bt;
+    std::vector<int32_t> bt_blk;
+    std::vector<int> bt_list, bt_col0;
+    ghexb::btile* d_bt = nullptr;
+    int32_t* d_bt_blk = nullptr;
+    size_t cap_bt = 0, cap_bt_blk = 0;
     bool forms_stale = false; // xp and xb moved on the host by a rebind, not yet on the device
     int32_t *d_xf_blk = nullptr, *d_xp_blk = nullptr, *d_xb_blk = nullptr;
     size_t cap_xf_blk = 0, cap_xp_blk = 0, cap_xb_blk = 0;

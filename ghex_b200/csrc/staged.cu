@@ -14,6 +14,7 @@
 
 #include <mutex>
 
+#include "async_copy.hpp"
 #include "staged.hpp"
 
 namespace ghexb
@@ -22,55 +23,8 @@ namespace
 {
 constexpr int k_max_stages = 16;
 constexpr int k_max_consumers = 8;
-constexpr unsigned long long k_wait_ns = 1000000000ull; // bound of every wait
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ uint32_t fdiv(uint32_t n, uint32_t m, uint32_t l) { return (__umulhi(n, m) + n) >> l; }
-
-__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* b)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_poll(uint64_t* b, uint32_t parity)
-{
-    uint32_t done;
-    asm volatile("{\n\t.reg .pred p;\n\t"
-                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                 "selp.u32 %0, 1, 0, p;\n\t}"
-                 : "=r"(done)
-                 : "r"(smem_u32(b)), "r"(parity)
-                 : "memory");
-    return done != 0;
-}
-
-__device__ __forceinline__ unsigned long long global_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Waits for the phase of parity `parity` of *b to complete; false after about a second.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity)
-{
-    if (mbar_poll(b, parity)) return true;
-    const unsigned long long deadline = global_ns() + k_wait_ns;
-    while (global_ns() < deadline)
-        if (mbar_poll(b, parity)) return true;
-    return false;
-}
 
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar)
 {
