@@ -97,7 +97,7 @@ def peaks() -> tuple[float, str]:
 
 
 TUNING_KEYS = ("elems_per_thread", "block", "grid", "pairs", "use_pairs", "staged_mode", "staged_boxes", "staged_items",
-               "stages", "stage_bytes", "stage_consumers", "stage_ctas_per_sm")
+               "stages", "stage_bytes", "stage_consumers", "stage_ctas_per_sm", "bulk_share", "bulk_tiles")
 
 
 def tuning_key(info: dict) -> str:
@@ -106,6 +106,8 @@ def tuning_key(info: dict) -> str:
     k = f"k{info['elems_per_thread']}.b{info['block']}.p{info['use_pairs']}.s{info['staged_mode']}"
     if info["staged_mode"]:
         k += f".st{info['stages']}x{info['stage_bytes']}.c{info['stage_consumers']}.g{info['stage_ctas_per_sm']}"
+    if info["bulk_tiles"]:
+        k += f".u{info['bulk_share']}"
     return k
 
 
@@ -124,6 +126,7 @@ def apply_tuning(plan, key: str) -> None:
             forward.append(tok)
     plan.set_tuning(parts["k"], parts["b"], parts["p"])
     plan.set_staged(parts["s"], parts.get("stages", 0), parts.get("stage_bytes", 0), parts.get("c", 0), parts.get("g", 0))
+    plan.set_bulk(parts.get("u", 0))
     if "a" in parts:
         plan.set_adjoint_tuning(parts["a"])
     if tuning_key(plan.info()) != ".".join(forward):

@@ -548,6 +548,11 @@ class ExchangePlan:
         rows and transposed edges, 2 every box it can take; and its pipeline shape (0 keeps)."""
         call("ghexb_plan_set_staged", self._h, mode, stages, stage_bytes, consumers, ctas_per_sm)
 
+    def set_bulk(self, share: int = 4) -> None:
+        """Quarters (0 to 4) of the contiguous 16-byte-unit index lists moved by the bulk kernel
+        (cp.async.bulk through shared memory) in the batched form."""
+        call("ghexb_plan_set_bulk", self._h, share)
+
     def set_adjoint_tuning(self, gather_scale: int = 0) -> None:
         """Adjoint gather tiles of short rows sized by row length (0), halved (-1), doubled (1) or
         quadrupled (2)."""

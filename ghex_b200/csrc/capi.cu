@@ -739,6 +739,13 @@ int64_t check_all(ghexb_plan_s& plan)
         (void)ghexb::check_tables(plan);
     }
     plan.gather_scale = 0;
+    // the bulk kernel taking none and half of the lists (all of them below)
+    for (int share : {0, 2})
+    {
+        plan.bulk_share = share;
+        (void)ghexb::check_tables(plan);
+    }
+    plan.bulk_share = 4;
     const int64_t n = ghexb::check_tables(plan);
     if (plan.shard_mode == 0) ghexb::check_relocation(plan);
     return n;
@@ -840,6 +847,8 @@ int ghexb_plan_get_info(ghexb_plan plan, ghexb_plan_info_t* info)
         info->stage_consumers = plan->stage_consumers;
         info->stage_ctas_per_sm = plan->stage_ctas_per_sm;
         info->gather_scale = plan->gather_scale;
+        info->bulk_share = plan->bulk_share;
+        info->bulk_tiles = (int32_t)plan->bt.size();
     });
 }
 
@@ -882,6 +891,17 @@ int ghexb_plan_set_staged(ghexb_plan plan, int mode, int stages, int stage_bytes
         plan->stages = st, plan->stage_bytes = sb;
         if (consumers > 0) plan->stage_consumers = consumers;
         if (ctas_per_sm > 0) plan->stage_ctas_per_sm = ctas_per_sm;
+        ghexb::retile(*plan);
+        ghexb::check_cuda(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
+    });
+}
+
+int ghexb_plan_set_bulk(ghexb_plan plan, int share)
+{
+    return guarded([&] {
+        require(plan != nullptr, "null plan");
+        require(share >= 0 && share <= 4, "bulk share must be 0 to 4 quarters");
+        plan->bulk_share = share;
         ghexb::retile(*plan);
         ghexb::check_cuda(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
     });

@@ -74,7 +74,7 @@ extern "C" int ghexb_exchange_noalloc(ghexb_context ctx, const ghexb_field* fiel
             throw ghexb::error(GHEXB_ERR_INVALID, "ghexb_exchange_noalloc cannot be captured into a CUDA graph");
         // host tables of the batched form at the default tuning, every tile in the element kernel
         ghexb_plan_s plan;
-        plan.bulk_lists = false;
+        plan.bulk_share = 0;
         ghexb::build_tables(plan, ctx, fields, n);
         for (const auto& f : plan.fields) ghexb::check_accessible(f.data, ghexb::field_bytes(f));
 

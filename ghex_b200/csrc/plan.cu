@@ -1769,8 +1769,8 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
         {
             const auto& l = plan.lists[i];
             const uint32_t cb = (uint32_t)l.levels * 16u;
-            if (!(plan.bulk_lists && l.unit == 16 && cb <= (uint32_t)k_bulk_stage && on_device(plan.list_src_slot[i]) &&
-                    on_device(plan.list_dst_slot[i])))
+            if (!((int)(i % 4) < plan.bulk_share && l.unit == 16 && cb <= (uint32_t)k_bulk_stage &&
+                    on_device(plan.list_src_slot[i]) && on_device(plan.list_dst_slot[i])))
             {
                 all.insert(all.end(), ltiles[i].begin(), ltiles[i].end());
                 continue;
@@ -1967,12 +1967,30 @@ void launch_plan(ghexb_plan_s& plan, int form, cudaStream_t stream)
     switch (form)
     {
         case GHEXB_FORM_BATCHED:
+        {
+            // the staged kernel, and the bulk kernel when the element kernel has work too, run on
+            // the second stream beside the element kernel
             launch_staged_plan(plan, stream);
-            check_cuda(launch_bulk(plan.d_bt, plan.d_bt_blk, (int)plan.bt.size(), plan.d_status, stream), "bulk kernel launch");
+            const bool side_bulk = !plan.bt.empty() && !plan.xf.empty();
+            if (side_bulk)
+            {
+                if (plan.sitems.empty())
+                {
+                    ensure_side_stream(plan);
+                    check_cuda(cudaEventRecord(plan.fork_event, stream), "cudaEventRecord(fork)");
+                    check_cuda(cudaStreamWaitEvent(plan.side_stream, plan.fork_event, 0), "cudaStreamWaitEvent(fork)");
+                }
+                check_cuda(launch_bulk(plan.d_bt, plan.d_bt_blk, (int)plan.bt.size(), plan.d_status, plan.side_stream),
+                    "bulk kernel launch");
+                check_cuda(cudaEventRecord(plan.join_event, plan.side_stream), "cudaEventRecord(join)");
+            }
+            else
+                check_cuda(launch_bulk(plan.d_bt, plan.d_bt_blk, (int)plan.bt.size(), plan.d_status, stream), "bulk kernel launch");
             run(plan.d_xf, plan.xf_blk.empty() ? nullptr : plan.d_xf_blk, {0, (int)plan.xf.size()});
-            if (!plan.sitems.empty())
+            if (!plan.sitems.empty() || side_bulk)
                 check_cuda(cudaStreamWaitEvent(stream, plan.join_event, 0), "cudaStreamWaitEvent(join)");
             break;
+        }
         case GHEXB_FORM_PER_FIELD:
             for (const auto& r : plan.xp_field) run(plan.d_xp, plan.xp_blk.empty() ? nullptr : plan.d_xp_blk, r);
             break;
@@ -2277,17 +2295,21 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         int k, block;
         bool pairs;
         int mode, stages, stage_bytes, consumers, ctas;
+        int bulk;
     };
     const cand start{plan.per_thread, plan.block, plan.use_pairs, plan.staged_mode, plan.stages, plan.stage_bytes,
-        plan.stage_consumers, plan.stage_ctas_per_sm};
-    // the element kernel alone first; then, with its best shape, the staged form beside it
+        plan.stage_consumers, plan.stage_ctas_per_sm, plan.bulk_share};
+    // the element kernel alone first; then, with its best shape, the bulk kernel taking a share of
+    // the lists beside it, and the staged form beside it
     std::vector<cand> cands;
     for (int k : {4, 8, 16})
         for (int block : {128, 256, 512})
             for (bool pairs : {false, true})
                 if (!pairs || !plan.pairs.empty()) cands.push_back({k, block, pairs, 0, start.stages, start.stage_bytes,
-                                                       start.consumers, start.ctas});
+                                                       start.consumers, start.ctas, 0});
     const bool stageable = !plan.boxes.empty() && plan.shard_mode == 0;
+    bool bulkable = false;
+    for (const auto& l : plan.lists) bulkable = bulkable || l.unit == 16;
     const size_t n_element = cands.size();
 
     // every timed launch starts with a cold L2: read a buffer of twice the L2 size first
@@ -2309,6 +2331,7 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         plan.per_thread = c.k, plan.block = c.block, plan.use_pairs = c.pairs;
         plan.staged_mode = c.mode, plan.stages = c.stages, plan.stage_bytes = c.stage_bytes;
         plan.stage_consumers = c.consumers, plan.stage_ctas_per_sm = c.ctas;
+        plan.bulk_share = c.bulk;
         retile(plan, stream);
     };
     try
@@ -2323,6 +2346,7 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
             const cand& c = cands[ci];
             apply(c);
             if (c.mode > 0 && plan.sitems.empty()) continue; // nothing to stage
+            if (c.bulk > 0 && plan.bt.empty()) continue;      // nothing for the bulk kernel
             for (int w = 0; w < 3; ++w) launch_plan(plan, GHEXB_FORM_BATCHED, stream); // warm-up
             // the launches queued back to back, each after a cold-L2 read outside its events, as
             // an application's exchanges follow its other kernels; the mean time per launch
@@ -2341,8 +2365,8 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
                 check_cuda(cudaEventElapsedTime(&ms, ev[2 * r], ev[2 * r + 1]), "cudaEventElapsedTime");
                 total += ms;
             }
-            // a staged candidate whose waits gave up is not a result
-            if (c.mode > 0 && plan.d_status)
+            // a staged or bulk candidate whose waits gave up is not a result
+            if ((c.mode > 0 || c.bulk > 0) && plan.d_status)
             {
                 unsigned st = 0;
                 check_cuda(cudaMemcpyAsync(&st, plan.d_status, sizeof st, cudaMemcpyDeviceToHost, stream), "cudaMemcpyAsync(status)");
@@ -2354,14 +2378,19 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
                 }
             }
             if (total < best) best = total, bestc = c;
-            if (ci + 1 == n_element && stageable)
+            if (ci + 1 == n_element)
             {
-                // the staged form beside the best element-kernel shape
                 const cand e = bestc;
-                for (int mode : {1, 2})
-                    for (const auto& sh : std::vector<std::array<int, 4>>{{8, 16384, 4, 1}, {6, 16384, 8, 1}, {4, 16384, 4, 2},
-                             {12, 8192, 4, 1}})
-                        cands.push_back({e.k, e.block, e.pairs, mode, sh[0], sh[1], sh[2], sh[3]});
+                // the bulk kernel beside the best element-kernel shape
+                if (bulkable)
+                    for (int share : {1, 2, 3, 4})
+                        cands.push_back({e.k, e.block, e.pairs, 0, e.stages, e.stage_bytes, e.consumers, e.ctas, share});
+                // the staged form beside it
+                if (stageable)
+                    for (int mode : {1, 2})
+                        for (const auto& sh : std::vector<std::array<int, 4>>{{8, 16384, 4, 1}, {6, 16384, 8, 1},
+                                 {4, 16384, 4, 2}, {12, 8192, 4, 1}})
+                            cands.push_back({e.k, e.block, e.pairs, mode, sh[0], sh[1], sh[2], sh[3], 0});
             }
         }
     }

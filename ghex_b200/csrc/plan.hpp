@@ -53,11 +53,12 @@ struct ghexb_plan_s
     // k_block_ints each): the indices of the tile's columns, loaded beside its record. Empty
     // when the plan has no lists.
     std::vector<int32_t> xf_blk, xp_blk, xb_blk;
-    // Bulk column tiles of the batched form (bulk.hpp): the list descriptors in 16-byte units
-    // between device fields, when bulk_lists is set, move by the copy engine instead of the element
-    // kernel. bt_blk holds each tile's index block; bt_list and bt_col0 (host only) its list and
-    // first column.
-    bool bulk_lists = true;
+    // Bulk column tiles of the batched form (bulk.hpp): of the list descriptors in 16-byte units
+    // between device fields, those with index i % 4 < bulk_share move by the copy engine (the bulk
+    // kernel, beside the element kernel on a second stream when both have work) instead of the
+    // element kernel: 0 none, 4 all; chosen by the autotuner. bt_blk holds each tile's index block;
+    // bt_list and bt_col0 (host only) its list and first column.
+    int bulk_share = 4;
     std::vector<ghexb::btile> bt;
     std::vector<int32_t> bt_blk;
     std::vector<int> bt_list, bt_col0;
@@ -232,6 +233,8 @@ void build_staged(ghexb_plan_s& plan);
 int64_t check_staged(const ghexb_plan_s& plan);
 // The staged kernel of the batched form on a side stream forked from and joined to `stream`.
 void launch_staged_plan(ghexb_plan_s& plan, cudaStream_t stream);
+// The second stream of the batched form and its fork and join events, made on first use.
+void ensure_side_stream(ghexb_plan_s& plan);
 // Host-only: the least DRAM traffic of one exchange with a cold cache at the given sector size:
 // every sector holding a source element is read, every sector holding a destination element is
 // written back, and a sector written in part that holds no source element is read first.

@@ -255,15 +255,18 @@ int64_t check_staged(const ghexb_plan_s& plan)
     return checked;
 }
 
+void ensure_side_stream(ghexb_plan_s& plan)
+{
+    if (plan.side_stream) return;
+    check_cuda(cudaStreamCreateWithFlags(&plan.side_stream, cudaStreamNonBlocking), "cudaStreamCreate(side)");
+    check_cuda(cudaEventCreateWithFlags(&plan.fork_event, cudaEventDisableTiming), "cudaEventCreate(fork)");
+    check_cuda(cudaEventCreateWithFlags(&plan.join_event, cudaEventDisableTiming), "cudaEventCreate(join)");
+}
+
 void launch_staged_plan(ghexb_plan_s& plan, cudaStream_t stream)
 {
     if (plan.sitems.empty()) return;
-    if (!plan.side_stream)
-    {
-        check_cuda(cudaStreamCreateWithFlags(&plan.side_stream, cudaStreamNonBlocking), "cudaStreamCreate(staged)");
-        check_cuda(cudaEventCreateWithFlags(&plan.fork_event, cudaEventDisableTiming), "cudaEventCreate(staged)");
-        check_cuda(cudaEventCreateWithFlags(&plan.join_event, cudaEventDisableTiming), "cudaEventCreate(staged)");
-    }
+    ensure_side_stream(plan);
     staged_launch a{};
     a.items = plan.d_sitems;
     a.maps = plan.d_smaps;

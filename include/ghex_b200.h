@@ -81,6 +81,9 @@ typedef struct ghexb_plan_info_t
     int32_t stage_ctas_per_sm; /* current tuning: staged CTAs per SM */
     int32_t gather_scale;      /* current adjoint tuning: gather tiles of short rows halved (-1),
                                   sized by row length (0), doubled (1) or quadrupled (2) */
+    int32_t bulk_share;        /* current tuning: quarters (0..4) of the contiguous 16-byte-unit
+                                  index-list descriptors that the bulk kernel moves */
+    int32_t bulk_tiles;        /* its tiles */
 } ghexb_plan_info_t;
 
 /* ---- errors / version ----------------------------------------------------------------- */
@@ -301,6 +304,12 @@ int ghexb_plan_set_tuning(ghexb_plan plan, int elems_per_thread, int block, int 
  * the current one (mode < 0 keeps). Fields in host memory stay on the element kernel.
  * Invalidates the captured graph. */
 int ghexb_plan_set_staged(ghexb_plan plan, int mode, int stages, int stage_bytes, int consumers, int ctas_per_sm);
+/* Bulk column kernel (no GHEX counterpart): index-list descriptors whose columns are contiguous
+ * and in 16-byte units, between device fields, move by the asynchronous copy engine
+ * (cp.async.bulk through shared memory) instead of the element kernel: list i when i % 4 < share
+ * (0 none, 4 all), beside the element kernel on a second stream when both have work. The batched
+ * form only. Invalidates the captured graph. */
+int ghexb_plan_set_bulk(ghexb_plan plan, int share);
 /* Adjoint tiles (no GHEX counterpart): the gather form's tiles of short rows are sized by row
  * length (gather_scale 0), halved (-1), doubled (1) or quadrupled (2), never beyond a full tile.
  * Invalidates the captured graphs. */

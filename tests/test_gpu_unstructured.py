@@ -95,6 +95,42 @@ def test_cfg2_bitexact(cuda, levels_first):
     assert not any(np.isnan(a).any() for a in got64)  # every halo vertex has an owner
 
 
+@pytest.mark.parametrize("share", [0, 1, 2, 4])
+def test_bulk_kernel_shares_bitexact(cuda, share):
+    """The bulk column kernel (cp.async.bulk through shared memory) taking none, a quarter, half
+    (beside the element kernel on a second stream) and all of the lists, in the batched form and
+    its graph: bit-exact against the oracle, and the staged/bulk status word stays 0."""
+    w = W.config2(ni=256, nj=512, levels=64)
+    f64 = [w.domain_array(d, np.float64, 1, True) for d in w.domains]
+    f32 = [w.domain_array(d, np.float32, 2, True) for d in w.domains]
+    doms = [U.DomainDescriptor(*d) for d in w.domains]
+    ctx = U.make_context()
+    pat = U.make_pattern(ctx, U.HaloGenerator(), doms)
+    tens, bis = [], []
+    for arrays in (f64, f32):
+        ts = [torch.from_numpy(a).to("cuda") for a in arrays]
+        tens.append(ts)
+        bis += [pat(U.make_field_descriptor(d, t)) for d, t in zip(doms, ts)]
+    plan = U.make_exchange_plan(ctx, bis)
+    plan.set_bulk(share)
+    info = plan.info()
+    assert info["bulk_share"] == share and (info["bulk_tiles"] > 0) == (share > 0)
+    odoms = [OU.Domain(*d) for d in w.domains]
+    recv, send, _ = OU.make_pattern(odoms)
+    exp64, exp32 = [a.copy() for a in f64], [a.copy() for a in f32]
+    OU.exchange(recv, send, exp64)
+    OU.exchange(recv, send, exp32)
+    for launch in (lambda: plan.launch(plan.BATCHED), lambda: plan.graph_launch()):
+        for ts, arrays in zip(tens, (f64, f32)):
+            for t, a in zip(ts, arrays):
+                t.copy_(torch.from_numpy(a))
+        launch()
+        torch.cuda.synchronize()
+        assert sum(bits_equal(t.cpu().numpy(), e) for t, e in zip(tens[0], exp64)) == 0
+        assert sum(bits_equal(t.cpu().numpy(), e) for t, e in zip(tens[1], exp32)) == 0
+    assert plan.staged_status() == 0
+
+
 @pytest.mark.parametrize("levels_first", [True, False])
 def test_cfg2_adjoint_one_launch_bitexact(cuda, levels_first):
     """The unstructured adjoint in gather form: one launch, every owner column adds its halo
