@@ -2347,14 +2347,15 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
             apply(c);
             if (c.mode > 0 && plan.sitems.empty()) continue; // nothing to stage
             if (c.bulk > 0 && plan.bt.empty()) continue;      // nothing for the bulk kernel
-            for (int w = 0; w < 3; ++w) launch_plan(plan, GHEXB_FORM_BATCHED, stream); // warm-up
-            // the launches queued back to back, each after a cold-L2 read outside its events, as
-            // an application's exchanges follow its other kernels; the mean time per launch
+            for (int w = 0; w < 3; ++w) graph_launch_plan(plan, stream); // capture and warm-up
+            // the graph launches queued back to back (the form the batched exchange runs in, where
+            // a second stream's fork and join are graph edges), each after a cold-L2 read outside
+            // its events, as an application's exchanges follow its other kernels; the mean time
             for (int r = 0; r < repeats; ++r)
             {
                 check_cuda(launch_l2_flush(flush, flush_bytes / 16, sink, fgrid, stream), "l2 flush");
                 check_cuda(cudaEventRecord(ev[2 * r], stream), "cudaEventRecord");
-                launch_plan(plan, GHEXB_FORM_BATCHED, stream);
+                graph_launch_plan(plan, stream);
                 check_cuda(cudaEventRecord(ev[2 * r + 1], stream), "cudaEventRecord");
             }
             check_cuda(cudaEventSynchronize(ev[2 * repeats - 1]), "cudaEventSynchronize");
