@@ -70,6 +70,8 @@ def parse():
                     help="cfg1 sharded over the ranks (one per GPU, domains dealt round-robin): each rank's "
                          "kernel moves its part of the exchange through the other GPUs' memory, between two "
                          "NCCL barriers on the exchange's stream (ghex_b200.distributed); total work fixed")
+    ap.add_argument("--bulk-ab", action="store_true",
+                    help="time the bulk column kernel's shares of the lists against the element kernel on cfg2")
     ap.add_argument("--staged-ab", action="store_true",
                     help="time the staged (tensor-map) form against the element kernel on cfg1, cfg3 and cfg4")
     ap.add_argument("--calibrate-host", action="store_true",
@@ -886,6 +888,34 @@ def staged_ab(args):
     print(json.dumps(out), flush=True)
 
 
+def bulk_ab(args):
+    """The bulk column kernel (cp.async.bulk through shared memory) against the element kernel on
+    the unstructured workloads: cold-L2 time of the batched graph at the autotuned element shape
+    with the bulk kernel taking 0 to 4 quarters of the lists (beside the element kernel on a second
+    stream when both have work), two runs of 40 launches each. One JSON line."""
+    import torch
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    l2 = torch.cuda.get_device_properties(dev).L2_cache_size
+    flush = torch.ones(max(2 * l2, 64 << 20) // 4, dtype=torch.float32, device=dev)
+    timer = Timer(stream, flush, 1, dev)
+    s = stream.cuda_stream
+    out = {"bulk_ab": "cold-L2 CUDA-event time of the batched graph, us, two runs of 40 launches", "configs": {}}
+    for cfg in ("cfg2", "cfg2_ipr"):
+        case = Case(cfg, dev, 0)
+        plan = case.plan
+        info = plan.autotune(repeats=20, stream=s)
+        row = {"autotuned": tuning_key(info)}
+        for share in (0, 1, 2, 3, 4):
+            plan.set_bulk(share)
+            row[f"share{share}"] = {"us": [timer(lambda: plan.graph_launch(s), 40, 5) * 1e3 for _ in range(2)],
+                                    "bulk_tiles": plan.info()["bulk_tiles"], "element_tiles": plan.info()["num_tiles"]}
+        row["status"] = plan.staged_status()
+        out["configs"][cfg] = row
+        del case, plan
+    print(json.dumps(out), flush=True)
+
+
 def run_sharded(args) -> None:
     """cfg1 sharded over the ranks: every rank holds the fields of its domains only; one step is a
     sharded exchange (NCCL barrier, this rank's kernel, NCCL barrier), timed with CUDA events on the
@@ -995,6 +1025,9 @@ def main():
         return
     if args.staged_ab:
         staged_ab(args)
+        return
+    if args.bulk_ab:
+        bulk_ab(args)
         return
     import torch
     import torch.distributed as dist
