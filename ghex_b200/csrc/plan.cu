@@ -1769,7 +1769,8 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
         {
             const auto& l = plan.lists[i];
             const uint32_t cb = (uint32_t)l.levels * 16u;
-            if (!((int)(i % 4) < plan.bulk_share && l.unit == 16 && cb <= (uint32_t)k_bulk_stage &&
+            // (not on a sharded plan: its fields include other processes' memory)
+            if (!((int)(i % 4) < plan.bulk_share && plan.shard_mode == 0 && l.unit == 16 && cb <= (uint32_t)k_bulk_stage &&
                     on_device(plan.list_src_slot[i]) && on_device(plan.list_dst_slot[i])))
             {
                 all.insert(all.end(), ltiles[i].begin(), ltiles[i].end());
@@ -2309,7 +2310,7 @@ void autotune_plan(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
                                                        start.consumers, start.ctas, 0});
     const bool stageable = !plan.boxes.empty() && plan.shard_mode == 0;
     bool bulkable = false;
-    for (const auto& l : plan.lists) bulkable = bulkable || l.unit == 16;
+    for (const auto& l : plan.lists) bulkable = bulkable || (l.unit == 16 && plan.shard_mode == 0);
     const size_t n_element = cands.size();
 
     // every timed launch starts with a cold L2: read a buffer of twice the L2 size first

@@ -257,7 +257,7 @@ int ghexb_plan_destroy(ghexb_plan plan);
  * plans, and together they hold every descriptor of the exchange. The caller orders the
  * processes: every process's fields must be final before any process launches, and no process
  * may change its fields until every process's launch is done (a barrier on both sides). The
- * staged form and rebinding are not available on sharded plans. */
+ * staged form, the bulk column kernel and rebinding are not available on sharded plans. */
 int ghexb_plan_create_sharded(ghexb_context ctx, const ghexb_field* fields, int n, const unsigned char* local, int mode,
     ghexb_plan* out);
 /* Host-only replay of a sharded plan's tables (as ghexb_plan_check, and every descriptor and
