@@ -254,42 +254,47 @@ __device__ __forceinline__ void gather_elements(const gtile& t)
     F* __restrict__ own = reinterpret_cast<F*>(t.own);
     F h[K][NI];
     F acc[K];
-    int32_t ooff[K];
-    int32_t hoff[K][NI];
+    // an element's cell coordinates are derived again for the stores rather than its offsets held
+    // in registers across the loads
+    auto coords = [&](uint32_t e, int32_t& i0, int32_t& i1, int32_t& i2) {
+        const uint32_t g = t.e0 + e;
+        const uint32_t r = fdiv(g, t.m0, t.l0);
+        i0 = (int32_t)(g - r * t.n0);
+        const uint32_t q = fdiv(r, t.m1, t.l1);
+        i1 = (int32_t)(r - q * t.n1), i2 = (int32_t)q;
+    };
 #pragma unroll
     for (int k = 0; k < K; ++k)
     {
         const uint32_t e = k * blockDim.x + threadIdx.x;
         if (e < t.count)
         {
-            const uint32_t g = t.e0 + e;
-            const uint32_t r = fdiv(g, t.m0, t.l0);
-            const int32_t i0 = (int32_t)(g - r * t.n0);
-            const uint32_t q = fdiv(r, t.m1, t.l1);
-            const int32_t i1 = (int32_t)(r - q * t.n1), i2 = (int32_t)q;
-            ooff[k] = i0 * t.o0 + i1 * t.o1 + i2 * t.o2;
-            acc[k] = __ldcg(own + ooff[k]);
+            int32_t i0, i1, i2;
+            coords(e, i0, i1, i2);
+            acc[k] = __ldcg(own + (i0 * t.o0 + i1 * t.o1 + i2 * t.o2));
 #pragma unroll
             for (int i = 0; i < NI; ++i)
-            {
-                hoff[k][i] = i0 * t.img[i].t0 + i1 * t.img[i].t1 + i2 * t.img[i].t2;
-                h[k][i] = __ldcg(reinterpret_cast<const F*>(t.img[i].ptr) + hoff[k][i]);
-            }
+                h[k][i] = __ldcg(reinterpret_cast<const F*>(t.img[i].ptr) + (i0 * t.img[i].t0 + i1 * t.img[i].t1 + i2 * t.img[i].t2));
         }
     }
 #pragma unroll
     for (int k = 0; k < K; ++k)
-        if (k * blockDim.x + threadIdx.x < t.count)
+    {
+        const uint32_t e = k * blockDim.x + threadIdx.x;
+        if (e < t.count)
         {
+            int32_t i0, i1, i2;
+            coords(e, i0, i1, i2);
             F a = acc[k];
 #pragma unroll
             for (int i = 0; i < NI; ++i)
             {
                 a = t.img[i].neg ? a - h[k][i] : a + h[k][i];
-                st_global(reinterpret_cast<F*>(t.img[i].ptr) + hoff[k][i], F(0));
+                st_global(reinterpret_cast<F*>(t.img[i].ptr) + (i0 * t.img[i].t0 + i1 * t.img[i].t1 + i2 * t.img[i].t2), F(0));
             }
-            st_global(own + ooff[k], a);
+            st_global(own + (i0 * t.o0 + i1 * t.o1 + i2 * t.o2), a);
         }
+    }
 }
 
 // Unstructured owner columns: element e is level e mod n0 of owner e / n0 of the group; the
@@ -300,42 +305,44 @@ __device__ __forceinline__ void list_gather_elements(const gtile& t, const uint6
 {
     F h[K][NI];
     F acc[K];
-    F* own[K];
-    F* img[K][NI];
-    // the tile's columns from its block in shared memory, else from the column table
+    // the tile's columns from its block in shared memory, else from the column table; a column's
+    // address is looked up again for the stores rather than held in registers across the loads
     const uint32_t j0 = blk ? fdiv(t.e0, t.m0, t.l0) : 0u;
     const uint64_t* base = blk ? blk - (size_t)j0 * (NI + 1) : cols + t.col0;
+    auto column = [&](uint32_t e, int i) {
+        const uint32_t g = t.e0 + e;
+        const uint32_t j = fdiv(g, t.m0, t.l0);
+        const int32_t lev = (int32_t)(g - j * t.n0);
+        const uint64_t* p = base + (size_t)j * (NI + 1) + i;
+        return reinterpret_cast<F*>(blk ? *p : __ldg(p)) + lev * (i == 0 ? t.o0 : t.img[0].t0);
+    };
 #pragma unroll
     for (int k = 0; k < K; ++k)
     {
         const uint32_t e = k * blockDim.x + threadIdx.x;
         if (e < t.count)
         {
-            const uint32_t g = t.e0 + e;
-            const uint32_t j = fdiv(g, t.m0, t.l0);
-            const int32_t lev = (int32_t)(g - j * t.n0);
-            const uint64_t* p = base + (size_t)j * (NI + 1);
-            own[k] = reinterpret_cast<F*>(blk ? p[0] : __ldg(p)) + lev * t.o0;
+            acc[k] = __ldcg(column(e, 0));
 #pragma unroll
-            for (int i = 0; i < NI; ++i) img[k][i] = reinterpret_cast<F*>(blk ? p[1 + i] : __ldg(p + 1 + i)) + lev * t.img[0].t0;
-            acc[k] = __ldcg(own[k]);
-#pragma unroll
-            for (int i = 0; i < NI; ++i) h[k][i] = __ldcg(img[k][i]);
+            for (int i = 0; i < NI; ++i) h[k][i] = __ldcg(column(e, 1 + i));
         }
     }
 #pragma unroll
     for (int k = 0; k < K; ++k)
-        if (k * blockDim.x + threadIdx.x < t.count)
+    {
+        const uint32_t e = k * blockDim.x + threadIdx.x;
+        if (e < t.count)
         {
             F a = acc[k];
 #pragma unroll
             for (int i = 0; i < NI; ++i)
             {
                 a = a + h[k][i];
-                st_global(img[k][i], F(0));
+                st_global(column(e, 1 + i), F(0));
             }
-            st_global(own[k], a);
+            st_global(column(e, 0), a);
         }
+    }
 }
 
 __global__ void __launch_bounds__(k_gather_block, 3) gather_kernel(const gtile* __restrict__ tiles)
@@ -364,7 +371,7 @@ __global__ void __launch_bounds__(k_gather_block, 3) gather_kernel(const gtile* 
 // its instruction-cache footprint) stays that of the box classes.
 static_assert(k_gblock_entries % 2 == 0 && 16 + k_gblock_entries / 2 <= k_gather_block, "column block load lanes");
 
-__global__ void __launch_bounds__(k_gather_block, 3) list_gather_kernel(const gtile* __restrict__ tiles,
+__global__ void __launch_bounds__(k_gather_block, 4) list_gather_kernel(const gtile* __restrict__ tiles,
     const uint64_t* __restrict__ cols, const uint64_t* __restrict__ blocks)
 {
     __shared__ gtile t;
