@@ -693,7 +693,7 @@ def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline
     if cfg in ("cfg2", "cfg3", "cfg4", "cfg4_f32"):
         ms_a = timer(lambda: plan.adjoint(s), steps, warmup)
         out["adjoint"] = {"ms": ms_a, "vs_forward": ms_a / ms_b, "launches": plan.info()["adjoint_launches"],
-                          "gather_scale": plan.info()["gather_scale"]}
+                          "gather_scale": plan.info()["gather_scale"], "gather_bulk": plan.info()["gather_bulk"]}
     if baseline:
         case.reset()
         plan.launch(plan.BATCHED, s)

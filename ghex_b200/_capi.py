@@ -78,6 +78,8 @@ class PlanInfo(C.Structure):
         ("gather_scale", C.c_int32),
         ("bulk_share", C.c_int32),
         ("bulk_tiles", C.c_int32),
+        ("gather_bulk", C.c_int32),
+        ("gather_bulk_tiles", C.c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -129,6 +131,7 @@ SIGNATURES = {
     "ghexb_plan_staged_status": [_vp, C.POINTER(C.c_uint)],
     "ghexb_plan_set_adjoint_tuning": [_vp, _i],
     "ghexb_plan_set_bulk": [_vp, _i],
+    "ghexb_plan_set_adjoint_bulk": [_vp, _i],
     "ghexb_plan_create_sharded": [_vp, C.POINTER(_vp), _i, C.c_char_p, _i, C.POINTER(_vp)],
     "ghexb_plan_check_sharded": [_vp, C.POINTER(_vp), _i, C.c_char_p, _i, _pi64],
     "ghexb_ipc_export": [_vp, C.c_char_p, _pi64],

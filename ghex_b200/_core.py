@@ -553,6 +553,11 @@ class ExchangePlan:
         (cp.async.bulk through shared memory) in the batched form."""
         call("ghexb_plan_set_bulk", self._h, share)
 
+    def set_adjoint_bulk(self, share: int = 0) -> None:
+        """Quarters (0 to 4) of the unstructured owners whose adjoint the bulk gather kernel
+        (cp.async.bulk through shared memory) takes, beside the element gather kernel."""
+        call("ghexb_plan_set_adjoint_bulk", self._h, share)
+
     def set_adjoint_tuning(self, gather_scale: int = 0) -> None:
         """Adjoint gather tiles of short rows sized by row length (0), halved (-1), doubled (1) or
         quadrupled (2)."""

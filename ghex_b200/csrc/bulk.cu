@@ -43,7 +43,75 @@ __global__ void __launch_bounds__(32) bulk_kernel(const btile* __restrict__ tile
     bulk_commit();
     bulk_wait_read();
 }
+
+// acc = own; acc = acc + image_i in order, for every level of every owner column of the stage
+template<typename F>
+__device__ __forceinline__ void gather_stage(unsigned char* stage, const bgtile& t, unsigned lane)
+{
+    const uint32_t per = t.nimg + 1, total = t.nown * t.levels;
+    for (uint32_t e = lane; e < total; e += 32)
+    {
+        const uint32_t c = e / t.levels, lev = e - c * t.levels;
+        F* own = reinterpret_cast<F*>(stage + (size_t)c * per * t.col_bytes) + lev;
+        F a = *own;
+        for (uint32_t i = 1; i <= t.nimg; ++i) a = a + reinterpret_cast<const F*>(stage + (size_t)(c * per + i) * t.col_bytes)[lev];
+        *own = a;
+    }
+}
+
+__global__ void __launch_bounds__(32) bulk_gather_kernel(const bgtile* __restrict__ tiles, const uint64_t* __restrict__ blocks,
+    unsigned* status)
+{
+    __shared__ __align__(128) unsigned char stage[k_bulk_stage];
+    __shared__ __align__(16) unsigned char zero[k_bgather_zero];
+    __shared__ __align__(16) bgtile t;
+    __shared__ __align__(16) uint64_t blk[k_bgather_entries];
+    __shared__ __align__(8) uint64_t bar;
+    const unsigned lane = threadIdx.x;
+    // the record (two words) and the column addresses (48 words), one round trip
+    const uint4* b = reinterpret_cast<const uint4*>(blocks + (size_t)blockIdx.x * k_bgather_entries);
+    if (lane < 2) reinterpret_cast<uint4*>(&t)[lane] = __ldg(reinterpret_cast<const uint4*>(tiles + blockIdx.x) + lane);
+    for (unsigned w = lane; w < k_bgather_entries / 2; w += 32) reinterpret_cast<uint4*>(blk)[w] = __ldg(b + w);
+    for (unsigned w = lane; w < k_bgather_zero / 16; w += 32) reinterpret_cast<uint4*>(zero)[w] = make_uint4(0, 0, 0, 0);
+    if (lane == 0)
+    {
+        mbar_init(&bar, 1);
+        mbar_init_fence();
+    }
+    __syncwarp();
+    const uint32_t n = t.nown * (t.nimg + 1), cb = t.col_bytes;
+    if (lane == 0) mbar_expect_tx(&bar, n * cb);
+    __syncwarp();
+    for (uint32_t c = lane; c < n; c += 32) bulk_load(stage + c * cb, reinterpret_cast<const void*>(blk[c]), cb, &bar);
+    if (!mbar_wait(&bar, 0))
+    {
+        // the loads did not complete in time: nothing is stored; the CTA waits (again bounded) for
+        // its loads, which write into its shared memory, before it ends
+        if (lane == 0 && status) atomicOr(status, 4u);
+        (void)mbar_wait(&bar, 0);
+        return;
+    }
+    if (t.esize == 8) gather_stage<double>(stage, t, lane);
+    else
+        gather_stage<float>(stage, t, lane);
+    // the sums and the zeros, written by the threads, are read by the copy engine
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    const uint32_t per = t.nimg + 1;
+    for (uint32_t c = lane; c < n; c += 32)
+        bulk_store(reinterpret_cast<void*>(blk[c]), c % per == 0 ? static_cast<const void*>(stage + c * cb) : zero, cb);
+    bulk_commit();
+    bulk_wait_read();
+}
 } // namespace
+
+cudaError_t launch_bulk_gather(const bgtile* tiles, const uint64_t* blocks, int ntiles, unsigned* status,
+    cudaStream_t stream)
+{
+    if (ntiles <= 0) return cudaSuccess;
+    bulk_gather_kernel<<<ntiles, 32, 0, stream>>>(tiles, blocks, status);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_bulk(const btile* tiles, const int32_t* blocks, int ntiles, unsigned* status, cudaStream_t stream)
 {

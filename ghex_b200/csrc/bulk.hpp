@@ -31,4 +31,23 @@ static_assert(sizeof(btile) == 48, "btile is three 16-byte words");
 // One CTA of 32 threads per tile. `status` (nullptr: none) gets bit 0 when a wait for a tile's
 // loads gave up (its columns are then not stored).
 cudaError_t launch_bulk(const btile* tiles, const int32_t* blocks, int ntiles, unsigned* status, cudaStream_t stream);
+
+// Adjoint of unstructured columns in bulk form: a tile of nown owner columns, each with nimg image
+// columns, all of col_bytes (a multiple of 16, at most k_bgather_zero) with their levels
+// contiguous. The CTA loads every column into shared memory, adds each owner's images into it in
+// order (acc = own; acc = acc + image_i), and stores the owner columns back and zeros into the
+// image columns, all by the copy engine. Its index block holds the columns' addresses, per owner
+// the owner's then its images' (k_bgather_entries at most). `status` gets bit 2 when a wait for a
+// tile's loads gave up (nothing of the tile is then stored).
+constexpr int k_bgather_entries = 96;
+constexpr int k_bgather_zero = 2048;
+struct alignas(16) bgtile
+{
+    uint32_t nown, nimg, col_bytes, levels;
+    uint32_t esize;
+    uint32_t pad[3];
+};
+static_assert(sizeof(bgtile) == 32, "bgtile is two 16-byte words");
+cudaError_t launch_bulk_gather(const bgtile* tiles, const uint64_t* blocks, int ntiles, unsigned* status,
+    cudaStream_t stream);
 } // namespace ghexb

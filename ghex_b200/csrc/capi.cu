@@ -739,13 +739,20 @@ int64_t check_all(ghexb_plan_s& plan)
         (void)ghexb::check_tables(plan);
     }
     plan.gather_scale = 0;
-    // the bulk kernel taking none and half of the lists (all of them below)
+    // the bulk kernel taking none and half of the lists (all of them below), and the bulk gather
+    // kernel taking half and all of the unstructured owners
     for (int share : {0, 2})
     {
         plan.bulk_share = share;
         (void)ghexb::check_tables(plan);
     }
     plan.bulk_share = 4;
+    for (int share : {2, 4})
+    {
+        plan.gather_bulk = share;
+        (void)ghexb::check_tables(plan);
+    }
+    plan.gather_bulk = 0;
     const int64_t n = ghexb::check_tables(plan);
     if (plan.shard_mode == 0) ghexb::check_relocation(plan);
     return n;
@@ -849,6 +856,8 @@ int ghexb_plan_get_info(ghexb_plan plan, ghexb_plan_info_t* info)
         info->gather_scale = plan->gather_scale;
         info->bulk_share = plan->bulk_share;
         info->bulk_tiles = (int32_t)plan->bt.size();
+        info->gather_bulk = plan->gather_bulk;
+        info->gather_bulk_tiles = (int32_t)plan->bgt.size();
     });
 }
 
@@ -902,6 +911,17 @@ int ghexb_plan_set_bulk(ghexb_plan plan, int share)
         require(plan != nullptr, "null plan");
         require(share >= 0 && share <= 4, "bulk share must be 0 to 4 quarters");
         plan->bulk_share = share;
+        ghexb::retile(*plan);
+        ghexb::check_cuda(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
+    });
+}
+
+int ghexb_plan_set_adjoint_bulk(ghexb_plan plan, int share)
+{
+    return guarded([&] {
+        require(plan != nullptr, "null plan");
+        require(share >= 0 && share <= 4, "adjoint bulk share must be 0 to 4 quarters");
+        plan->gather_bulk = share;
         ghexb::retile(*plan);
         ghexb::check_cuda(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize");
     });

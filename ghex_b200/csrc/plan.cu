@@ -1169,6 +1169,7 @@ void relocate_tiles(ghexb_plan_s& plan, const relocator& R)
     for (auto& c : plan.lcols) R(c);
     for (auto& c : plan.gblk) R(c);
     for (auto& t : plan.bt) R(t.src), R(t.dst);
+    for (auto& c : plan.bgt_blk) R(c);
 }
 
 } // namespace
@@ -1183,7 +1184,7 @@ void check_relocation(ghexb_plan_s& plan)
     if (!R.ok) return;
     ghexb_plan_s copy;
     copy.xf = plan.xf, copy.xp = plan.xp, copy.xb = plan.xb, copy.xpair = plan.xpair, copy.gt = plan.gt, copy.lcols = plan.lcols;
-    copy.gblk = plan.gblk, copy.bt = plan.bt;
+    copy.gblk = plan.gblk, copy.bt = plan.bt, copy.bgt_blk = plan.bgt_blk;
     relocate_tiles(copy, R);
     const auto old_data = plan.fields;
     const auto old_boxes = plan.boxes;
@@ -1205,7 +1206,7 @@ void check_relocation(ghexb_plan_s& plan)
     };
     const bool equal = same(copy.xf, plan.xf) && same(copy.xp, plan.xp) && same(copy.xb, plan.xb) &&
                        same(copy.xpair, plan.xpair) && same(copy.gt, plan.gt) && same(copy.lcols, plan.lcols) &&
-                       same(copy.gblk, plan.gblk) && same(copy.bt, plan.bt);
+                       same(copy.gblk, plan.gblk) && same(copy.bt, plan.bt) && same(copy.bgt_blk, plan.bgt_blk);
     plan.fields = old_data, plan.boxes = old_boxes, plan.lists = old_lists;
     build_tiles(plan, plan.idx.data());
     if (!equal) throw error(GHEXB_ERR_INTERNAL, "moved tile tables differ from the tables built at the new address");
@@ -1478,6 +1479,26 @@ int64_t check_tables(ghexb_plan_s& plan)
                 if ((int64_t)t.col0 + (int64_t)(t.e0 + t.count - 1) / t.n0 * (t.nimg + 1) + t.nimg >= (int64_t)plan.lcols.size())
                     throw error(GHEXB_ERR_INTERNAL, "adjoint tile outside the column table");
             }
+        // bulk gather tiles: their column addresses as the column table holds them, 16-byte aligned,
+        // within the shared stage; their owners are covered by them and by no element tile
+        if (plan.bgt_blk.size() != plan.bgt.size() * k_bgather_entries || plan.bgt_first.size() != plan.bgt.size())
+            throw error(GHEXB_ERR_INTERNAL, "bulk gather tiles and their blocks differ in number");
+        for (size_t u = 0; u < plan.bgt.size(); ++u)
+        {
+            const auto& t = plan.bgt[u];
+            const uint64_t per = (uint64_t)t.nimg + 1, n = t.nown * per;
+            if (t.nown == 0 || n > (uint64_t)k_bgather_entries || t.col_bytes % 16 || t.col_bytes > (uint32_t)k_bgather_zero ||
+                n * t.col_bytes > (uint64_t)k_bulk_stage || t.col_bytes != t.levels * t.esize ||
+                (uint64_t)plan.bgt_first[u] + n > plan.lcols.size())
+                throw error(GHEXB_ERR_INTERNAL, "bulk gather tile out of shape");
+            for (uint64_t c = 0; c < n; ++c)
+            {
+                const uint64_t a = plan.bgt_blk[u * k_bgather_entries + c];
+                if (a != plan.lcols[plan.bgt_first[u] + c] || a % 16)
+                    throw error(GHEXB_ERR_INTERNAL, "bulk gather block differs from the column table");
+            }
+            covered += (int64_t)t.nown * t.levels;
+        }
         if (covered != levels) throw error(GHEXB_ERR_INTERNAL, "adjoint tiles do not cover every owner level");
         // column blocks: the flagged tiles' blocks hold their slices of the column table
         if (plan.gblk.size() != (plan.gt.size() - (size_t)plan.gt_boxes) * k_gblock_entries)
@@ -1565,6 +1586,8 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
     ensure(plan.d_gblk, plan.cap_gblk, plan.gblk.size());
     ensure(plan.d_bt, plan.cap_bt, plan.bt.size());
     ensure(plan.d_bt_blk, plan.cap_bt_blk, plan.bt_blk.size());
+    ensure(plan.d_bgt, plan.cap_bgt, plan.bgt.size());
+    ensure(plan.d_bgt_blk, plan.cap_bgt_blk, plan.bgt_blk.size());
     ensure(plan.d_smaps, plan.cap_smaps, plan.smaps.size());
     ensure(plan.d_sitems, plan.cap_sitems, plan.sitems.size());
     ensure(plan.d_xf_blk, plan.cap_xf_blk, plan.xf_blk.size());
@@ -1582,9 +1605,11 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
     st.put(plan.d_gblk, plan.gblk);
     st.put(plan.d_bt, plan.bt);
     st.put(plan.d_bt_blk, plan.bt_blk);
+    st.put(plan.d_bgt, plan.bgt);
+    st.put(plan.d_bgt_blk, plan.bgt_blk);
     st.put(plan.d_smaps, plan.smaps);
     st.put(plan.d_sitems, plan.sitems);
-    if ((!plan.sitems.empty() || !plan.bt.empty()) && !plan.d_status)
+    if ((!plan.sitems.empty() || !plan.bt.empty() || !plan.bgt.empty()) && !plan.d_status)
     {
         check_cuda(cudaMalloc(&plan.d_status, sizeof(unsigned)), "cudaMalloc(staged status)");
         check_cuda(cudaMemsetAsync(plan.d_status, 0, sizeof(unsigned), stream), "cudaMemsetAsync(staged status)");
@@ -1854,8 +1879,11 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
         append_range(plan.gt, all);
     }
     plan.gt_boxes = (int)plan.gt.size();
-    // ---- unstructured adjoint, gather form: owner groups and their column table
+    // ---- unstructured adjoint, gather form: owner groups and their column table; of a group whose
+    // columns are contiguous and 16-byte aligned, the first gather_bulk quarters of its owners go
+    // to the bulk gather kernel
     plan.lcols.clear();
+    plan.bgt.clear(), plan.bgt_blk.clear(), plan.bgt_first.clear();
     if (plan.list_gather_ok)
     {
         for (size_t a = 0; a < plan.lowners.size();)
@@ -1865,7 +1893,8 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
             while (b < plan.lowners.size() && plan.lowners[b].esize == o0.esize && plan.lowners[b].nimg == o0.nimg &&
                    plan.lowners[b].levels == o0.levels && plan.lowners[b].s_ls == o0.s_ls && plan.lowners[b].d_ls == o0.d_ls)
                 ++b;
-            const uint32_t col0 = (uint32_t)plan.lcols.size();
+            const uint32_t group0 = (uint32_t)plan.lcols.size();
+            bool aligned = true;
             for (size_t j = a; j < b; ++j)
             {
                 const auto& o = plan.lowners[j];
@@ -1873,8 +1902,39 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
                 for (int i = 0; i < o.nimg; ++i)
                     plan.lcols.push_back((uint64_t)(uintptr_t)(plan.fields[o.img_slot[i]].data + o.img_off[i]));
             }
+            for (size_t c = group0; c < plan.lcols.size(); ++c) aligned = aligned && plan.lcols[c] % 16 == 0;
+            const uint32_t per = (uint32_t)o0.nimg + 1, cb = (uint32_t)(o0.levels * o0.esize);
+            auto on_device = [&](int slot) { return plan.field_on_device.empty() || plan.field_on_device[slot]; };
+            bool devices = true;
+            for (size_t j = a; j < b && devices; ++j)
+            {
+                devices = on_device(plan.lowners[j].slot);
+                for (int i = 0; i < plan.lowners[j].nimg; ++i) devices = devices && on_device(plan.lowners[j].img_slot[i]);
+            }
+            const bool bulkable = plan.gather_bulk > 0 && plan.shard_mode == 0 && aligned && devices && o0.s_ls == 1 &&
+                                  o0.d_ls == 1 && cb % 16 == 0 && cb <= (uint32_t)k_bgather_zero &&
+                                  per * cb <= (uint32_t)k_bulk_stage;
+            const size_t nb = bulkable ? (b - a) * (size_t)plan.gather_bulk / 4 : 0;
+            if (nb > 0)
+            {
+                const uint32_t cap = std::min<uint32_t>((uint32_t)k_bulk_stage / (per * cb), (uint32_t)k_bgather_entries / per);
+                for (size_t j = 0; j < nb; j += cap)
+                {
+                    bgtile t{};
+                    t.nown = (uint32_t)std::min<size_t>(cap, nb - j), t.nimg = per - 1, t.col_bytes = cb;
+                    t.levels = (uint32_t)o0.levels, t.esize = (uint32_t)o0.esize;
+                    const size_t blk0 = plan.bgt_blk.size();
+                    plan.bgt_blk.resize(blk0 + k_bgather_entries, 0);
+                    std::copy(plan.lcols.begin() + (int64_t)(group0 + j * per), plan.lcols.begin() + (int64_t)(group0 + (j + t.nown) * per),
+                        plan.bgt_blk.begin() + (int64_t)blk0);
+                    plan.bgt.push_back(t);
+                    plan.bgt_first.push_back((int)(group0 + j * per));
+                }
+            }
+            // the other owners of the group: element tiles of list_gather_kernel
+            const uint32_t col0 = group0 + (uint32_t)(nb * per);
             const uint32_t gc = (uint32_t)(gather_per_thread(o0.nimg) * k_gather_block);
-            const uint32_t n = (uint32_t)((int64_t)(b - a) * o0.levels);
+            const uint32_t n = (uint32_t)((int64_t)(b - a - nb) * o0.levels);
             const fast_div f0 = fast_div::make((uint32_t)o0.levels);
             for (uint32_t e0 = 0; e0 < n; e0 += gc)
             {
@@ -2040,6 +2100,21 @@ void adjoint_launches(ghexb_plan_s& plan, cudaStream_t stream)
     check_cuda(launch_list_gather(plan.d_gt + plan.gt_boxes, (int)plan.gt.size() - plan.gt_boxes, plan.d_lcols,
                    plan.gblk.empty() ? nullptr : plan.d_gblk, stream),
         "adjoint kernel launch");
+    // the bulk gather kernel, on the second stream when other adjoint kernels run (its owners and
+    // images are no other kernel's)
+    const bool side_bulk = !plan.bgt.empty() && (!plan.gt.empty() || !plan.adj_btiles.empty() || !plan.adj_ltiles.empty());
+    if (side_bulk)
+    {
+        ensure_side_stream(plan);
+        check_cuda(cudaEventRecord(plan.fork_event, stream), "cudaEventRecord(fork)");
+        check_cuda(cudaStreamWaitEvent(plan.side_stream, plan.fork_event, 0), "cudaStreamWaitEvent(fork)");
+        check_cuda(launch_bulk_gather(plan.d_bgt, plan.d_bgt_blk, (int)plan.bgt.size(), plan.d_status, plan.side_stream),
+            "bulk gather kernel launch");
+        check_cuda(cudaEventRecord(plan.join_event, plan.side_stream), "cudaEventRecord(join)");
+    }
+    else
+        check_cuda(launch_bulk_gather(plan.d_bgt, plan.d_bgt_blk, (int)plan.bgt.size(), plan.d_status, stream),
+            "bulk gather kernel launch");
     const int sms = plan.ctx ? plan.ctx->num_sms : 148;
     auto grid = [&](int n) { return std::min(n, 4 * sms); };
     for (size_t ph = 0; ph < plan.adj_bphase_range.size(); ++ph)
@@ -2055,6 +2130,7 @@ void adjoint_launches(ghexb_plan_s& plan, cudaStream_t stream)
                            grid(rl.second), 256, stream),
                 "adjoint kernel launch");
     }
+    if (side_bulk) check_cuda(cudaStreamWaitEvent(stream, plan.join_event, 0), "cudaStreamWaitEvent(join)");
 }
 } // namespace
 
@@ -2175,6 +2251,8 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
     st.put(plan.d_gblk, plan.gblk);
     st.put(plan.d_bt, plan.bt);
     st.put(plan.d_bt_blk, plan.bt_blk);
+    st.put(plan.d_bgt, plan.bgt);
+    st.put(plan.d_bgt_blk, plan.bgt_blk);
     st.put(plan.d_boxes, plan.boxes);
     st.put(plan.d_lists, plan.lists);
     st.put(plan.d_adj_lists, plan.adj_lists);
@@ -2231,9 +2309,11 @@ void autotune_adjoint(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         for (auto e : ev)
             if (e) cudaEventDestroy(e);
     };
-    const int start = plan.gather_scale;
-    int best_scale = start;
+    const int start = plan.gather_scale, start_bulk = plan.gather_bulk;
+    int best_scale = start, best_bulk = start_bulk;
     float best = 1e30f;
+    bool bulk_candidates = false;
+    for (const auto& o : plan.lowners) bulk_candidates = bulk_candidates || (o.s_ls == 1 && o.d_ls == 1);
     try
     {
         copy_fields(false);
@@ -2242,10 +2322,16 @@ void autotune_adjoint(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         check_cuda(cudaMalloc(&sink, sizeof(unsigned)), "cudaMalloc(l2 flush sink)");
         for (auto& e : ev) check_cuda(cudaEventCreate(&e), "cudaEventCreate");
         const int fgrid = (plan.ctx ? plan.ctx->num_sms : 148) * 8;
-        for (int scale : {-1, 0, 1, 2})
+        // the gather-tile sizes of the box cells, then, at the best size, the bulk gather kernel's
+        // shares of the unstructured owners
+        std::vector<std::pair<int, int>> cands;
+        for (int scale : {-1, 0, 1, 2}) cands.push_back({scale, start_bulk});
+        for (size_t ci = 0; ci < cands.size(); ++ci)
         {
-            plan.gather_scale = scale;
+            const int scale = cands[ci].first;
+            plan.gather_scale = scale, plan.gather_bulk = cands[ci].second;
             retile(plan, stream);
+            if (ci > 3 && plan.gather_bulk > 0 && plan.bgt.empty()) continue; // nothing for the bulk kernel
             for (int w = 0; w < 3; ++w) adjoint_plan(plan, stream);
             for (int r = 0; r < repeats; ++r)
             {
@@ -2262,7 +2348,20 @@ void autotune_adjoint(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
                 check_cuda(cudaEventElapsedTime(&ms, ev[2 * r], ev[2 * r + 1]), "cudaEventElapsedTime");
                 total += ms;
             }
-            if (total < best) best = total, best_scale = scale;
+            // a bulk candidate whose waits gave up is not a result
+            bool failed = false;
+            if (!plan.bgt.empty() && plan.d_status)
+            {
+                unsigned st = 0;
+                check_cuda(cudaMemcpyAsync(&st, plan.d_status, sizeof st, cudaMemcpyDeviceToHost, stream), "cudaMemcpyAsync(status)");
+                check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+                if (st) check_cuda(cudaMemsetAsync(plan.d_status, 0, sizeof st, stream), "cudaMemsetAsync(status)");
+                failed = st != 0;
+            }
+            if (!failed && total < best) best = total, best_scale = scale, best_bulk = plan.gather_bulk;
+            if (ci == 3 && bulk_candidates)
+                for (int share : {0, 1, 2, 3, 4})
+                    if (share != start_bulk) cands.push_back({best_scale, share});
         }
     }
     catch (...)
@@ -2277,11 +2376,11 @@ void autotune_adjoint(ghexb_plan_s& plan, cudaStream_t stream, int repeats)
         cudaStreamSynchronize(stream);
         cleanup();
         cudaFree(saved);
-        plan.gather_scale = start;
+        plan.gather_scale = start, plan.gather_bulk = start_bulk;
         throw;
     }
     cleanup();
-    plan.gather_scale = best_scale;
+    plan.gather_scale = best_scale, plan.gather_bulk = best_bulk;
     retile(plan, stream);
     copy_fields(true);
     check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
@@ -2422,7 +2521,7 @@ ghexb_plan_s::~ghexb_plan_s()
     if (fork_event) cudaEventDestroy(fork_event);
     if (join_event) cudaEventDestroy(join_event);
     for (void* p : {(void*)d_smaps, (void*)d_sitems, (void*)d_status, (void*)d_xf_blk, (void*)d_xp_blk, (void*)d_xb_blk,
-             (void*)d_gblk, (void*)d_bt, (void*)d_bt_blk})
+             (void*)d_gblk, (void*)d_bt, (void*)d_bt_blk, (void*)d_bgt, (void*)d_bgt_blk})
         if (p) cudaFree(p);
     for (void* p : {(void*)d_boxes, (void*)d_lists, (void*)d_adj_lists, (void*)d_idx, (void*)d_xf, (void*)d_xp,
              (void*)d_xb, (void*)d_gt, (void*)d_lcols, (void*)d_adj_btiles, (void*)d_adj_ltiles, (void*)d_counters})
@@ -2438,7 +2537,7 @@ int64_t ghexb_plan_s::num_tiles() const
 
 int ghexb_plan_s::adjoint_launches() const
 {
-    int n = (gt_boxes > 0) + ((int)gt.size() > gt_boxes);
+    int n = (gt_boxes > 0) + ((int)gt.size() > gt_boxes) + !bgt.empty();
     for (size_t ph = 0; ph < adj_bphase_range.size(); ++ph)
         n += (adj_bphase_range[ph].second > 0) + (adj_lphase_range[ph].second > 0);
     return n;

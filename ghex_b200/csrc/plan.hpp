@@ -138,6 +138,17 @@ struct ghexb_plan_s
     // adjoint gather tiles of short rows: -1 half the size, 0 sized by row length, 1 and 2 that
     // size doubled or quadrupled (never beyond a full tile); chosen by the autotuner
     int gather_scale = 0;
+    // Unstructured adjoint in bulk form (bulk.hpp): of every owner group whose columns are
+    // contiguous and 16-byte aligned, the first gather_bulk quarters of the owners go to the bulk
+    // gather kernel, beside list_gather_kernel on a second stream; chosen by the autotuner.
+    // bgt_blk: per tile its column addresses; bgt_first (host only): its first owner in lowners.
+    int gather_bulk = 0;
+    std::vector<ghexb::bgtile> bgt;
+    std::vector<uint64_t> bgt_blk;
+    std::vector<int> bgt_first;
+    ghexb::bgtile* d_bgt = nullptr;
+    uint64_t* d_bgt_blk = nullptr;
+    size_t cap_bgt = 0, cap_bgt_blk = 0;
 
     // Staged form of box descriptors (staged.hpp), batched form only: the boxes marked in
     // box_staged are loaded through tensor maps by the staged kernel, which runs beside the

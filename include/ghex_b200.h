@@ -84,6 +84,9 @@ typedef struct ghexb_plan_info_t
     int32_t bulk_share;        /* current tuning: quarters (0..4) of the contiguous 16-byte-unit
                                   index-list descriptors that the bulk kernel moves */
     int32_t bulk_tiles;        /* its tiles */
+    int32_t gather_bulk;       /* current adjoint tuning: quarters (0..4) of the unstructured owners
+                                  whose adjoint the bulk gather kernel takes */
+    int32_t gather_bulk_tiles; /* its tiles */
 } ghexb_plan_info_t;
 
 /* ---- errors / version ----------------------------------------------------------------- */
@@ -314,9 +317,15 @@ int ghexb_plan_set_bulk(ghexb_plan plan, int share);
  * length (gather_scale 0), halved (-1), doubled (1) or quadrupled (2), never beyond a full tile.
  * Invalidates the captured graphs. */
 int ghexb_plan_set_adjoint_tuning(ghexb_plan plan, int gather_scale);
-/* Status word of the staged kernel since the last call, then cleared: 0 when every wait of the
- * kernel ended in time; bit 0 a load, bit 1 a write that gave up waiting (its halos are then
- * incomplete). Synchronises the device. */
+/* Bulk form of the unstructured adjoint (no GHEX counterpart): of every owner group whose columns
+ * are contiguous and 16-byte aligned, the first `share` quarters (0..4) of the owners are gathered
+ * by a kernel that moves their columns with the asynchronous copy engine (cp.async.bulk) through
+ * shared memory, beside the element gather kernel on a second stream. The additions keep the
+ * receive order: the result is the same bit for bit. Invalidates the captured graphs. */
+int ghexb_plan_set_adjoint_bulk(ghexb_plan plan, int share);
+/* Status word of the staged and bulk kernels since the last call, then cleared: 0 when every wait
+ * ended in time; bit 0 a load (staged or bulk kernel), bit 1 a staged write, bit 2 a bulk gather
+ * load that gave up waiting (its halos or owners are then incomplete). Synchronises the device. */
 int ghexb_plan_staged_status(ghexb_plan plan, unsigned* status);
 /* One forward exchange in the given form, stream-ordered. */
 int ghexb_plan_launch(ghexb_plan plan, int form, void* stream);

@@ -159,6 +159,38 @@ def test_cfg2_adjoint_one_launch_bitexact(cuda, levels_first):
     assert sum(bits_equal(t.cpu().numpy(), e) for t, e in zip(t32, g32)) == 0
 
 
+@pytest.mark.parametrize("share", [2, 4])
+def test_adjoint_bulk_gather_shares_bitexact(cuda, share):
+    """The bulk gather kernel (columns by cp.async.bulk through shared memory, sums in shared
+    memory in receive order) taking half or all of the owners, beside the element gather kernel:
+    bit-exact against the explicit transpose, status word 0."""
+    w = W.config2(ni=256, nj=512, levels=64)
+    rng = np.random.default_rng(23)
+    g64 = [np.asarray(rng.standard_normal((d[1].size, w.levels)), order="C") for d in w.domains]
+    g32 = [np.asarray(rng.standard_normal((d[1].size, w.levels)), dtype=np.float32, order="C") for d in w.domains]
+    ctx = U.make_context()
+    doms = [U.DomainDescriptor(*d) for d in w.domains]
+    pat = U.make_pattern(ctx, U.HaloGenerator(), doms)
+    t64 = [torch.from_numpy(a).to("cuda") for a in g64]
+    t32 = [torch.from_numpy(a).to("cuda") for a in g32]
+    bis = [pat(U.make_field_descriptor(d, t)) for d, t in zip(doms, t64)] + \
+          [pat(U.make_field_descriptor(d, t)) for d, t in zip(doms, t32)]
+    plan = U.make_exchange_plan(ctx, bis)
+    plan.set_adjoint_bulk(share)
+    info = plan.info()
+    assert info["gather_bulk"] == share and info["gather_bulk_tiles"] > 0
+    assert info["adjoint_launches"] == (2 if share < 4 else 1)
+    plan.adjoint()
+    torch.cuda.synchronize()
+    odoms = [OU.Domain(*d) for d in w.domains]
+    recv, send, _ = OU.make_pattern(odoms)
+    OU.adjoint(recv, send, g64)
+    OU.adjoint(recv, send, g32)
+    assert sum(bits_equal(t.cpu().numpy(), e) for t, e in zip(t64, g64)) == 0
+    assert sum(bits_equal(t.cpu().numpy(), e) for t, e in zip(t32, g32)) == 0
+    assert plan.staged_status() == 0
+
+
 @pytest.mark.parametrize("levels", [1, 2])
 def test_receive_domain_ids_generator(levels):
     """make_pattern(ctx, hg, recv_domain_ids_gen, domains) of GHEX's C++ test case: GHEX's own
