@@ -9,8 +9,24 @@ namespace ghexb
 {
 namespace
 {
+__device__ __forceinline__ void gather4(void* dst, const CUtensorMap* map, const int32_t* rows, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+                 ::"r"(smem_u32(dst)), "l"(map), "r"(0), "r"(rows[0]), "r"(rows[1]), "r"(rows[2]), "r"(rows[3]),
+                 "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void scatter4(const CUtensorMap* map, const int32_t* rows, const void* src)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile::scatter4.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];"
+                 ::"l"(map), "r"(0), "r"(rows[0]), "r"(rows[1]), "r"(rows[2]), "r"(rows[3]), "r"(smem_u32(src))
+                 : "memory");
+}
+
 __global__ void __launch_bounds__(32) bulk_kernel(const btile* __restrict__ tiles, const int32_t* __restrict__ blocks,
-    unsigned* status)
+    const CUtensorMap* __restrict__ maps, unsigned* status)
 {
     __shared__ __align__(128) unsigned char stage[k_bulk_stage];
     __shared__ __align__(16) btile t;
@@ -27,9 +43,21 @@ __global__ void __launch_bounds__(32) bulk_kernel(const btile* __restrict__ tile
     }
     __syncwarp();
     const uint32_t n = t.ncols, cb = t.col_bytes;
-    if (lane == 0) mbar_expect_tx(&bar, n * cb);
+    const bool four = t.smap >= 0;
+    const uint32_t groups = (n + 3) / 4; // four columns at a time: lanes 0 .. groups - 1
+    int32_t rows[4];
+    if (lane == 0) mbar_expect_tx(&bar, four ? groups * 4 * cb : n * cb);
     __syncwarp();
-    for (uint32_t c = lane; c < n; c += 32) bulk_load(stage + c * cb, t.src + (int64_t)blk[c] * t.s_is, cb, &bar);
+    if (four)
+    {
+        if (lane < groups)
+        {
+            for (int q = 0; q < 4; ++q) rows[q] = blk[min(4 * lane + (uint32_t)q, n - 1)];
+            gather4(stage + lane * 4 * cb, maps + t.smap, rows, &bar);
+        }
+    }
+    else
+        for (uint32_t c = lane; c < n; c += 32) bulk_load(stage + c * cb, t.src + (int64_t)blk[c] * t.s_is, cb, &bar);
     if (!mbar_wait(&bar, 0))
     {
         // the loads did not complete in time: the tile's columns are not stored; the CTA waits
@@ -39,7 +67,16 @@ __global__ void __launch_bounds__(32) bulk_kernel(const btile* __restrict__ tile
         return;
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    for (uint32_t c = lane; c < n; c += 32) bulk_store(t.dst + (int64_t)blk[k_bulk_columns + c] * t.d_is, stage + c * cb, cb);
+    if (four)
+    {
+        if (lane < groups)
+        {
+            for (int q = 0; q < 4; ++q) rows[q] = blk[k_bulk_columns + min(4 * lane + (uint32_t)q, n - 1)];
+            scatter4(maps + t.dmap, rows, stage + lane * 4 * cb);
+        }
+    }
+    else
+        for (uint32_t c = lane; c < n; c += 32) bulk_store(t.dst + (int64_t)blk[k_bulk_columns + c] * t.d_is, stage + c * cb, cb);
     bulk_commit();
     bulk_wait_read();
 }
@@ -113,10 +150,11 @@ cudaError_t launch_bulk_gather(const bgtile* tiles, const uint64_t* blocks, int 
     return cudaGetLastError();
 }
 
-cudaError_t launch_bulk(const btile* tiles, const int32_t* blocks, int ntiles, unsigned* status, cudaStream_t stream)
+cudaError_t launch_bulk(const btile* tiles, const int32_t* blocks, const CUtensorMap* maps, int ntiles, unsigned* status,
+    cudaStream_t stream)
 {
     if (ntiles <= 0) return cudaSuccess;
-    bulk_kernel<<<ntiles, 32, 0, stream>>>(tiles, blocks, status);
+    bulk_kernel<<<ntiles, 32, 0, stream>>>(tiles, blocks, maps, status);
     return cudaGetLastError();
 }
 } // namespace ghexb

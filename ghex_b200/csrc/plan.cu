@@ -1355,6 +1355,15 @@ int64_t check_tables(ghexb_plan_s& plan)
         if (t.ncols == 0 || t.ncols > (uint32_t)k_bulk_columns || t.col_bytes % 16 || t.col_bytes != (uint32_t)l.levels * 16u ||
             (int64_t)t.ncols * t.col_bytes > k_bulk_stage || t.src != l.src || t.dst != l.dst)
             throw error(GHEXB_ERR_INTERNAL, "bulk tile out of shape");
+        const bool four = t.smap >= 0;
+        if (four != (t.dmap >= 0) || (four && (t.smap >= (int32_t)plan.bmap_geo.size() || t.dmap >= (int32_t)plan.bmap_geo.size() ||
+                                                  (int64_t)(t.ncols + 3) / 4 * 4 * t.col_bytes > k_bulk_stage || (4 * t.col_bytes) % 128)))
+            throw error(GHEXB_ERR_INTERNAL, "bulk tile's tensor maps out of shape");
+        if (four)
+            for (const auto& [g, base, is] : {std::tuple{plan.bmap_geo[t.smap], t.src, t.s_is}, std::tuple{plan.bmap_geo[t.dmap], (const char*)t.dst, t.d_is}})
+                if (g.base != base || g.stride != is || (int64_t)g.width * g.es != (int64_t)t.col_bytes || g.stride % 16 ||
+                    reinterpret_cast<uintptr_t>(g.base) % 16 || g.width > 256)
+                    throw error(GHEXB_ERR_INTERNAL, "bulk tile's tensor map differs from its columns");
         const int32_t* S = plan.idx.data() + plan.list_idx_off[i];
         for (uint32_t c = 0; c < t.ncols; ++c)
         {
@@ -1366,6 +1375,9 @@ int64_t check_tables(ghexb_plan_s& plan)
             const int64_t dof = (t.dst - df.data) + (int64_t)S[l.count + col] * t.d_is;
             if (so < 0 || so + t.col_bytes > sbytes || dof < 0 || dof + t.col_bytes > dbytes)
                 throw error(GHEXB_ERR_RANGE, "bulk column outside its field's memory");
+            if (four && (S[col] < 0 || S[col] >= plan.bmap_geo[t.smap].rows || S[l.count + col] < 0 ||
+                            S[l.count + col] >= plan.bmap_geo[t.dmap].rows))
+                throw error(GHEXB_ERR_RANGE, "bulk column outside its tensor map");
             if ((reinterpret_cast<uintptr_t>(sf.data) + (uint64_t)so) % 16 || (reinterpret_cast<uintptr_t>(df.data) + (uint64_t)dof) % 16)
                 throw error(GHEXB_ERR_INTERNAL, "bulk column not 16-byte aligned");
         }
@@ -1586,6 +1598,7 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
     ensure(plan.d_gblk, plan.cap_gblk, plan.gblk.size());
     ensure(plan.d_bt, plan.cap_bt, plan.bt.size());
     ensure(plan.d_bt_blk, plan.cap_bt_blk, plan.bt_blk.size());
+    ensure(plan.d_bmaps, plan.cap_bmaps, plan.bmaps.size());
     ensure(plan.d_bgt, plan.cap_bgt, plan.bgt.size());
     ensure(plan.d_bgt_blk, plan.cap_bgt_blk, plan.bgt_blk.size());
     ensure(plan.d_smaps, plan.cap_smaps, plan.smaps.size());
@@ -1605,6 +1618,7 @@ void retile(ghexb_plan_s& plan, cudaStream_t stream)
     st.put(plan.d_gblk, plan.gblk);
     st.put(plan.d_bt, plan.bt);
     st.put(plan.d_bt_blk, plan.bt_blk);
+    st.put(plan.d_bmaps, plan.bmaps);
     st.put(plan.d_bgt, plan.bgt);
     st.put(plan.d_bgt_blk, plan.bgt_blk);
     st.put(plan.d_smaps, plan.smaps);
@@ -1789,7 +1803,36 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
                     all.insert(all.end(), ptiles[p].begin(), ptiles[p].end());
         // lists in 16-byte units between device fields: bulk column tiles, else element tiles
         plan.bt.clear(), plan.bt_blk.clear(), plan.bt_list.clear(), plan.bt_col0.clear();
+        plan.bmaps.clear(), plan.bmap_geo.clear();
         auto on_device = [&](int slot) { return plan.field_on_device.empty() || plan.field_on_device[slot]; };
+        // the tensor map of a field's columns from `base` (a row per index, `width` elements a
+        // row): its index in bmaps, or -1 when it cannot be had (a column wider than a load box)
+        auto bmap = [&](int slot, const char* base, int width) -> int32_t {
+            const auto& f = plan.fields[slot];
+            const int64_t rows = f.pattern->domains[f.domain_index].size, stride = f.index_stride * f.esize;
+            if (width < 1 || width > 256 || rows < 1 || rows > k_i32max || stride % 16 || reinterpret_cast<uintptr_t>(base) % 16)
+                return -1;
+            for (size_t m = 0; m < plan.bmap_geo.size(); ++m)
+            {
+                const auto& g = plan.bmap_geo[m];
+                if (g.base == base && g.rows == rows && g.stride == stride && g.width == width && g.es == f.esize) return (int32_t)m;
+            }
+            CUtensorMap map{};
+            if (plan.encode_maps)
+            {
+                const cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)rows};
+                const cuuint64_t strides[1] = {(cuuint64_t)stride};
+                const cuuint32_t box[2] = {(cuuint32_t)width, 1};
+                const CUtensorMapDataType type = f.esize == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : f.esize == 4 ? CU_TENSOR_MAP_DATA_TYPE_UINT32
+                                                 : f.esize == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+                if (encode_tensor_map(&map, type, 2, const_cast<char*>(base), dims, strides, box, CU_TENSOR_MAP_L2_PROMOTION_NONE) !=
+                    CUDA_SUCCESS)
+                    return -1;
+            }
+            plan.bmaps.push_back(map);
+            plan.bmap_geo.push_back({base, rows, stride, width, f.esize});
+            return (int32_t)plan.bmaps.size() - 1;
+        };
         for (size_t i = 0; i < plan.lists.size(); ++i)
         {
             const auto& l = plan.lists[i];
@@ -1801,7 +1844,14 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
                 all.insert(all.end(), ltiles[i].begin(), ltiles[i].end());
                 continue;
             }
-            const int32_t per = (int32_t)std::min<uint32_t>(k_bulk_columns, (uint32_t)k_bulk_stage / cb);
+            // four columns at a time through tensor maps when both fields have one, else one at a time
+            const int es = plan.fields[plan.list_src_slot[i]].esize;
+            int32_t smap = bmap(plan.list_src_slot[i], l.src, (int)(cb / es));
+            int32_t dmap = smap >= 0 ? bmap(plan.list_dst_slot[i], l.dst, (int)(cb / es)) : -1;
+            const uint32_t four = (uint32_t)k_bulk_stage / (4 * cb) * 4;
+            // (each group of four starts on a 128-byte boundary of the shared stage)
+            if (smap < 0 || dmap < 0 || four < 4 || (4 * cb) % 128) smap = dmap = -1;
+            const int32_t per = (int32_t)std::min<uint32_t>(k_bulk_columns, smap >= 0 ? four : (uint32_t)k_bulk_stage / cb);
             const int32_t* S = plan.idx.data() + plan.list_idx_off[i];
             const int32_t* D = S + l.count;
             for (int32_t c0 = 0; c0 < l.count; c0 += per)
@@ -1811,6 +1861,7 @@ void build_tiles(ghexb_plan_s& plan, const int32_t* idx)
                 t.s_is = (int64_t)l.s_is * 16, t.d_is = (int64_t)l.d_is * 16;
                 t.ncols = (uint32_t)std::min(per, l.count - c0);
                 t.col_bytes = cb;
+                t.smap = smap, t.dmap = dmap;
                 const size_t b = plan.bt_blk.size();
                 plan.bt_blk.resize(b + k_bulk_block_ints, 0);
                 for (uint32_t c = 0; c < t.ncols; ++c)
@@ -2041,12 +2092,15 @@ void launch_plan(ghexb_plan_s& plan, int form, cudaStream_t stream)
                     check_cuda(cudaEventRecord(plan.fork_event, stream), "cudaEventRecord(fork)");
                     check_cuda(cudaStreamWaitEvent(plan.side_stream, plan.fork_event, 0), "cudaStreamWaitEvent(fork)");
                 }
-                check_cuda(launch_bulk(plan.d_bt, plan.d_bt_blk, (int)plan.bt.size(), plan.d_status, plan.side_stream),
+                check_cuda(launch_bulk(plan.d_bt, plan.d_bt_blk, plan.bmaps.empty() ? nullptr : plan.d_bmaps, (int)plan.bt.size(),
+                               plan.d_status, plan.side_stream),
                     "bulk kernel launch");
                 check_cuda(cudaEventRecord(plan.join_event, plan.side_stream), "cudaEventRecord(join)");
             }
             else
-                check_cuda(launch_bulk(plan.d_bt, plan.d_bt_blk, (int)plan.bt.size(), plan.d_status, stream), "bulk kernel launch");
+                check_cuda(launch_bulk(plan.d_bt, plan.d_bt_blk, plan.bmaps.empty() ? nullptr : plan.d_bmaps, (int)plan.bt.size(),
+                           plan.d_status, stream),
+                    "bulk kernel launch");
             run(plan.d_xf, plan.xf_blk.empty() ? nullptr : plan.d_xf_blk, {0, (int)plan.xf.size()});
             if (!plan.sitems.empty() || side_bulk)
                 check_cuda(cudaStreamWaitEvent(stream, plan.join_event, 0), "cudaStreamWaitEvent(join)");
@@ -2216,7 +2270,7 @@ void rebind_plan(ghexb_plan_s& plan, void* const* data, int n, cudaStream_t stre
         plan.adj_lists[i].src = plan.fields[plan.adj_src_slot[i]].data + plan.adj_src_off[i];
         plan.adj_lists[i].dst = plan.fields[plan.adj_dst_slot[i]].data + plan.adj_dst_off[i];
     }
-    if (plan.staged_mode > 0)
+    if (plan.staged_mode > 0 || !plan.bmaps.empty())
     {
         // tensor maps hold addresses, and which boxes a map can load depends on the alignment of
         // the new memory: the tables are rebuilt (and the graph recaptured on its next launch)
@@ -2521,7 +2575,7 @@ ghexb_plan_s::~ghexb_plan_s()
     if (fork_event) cudaEventDestroy(fork_event);
     if (join_event) cudaEventDestroy(join_event);
     for (void* p : {(void*)d_smaps, (void*)d_sitems, (void*)d_status, (void*)d_xf_blk, (void*)d_xp_blk, (void*)d_xb_blk,
-             (void*)d_gblk, (void*)d_bt, (void*)d_bt_blk, (void*)d_bgt, (void*)d_bgt_blk})
+             (void*)d_gblk, (void*)d_bt, (void*)d_bt_blk, (void*)d_bgt, (void*)d_bgt_blk, (void*)d_bmaps})
         if (p) cudaFree(p);
     for (void* p : {(void*)d_boxes, (void*)d_lists, (void*)d_adj_lists, (void*)d_idx, (void*)d_xf, (void*)d_xp,
              (void*)d_xb, (void*)d_gt, (void*)d_lcols, (void*)d_adj_btiles, (void*)d_adj_ltiles, (void*)d_counters})

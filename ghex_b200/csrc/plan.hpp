@@ -65,6 +65,18 @@ struct ghexb_plan_s
     ghexb::btile* d_bt = nullptr;
     int32_t* d_bt_blk = nullptr;
     size_t cap_bt = 0, cap_bt_blk = 0;
+    // tensor maps of the bulk tiles' fields (a row per index, the levels of a column in a row),
+    // for their four-column gather and scatter copies, and their geometry for the host replay
+    struct bmap_info
+    {
+        const char* base;
+        int64_t rows, stride; // rows (indices) and bytes per row step
+        int width, es;        // elements per row moved (the column), element size
+    };
+    std::vector<CUtensorMap> bmaps;
+    std::vector<bmap_info> bmap_geo;
+    CUtensorMap* d_bmaps = nullptr;
+    size_t cap_bmaps = 0;
     bool forms_stale = false; // xp and xb moved on the host by a rebind, not yet on the device
     int32_t *d_xf_blk = nullptr, *d_xp_blk = nullptr, *d_xb_blk = nullptr;
     size_t cap_xf_blk = 0, cap_xp_blk = 0, cap_xb_blk = 0;
