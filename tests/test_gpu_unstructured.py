@@ -159,6 +159,31 @@ def test_cfg2_adjoint_one_launch_bitexact(cuda, levels_first):
     assert sum(bits_equal(t.cpu().numpy(), e) for t, e in zip(t32, g32)) == 0
 
 
+def test_bulk_plan_rebind_bitexact(cuda):
+    """A plan whose lists move through tensor maps (four-column bulk tiles) rebound to other
+    memory: its maps are made again for the new fields, and the exchange there is bit-exact."""
+    w = W.config2(ni=256, nj=512, levels=64)
+    f64 = [w.domain_array(d, np.float64, 1, True) for d in w.domains]
+    doms = [U.DomainDescriptor(*d) for d in w.domains]
+    ctx = U.make_context()
+    pat = U.make_pattern(ctx, U.HaloGenerator(), doms)
+    first = [torch.from_numpy(a).to("cuda") for a in f64]
+    plan = U.make_exchange_plan(ctx, [pat(U.make_field_descriptor(d, t)) for d, t in zip(doms, first)])
+    plan.set_bulk(4)
+    assert plan.info()["bulk_tiles"] > 0
+    second = [torch.from_numpy(a).to("cuda") for a in f64]
+    plan.rebind(second)
+    plan.graph_launch()
+    torch.cuda.synchronize()
+    odoms = [OU.Domain(*d) for d in w.domains]
+    recv, send, _ = OU.make_pattern(odoms)
+    exp = [a.copy() for a in f64]
+    OU.exchange(recv, send, exp)
+    assert sum(bits_equal(t.cpu().numpy(), e) for t, e in zip(second, exp)) == 0
+    assert sum(bits_equal(t.cpu().numpy(), a) for t, a in zip(first, f64)) == 0  # the old memory untouched
+    assert plan.staged_status() == 0
+
+
 @pytest.mark.parametrize("share", [2, 4])
 def test_adjoint_bulk_gather_shares_bitexact(cuda, share):
     """The bulk gather kernel (columns by cp.async.bulk through shared memory, sums in shared
