@@ -1,6 +1,7 @@
 /*
  * ghex_b200.hpp — C++ front end over the C ABI of ghex_b200.h, with the names and call shapes of
- * GHEX's own C++ interface for the regular structured grid, so that GHEX code of the form
+ * GHEX's own C++ interface for the regular structured grid and for unstructured column data, so
+ * that GHEX code of the form
  *
  *     auto ctxt    = ghexb::context(device);
  *     auto pattern = ghexb::make_pattern<ghexb::structured::grid>(ctxt, halo_gen, local_domains);
@@ -18,6 +19,10 @@
  *   make_communication_object<Pattern>     communication_object.hpp:653-660
  *   communication_object::exchange         communication_object.hpp:233-274
  *   communication_handle::wait/is_ready    communication_object.hpp:627-648
+ *   unstructured::domain_descriptor        unstructured/user_concepts.hpp:37-174
+ *   unstructured::halo_generator           unstructured/user_concepts.hpp:181-256
+ *   unstructured::data_descriptor          unstructured/user_concepts.hpp:264-581
+ *   make_pattern<unstructured::grid>       pattern_container.hpp:112-120, unstructured/pattern.hpp:187-370
  *
  * Header only; link with libghex_b200.so. Every failing C call throws ghexb::error (a
  * std::runtime_error carrying the status code and the library's message), as GHEX throws
@@ -35,6 +40,7 @@
 #include <stdexcept>
 #include <string>
 #include <type_traits>
+#include <unordered_set>
 #include <utility>
 #include <vector>
 
@@ -241,6 +247,113 @@ class field_descriptor
 } // namespace regular
 } // namespace structured
 
+namespace unstructured
+{
+struct grid
+{
+};
+
+// unstructured::domain_descriptor<DomainId, Idx>(id, gids first, last, outer lids first, last):
+// the domain's global ids in storage order and the local ids of its outer (halo) elements
+template<typename DomainId, typename Idx>
+class domain_descriptor
+{
+  public:
+    using domain_id_type = DomainId;
+    using global_index_type = Idx;
+    using local_index_type = std::size_t;
+
+    template<typename GidIt, typename LidIt>
+    domain_descriptor(domain_id_type id, GidIt first, GidIt last, LidIt outer_first, LidIt outer_last)
+    : m_id(id)
+    , m_gids(first, last)
+    {
+        std::unordered_set<local_index_type> seen;
+        for (auto it = outer_first; it != outer_last; ++it)
+        {
+            const local_index_type lid = (local_index_type)*it;
+            if (!seen.insert(lid).second) throw std::runtime_error("repeated outer (local) index");
+            if (lid >= m_gids.size()) throw std::runtime_error("outer local index out of range");
+            m_outer.push_back(lid);
+        }
+    }
+
+    domain_id_type domain_id() const noexcept { return m_id; }
+    std::size_t size() const noexcept { return m_gids.size(); }
+    std::size_t inner_size() const noexcept { return m_gids.size() - m_outer.size(); }
+    const std::vector<global_index_type>& gids() const noexcept { return m_gids; }
+    const std::vector<local_index_type>& outer_lids() const noexcept { return m_outer; }
+
+  private:
+    domain_id_type m_id;
+    std::vector<global_index_type> m_gids;
+    std::vector<local_index_type> m_outer;
+};
+
+// halo_generator(): every outer element is a halo element; halo_generator(gids): the halo of a
+// domain is its outer elements with these global ids, in this order
+template<typename DomainId, typename Idx>
+class halo_generator
+{
+  public:
+    halo_generator() = default;
+    explicit halo_generator(std::vector<Idx> gids)
+    : m_all(false)
+    , m_gids(std::move(gids))
+    {
+    }
+    bool all() const noexcept { return m_all; }
+    const std::vector<Idx>& gids() const noexcept { return m_gids; }
+
+  private:
+    bool m_all = true;
+    std::vector<Idx> m_gids;
+};
+
+// data_descriptor<Arch, DomainId, Idx, T>(domain, data, levels, levels_first, outer_stride): a
+// column field of `levels` values per element; levels_first: the levels of an element are
+// adjacent; outer_stride: elements between consecutive outer indices (0: no padding)
+template<typename Arch, typename DomainId, typename Idx, typename T>
+class data_descriptor
+{
+  public:
+    using arch_type = Arch;
+    using value_type = T;
+    using domain_descriptor_type = domain_descriptor<DomainId, Idx>;
+
+    data_descriptor(const domain_descriptor_type& domain, T* field, std::size_t levels = 1u, bool levels_first = true,
+        std::size_t outer_stride = 0u)
+    : m_domain_id(domain.domain_id())
+    , m_size(domain.size())
+    , m_levels(levels)
+    , m_levels_first(levels_first)
+    , m_outer_stride(outer_stride)
+    , m_data(field)
+    {
+    }
+
+    DomainId domain_id() const noexcept { return m_domain_id; }
+    T* data() const noexcept { return m_data; }
+    std::size_t levels() const noexcept { return m_levels; }
+    bool levels_first() const noexcept { return m_levels_first; }
+    std::size_t outer_stride() const noexcept { return m_outer_stride; }
+    // bytes from the first element to one past the last one the field may address
+    std::size_t span_bytes() const noexcept
+    {
+        const std::size_t index_stride = m_levels_first ? (m_outer_stride ? m_outer_stride : m_levels) : 1u;
+        const std::size_t level_stride = m_levels_first ? 1u : (m_outer_stride ? m_outer_stride : m_size);
+        return ((m_size - 1) * index_stride + (m_levels - 1) * level_stride + 1) * sizeof(T);
+    }
+
+  private:
+    DomainId m_domain_id;
+    std::size_t m_size, m_levels;
+    bool m_levels_first;
+    std::size_t m_outer_stride;
+    T* m_data;
+};
+} // namespace unstructured
+
 // wrap_field<Arch, Layout>(dom, data, offsets, extents[, byte_strides])
 template<typename Arch, typename Layout, typename DomainDescriptor, typename T>
 structured::regular::field_descriptor<T, Arch, DomainDescriptor, Layout> wrap_field(const DomainDescriptor& dom, T* data,
@@ -315,6 +428,24 @@ class pattern_container
         return bi;
     }
 
+    // pattern(data_descriptor) -> buffer_info for unstructured column fields
+    template<typename Arch, typename DomainId, typename Idx, typename T>
+    buffer_info operator()(const unstructured::data_descriptor<Arch, DomainId, Idx, T>& f) const
+    {
+        buffer_info bi;
+        if (std::is_same<Arch, cpu>::value)
+        {
+            int owned = 0;
+            check(ghexb_host_register(f.data(), f.span_bytes(), &owned));
+            if (owned) bi.m_state->registered = f.data();
+        }
+        ghexb_field h = nullptr;
+        check(ghexb_field_wrap_unstructured(get(), (std::int64_t)f.domain_id(), detail::dtype_of<T>::value, f.data(),
+            (std::int64_t)f.levels(), f.levels_first() ? 1 : 0, (std::int64_t)f.outer_stride(), &h));
+        bi.m_state->field.reset(h);
+        return bi;
+    }
+
   private:
     std::shared_ptr<ghexb_pattern_s> m_h;
     explicit pattern_container(ghexb_pattern h)
@@ -325,27 +456,53 @@ class pattern_container
     friend auto make_pattern(context&, const H&, const R&);
 };
 
-// make_pattern<structured::grid>(ctxt, halo_gen, domain_range)
+// make_pattern<structured::grid>(ctxt, halo_gen, domain_range) and
+// make_pattern<unstructured::grid>(ctxt, halo_gen, domain_range)
 template<typename Grid, typename HaloGenerator, typename DomainRange>
 auto make_pattern(context& ctxt, const HaloGenerator& hg, const DomainRange& domains)
 {
-    static_assert(std::is_same<Grid, structured::grid>::value, "this front end covers the regular structured grid");
+    static_assert(std::is_same<Grid, structured::grid>::value || std::is_same<Grid, unstructured::grid>::value,
+        "this front end covers the regular structured grid and unstructured column data");
     using dom_type = typename std::decay<decltype(*std::begin(domains))>::type;
-    constexpr int dim = dom_type::dim;
-    std::vector<std::int64_t> ids;
-    std::vector<int> firsts, lasts;
-    for (const auto& d : domains)
+    if constexpr (std::is_same<Grid, unstructured::grid>::value)
     {
-        ids.push_back((std::int64_t)d.domain_id());
-        firsts.insert(firsts.end(), d.first().begin(), d.first().end());
-        lasts.insert(lasts.end(), d.last().begin(), d.last().end());
+        std::vector<std::int64_t> ids, gid_off{0}, gids, outer_off{0}, outer, halo_off{0}, halo;
+        for (const auto& d : domains)
+        {
+            ids.push_back((std::int64_t)d.domain_id());
+            for (auto g : d.gids()) gids.push_back((std::int64_t)g);
+            for (auto l : d.outer_lids()) outer.push_back((std::int64_t)l);
+            gid_off.push_back((std::int64_t)gids.size());
+            outer_off.push_back((std::int64_t)outer.size());
+            if (!hg.all())
+            {
+                for (auto g : hg.gids()) halo.push_back((std::int64_t)g);
+                halo_off.push_back((std::int64_t)halo.size());
+            }
+        }
+        ghexb_pattern h = nullptr;
+        check(ghexb_pattern_create_unstructured(ctxt.get(), (int)ids.size(), ids.data(), gid_off.data(), gids.data(),
+            outer_off.data(), outer.data(), hg.all() ? nullptr : halo_off.data(), hg.all() ? nullptr : halo.data(), &h));
+        return pattern_container<Grid, dom_type>(h);
     }
-    std::array<int, dim> periodic{};
-    for (int a = 0; a < dim; ++a) periodic[a] = hg.periodic()[a] ? 1 : 0;
-    ghexb_pattern h = nullptr;
-    check(ghexb_pattern_create_regular(ctxt.get(), dim, hg.global_first().data(), hg.global_last().data(), hg.halos().data(),
-        periodic.data(), (int)ids.size(), ids.data(), firsts.data(), lasts.data(), &h));
-    return pattern_container<Grid, dom_type>(h);
+    else
+    {
+        constexpr int dim = dom_type::dim;
+        std::vector<std::int64_t> ids;
+        std::vector<int> firsts, lasts;
+        for (const auto& d : domains)
+        {
+            ids.push_back((std::int64_t)d.domain_id());
+            firsts.insert(firsts.end(), d.first().begin(), d.first().end());
+            lasts.insert(lasts.end(), d.last().begin(), d.last().end());
+        }
+        std::array<int, dim> periodic{};
+        for (int a = 0; a < dim; ++a) periodic[a] = hg.periodic()[a] ? 1 : 0;
+        ghexb_pattern h = nullptr;
+        check(ghexb_pattern_create_regular(ctxt.get(), dim, hg.global_first().data(), hg.global_last().data(), hg.halos().data(),
+            periodic.data(), (int)ids.size(), ids.data(), firsts.data(), lasts.data(), &h));
+        return pattern_container<Grid, dom_type>(h);
+    }
 }
 
 // The handle of one exchange: wait() blocks until the halos are written (communication_handle)

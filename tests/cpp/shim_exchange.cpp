@@ -4,7 +4,8 @@
 // which is known in closed form (value = global linear index + 0.5); the interior must stay as it
 // was. Run once with device fields (ghexb::gpu) and once with fields in ordinary host memory
 // (ghexb::cpu). Also checks GHEX's error behaviour: a second exchange before wait() and a field of
-// a domain outside the pattern. Prints "shim: ok" and returns 0 when every check passes.
+// a domain outside the pattern. Then unstructured column data (run_unstructured) the same two ways.
+// Prints "shim: ok" and returns 0 when every check passes.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -124,6 +125,71 @@ int run(ghexb::context& ctxt, bool device)
         for (double* p : data) cudaFree(p);
     return errors;
 }
+
+// Unstructured column data as GHEX's unstructured tests write it: a ring of NV vertices in four
+// domains of consecutive global ids, each storing its inner vertices and then its two neighbours
+// (the outer, halo, elements), LV levels per vertex, levels first. After the exchange a halo
+// column holds its owner's values (value = gid * 10 + level + 0.25).
+constexpr int NV = 64, ND = 4, LV = 3;
+using udomain = ghexb::unstructured::domain_descriptor<int, int>;
+using uhalo_gen = ghexb::unstructured::halo_generator<int, int>;
+
+double column_value(int gid, int lev) { return gid * 10.0 + lev + 0.25; }
+
+template<typename Arch>
+int run_unstructured(ghexb::context& ctxt, bool device)
+{
+    const int per = NV / ND;
+    std::vector<udomain> doms;
+    std::vector<std::vector<int>> gids(ND);
+    for (int d = 0; d < ND; ++d)
+    {
+        for (int k = 0; k < per; ++k) gids[d].push_back(d * per + k);
+        gids[d].push_back((d * per + NV - 1) % NV); // left neighbour
+        gids[d].push_back(((d + 1) * per) % NV);    // right neighbour
+        const std::vector<int> outer{per, per + 1};
+        doms.emplace_back(d, gids[d].begin(), gids[d].end(), outer.begin(), outer.end());
+    }
+    auto pattern = ghexb::make_pattern<ghexb::unstructured::grid>(ctxt, uhalo_gen(), doms);
+    auto co = ghexb::make_communication_object<decltype(pattern)>(ctxt);
+    std::vector<std::vector<double>> host(ND);
+    std::vector<double*> data;
+    for (int d = 0; d < ND; ++d)
+    {
+        host[d].assign((size_t)(per + 2) * LV, std::nan(""));
+        for (int k = 0; k < per; ++k)
+            for (int l = 0; l < LV; ++l) host[d][(size_t)k * LV + l] = column_value(gids[d][k], l);
+        if (device)
+        {
+            double* p = nullptr;
+            if (cudaMalloc(&p, host[d].size() * sizeof(double)) != cudaSuccess) return 100;
+            cudaMemcpy(p, host[d].data(), host[d].size() * sizeof(double), cudaMemcpyHostToDevice);
+            data.push_back(p);
+        }
+        else
+            data.push_back(host[d].data());
+    }
+    std::vector<ghexb::buffer_info> bis;
+    for (int d = 0; d < ND; ++d)
+        bis.push_back(pattern(ghexb::unstructured::data_descriptor<Arch, int, int, double>(doms[d], data[d], LV, true)));
+    co.exchange(bis.begin(), bis.end()).wait();
+    int errors = 0;
+    for (int d = 0; d < ND; ++d)
+    {
+        if (device) cudaMemcpy(host[d].data(), data[d], host[d].size() * sizeof(double), cudaMemcpyDeviceToHost);
+        for (int k = 0; k < per + 2; ++k)
+            for (int l = 0; l < LV; ++l)
+            {
+                const double want = column_value(gids[d][k], l), got = host[d][(size_t)k * LV + l];
+                if (std::memcmp(&want, &got, sizeof got)) ++errors;
+            }
+    }
+    if (errors) std::printf("shim: %d wrong unstructured values (%s fields)\n", errors, device ? "device" : "host");
+    bis.clear();
+    if (device)
+        for (double* p : data) cudaFree(p);
+    return errors;
+}
 } // namespace
 
 int main()
@@ -131,8 +197,8 @@ int main()
     try
     {
         ghexb::context ctxt(0);
-        const int dev_errors = run<ghexb::gpu>(ctxt, true);
-        const int host_errors = run<ghexb::cpu>(ctxt, false);
+        const int dev_errors = run<ghexb::gpu>(ctxt, true) + run_unstructured<ghexb::gpu>(ctxt, true);
+        const int host_errors = run<ghexb::cpu>(ctxt, false) + run_unstructured<ghexb::cpu>(ctxt, false);
         if (dev_errors || host_errors)
         {
             std::printf("shim: %d device and %d host errors\n", dev_errors, host_errors);
