@@ -1,6 +1,7 @@
 /*
  * ghex_b200.hpp — C++ front end over the C ABI of ghex_b200.h, with the names and call shapes of
- * GHEX's own C++ interface for the regular structured grid and for unstructured column data, so
+ * GHEX's own C++ interface for the regular structured grid, the cubed sphere and unstructured column
+ * data, so
  * that GHEX code of the form
  *
  *     auto ctxt    = ghexb::context(device);
@@ -23,6 +24,9 @@
  *   unstructured::halo_generator           unstructured/user_concepts.hpp:181-256
  *   unstructured::data_descriptor          unstructured/user_concepts.hpp:264-581
  *   make_pattern<unstructured::grid>       pattern_container.hpp:112-120, unstructured/pattern.hpp:187-370
+ *   structured::cubed_sphere::cube, domain_descriptor, halo_generator, field_descriptor
+ *                                          structured/cubed_sphere/domain_descriptor.hpp:26-104,
+ *                                          halo_generator.hpp:59-71, field_descriptor.hpp:26-121
  *
  * Header only; link with libghex_b200.so. Every failing C call throws ghexb::error (a
  * std::runtime_error carrying the status code and the library's message), as GHEX throws
@@ -245,6 +249,102 @@ class field_descriptor
     std::vector<std::int64_t> m_byte_strides;
 };
 } // namespace regular
+
+namespace cubed_sphere
+{
+// cubed_sphere::cube{edge_size, levels}
+struct cube
+{
+    int edge_size;
+    int levels;
+};
+
+// cubed_sphere::domain_descriptor(cube, tile, x_first, x_last, y_first, y_last); its id is
+// (tile, x_first, y_first)
+class domain_descriptor
+{
+  public:
+    struct domain_id_type
+    {
+        int tile, x, y;
+        bool operator==(const domain_id_type& o) const noexcept { return tile == o.tile && x == o.x && y == o.y; }
+    };
+    domain_descriptor(const cube& c, int tile, int x_first, int x_last, int y_first, int y_last)
+    : m_cube(c)
+    , m_tile(tile)
+    , m_x{x_first, x_last}
+    , m_y{y_first, y_last}
+    {
+    }
+    domain_id_type domain_id() const noexcept { return {m_tile, m_x[0], m_y[0]}; }
+    int edge_size() const noexcept { return m_cube.edge_size; }
+    int levels() const noexcept { return m_cube.levels; }
+    int tile() const noexcept { return m_tile; }
+    const std::array<int, 2>& x() const noexcept { return m_x; }
+    const std::array<int, 2>& y() const noexcept { return m_y; }
+
+  private:
+    cube m_cube;
+    int m_tile;
+    std::array<int, 2> m_x, m_y;
+};
+
+// cubed_sphere::halo_generator(halo) or (halos: -x, +x, -y, +y)
+class halo_generator
+{
+  public:
+    explicit halo_generator(int halo) noexcept
+    : m_halos{halo, halo, halo, halo}
+    {
+    }
+    explicit halo_generator(const std::array<int, 4>& halos) noexcept
+    : m_halos(halos)
+    {
+    }
+    const std::array<int, 4>& halos() const noexcept { return m_halos; }
+
+  private:
+    std::array<int, 4> m_halos;
+};
+
+// cubed_sphere::field_descriptor<T, Arch, Layout>(dom, data, offsets, extents, num_components,
+// is_vector_field) on (x, y, z, component), x fastest by default; a vector field's components
+// 0 and 1 are negated where a tile edge's rotation turns them
+template<typename T, typename Arch, typename Layout = layout_map<3, 2, 1, 0>>
+class field_descriptor
+{
+  public:
+    using value_type = T;
+    using arch_type = Arch;
+    field_descriptor(const domain_descriptor& dom, T* data, const std::array<int, 3>& offsets, const std::array<int, 3>& extents,
+        unsigned num_components = 1u, bool is_vector_field = false)
+    : m_dom(dom)
+    , m_data(data)
+    , m_offsets{offsets[0], offsets[1], offsets[2], 0}
+    , m_extents{extents[0], extents[1], extents[2], (int)num_components}
+    , m_is_vector(is_vector_field)
+    {
+    }
+    const domain_descriptor& domain() const noexcept { return m_dom; }
+    T* data() const noexcept { return m_data; }
+    const std::array<int, 4>& offsets() const noexcept { return m_offsets; }
+    const std::array<int, 4>& extents() const noexcept { return m_extents; }
+    int num_components() const noexcept { return m_extents[3]; }
+    bool is_vector_field() const noexcept { return m_is_vector; }
+    std::size_t span_bytes() const noexcept
+    {
+        std::size_t n = sizeof(T);
+        for (int e : m_extents) n *= (std::size_t)e;
+        return n;
+    }
+
+  private:
+    domain_descriptor m_dom;
+    T* m_data;
+    std::array<int, 4> m_offsets, m_extents;
+    bool m_is_vector;
+};
+} // namespace cubed_sphere
 } // namespace structured
 
 namespace unstructured
@@ -428,6 +528,31 @@ class pattern_container
         return bi;
     }
 
+    // pattern(field_descriptor) -> buffer_info for cubed-sphere fields (addressed by the domain's
+    // place in the pattern's list)
+    template<typename T, typename Arch, typename Layout>
+    buffer_info operator()(const structured::cubed_sphere::field_descriptor<T, Arch, Layout>& f) const
+    {
+        const auto id = f.domain().domain_id();
+        int index = -1;
+        for (size_t k = 0; k < m_cubed_ids.size() && index < 0; ++k)
+            if (m_cubed_ids[k] == id) index = (int)k;
+        if (index < 0) throw error(GHEXB_ERR_INCOMPATIBLE, "field incompatible with available domains!");
+        const auto lm = Layout::values();
+        buffer_info bi;
+        if (std::is_same<Arch, cpu>::value)
+        {
+            int owned = 0;
+            check(ghexb_host_register(f.data(), f.span_bytes(), &owned));
+            if (owned) bi.m_state->registered = f.data();
+        }
+        ghexb_field h = nullptr;
+        check(ghexb_field_wrap(get(), index, detail::dtype_of<T>::value, f.data(), 4, f.offsets().data(), f.extents().data(),
+            lm.data(), nullptr, f.num_components(), f.is_vector_field() ? 1 : 0, &h));
+        bi.m_state->field.reset(h);
+        return bi;
+    }
+
     // pattern(data_descriptor) -> buffer_info for unstructured column fields
     template<typename Arch, typename DomainId, typename Idx, typename T>
     buffer_info operator()(const unstructured::data_descriptor<Arch, DomainId, Idx, T>& f) const
@@ -448,6 +573,7 @@ class pattern_container
 
   private:
     std::shared_ptr<ghexb_pattern_s> m_h;
+    std::vector<structured::cubed_sphere::domain_descriptor::domain_id_type> m_cubed_ids; // cubed-sphere patterns
     explicit pattern_container(ghexb_pattern h)
     : m_h(h, [](ghexb_pattern p) { if (p) ghexb_pattern_destroy(p); })
     {
@@ -464,7 +590,27 @@ auto make_pattern(context& ctxt, const HaloGenerator& hg, const DomainRange& dom
     static_assert(std::is_same<Grid, structured::grid>::value || std::is_same<Grid, unstructured::grid>::value,
         "this front end covers the regular structured grid and unstructured column data");
     using dom_type = typename std::decay<decltype(*std::begin(domains))>::type;
-    if constexpr (std::is_same<Grid, unstructured::grid>::value)
+    if constexpr (std::is_same<dom_type, structured::cubed_sphere::domain_descriptor>::value)
+    {
+        // make_pattern<structured::grid> over cubed-sphere domains (GHEX dispatches on the domain type)
+        std::vector<int> tiles, x0, x1, y0, y1;
+        int edge = 0, levels = 0;
+        std::vector<structured::cubed_sphere::domain_descriptor::domain_id_type> ids;
+        for (const auto& d : domains)
+        {
+            tiles.push_back(d.tile()), x0.push_back(d.x()[0]), x1.push_back(d.x()[1]);
+            y0.push_back(d.y()[0]), y1.push_back(d.y()[1]);
+            edge = d.edge_size(), levels = d.levels();
+            ids.push_back(d.domain_id());
+        }
+        ghexb_pattern h = nullptr;
+        check(ghexb_pattern_create_cubed_sphere(ctxt.get(), edge, levels, hg.halos().data(), (int)tiles.size(), tiles.data(),
+            x0.data(), x1.data(), y0.data(), y1.data(), &h));
+        pattern_container<Grid, dom_type> pc(h);
+        pc.m_cubed_ids = std::move(ids);
+        return pc;
+    }
+    else if constexpr (std::is_same<Grid, unstructured::grid>::value)
     {
         std::vector<std::int64_t> ids, gid_off{0}, gids, outer_off{0}, outer, halo_off{0}, halo;
         for (const auto& d : domains)
