@@ -742,10 +742,24 @@ def measure_program(dev, timer, dtype, steps, warmup, baseline=True) -> dict:
         ms_f = timer(fwd, steps, warmup)
         fwd_bwd()
     torch.cuda.synchronize()
+    # the same program and gradient replayed from one CUDA graph
+    graphed = AG.GraphedDiffusion(dx, x0, nsteps, alpha)
+    with torch.cuda.stream(timer.stream):
+        ms_graph = timer(lambda: graphed.run(x0), steps, warmup)
+        loss_g, grad_g = graphed.run(x0)
+    torch.cuda.synchronize()
+    loss_a = AG.interior_loss(out["ys"]).detach()
+
+    def bits(a, b):
+        return torch.equal(a.contiguous().view(torch.int64 if a.dtype == torch.float64 else torch.int32),
+                           b.contiguous().view(torch.int64 if b.dtype == torch.float64 else torch.int32))
     res = {"workload": w.name + f", {nsteps} x (exchange, 7-point update), loss = sum of squares, forward + backward",
            "dtype": np.dtype(dtype).name.replace("float", "f"),
            "forward_backward_ms": ms_fb, "forward_ms": ms_f, "inner_steps": nsteps,
-           "forward_backward_ms_per_inner_step": ms_fb / nsteps, "plan_pool": dx.pool_stats()}
+           "forward_backward_ms_per_inner_step": ms_fb / nsteps, "plan_pool": dx.pool_stats(),
+           "graphed": {"forward_backward_ms": ms_graph, "forward_backward_ms_per_inner_step": ms_graph / nsteps,
+                       "form": "GraphedDiffusion: the same kernels in one CUDA graph on fixed buffers",
+                       "same_bits_as_autograd": bool(bits(loss_g, loss_a) and all(bits(g, a) for g, a in zip(grad_g, out["grad"])))}}
     if baseline:
         from oracle import regular as O
         from oracle import stencil as S

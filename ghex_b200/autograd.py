@@ -33,7 +33,7 @@ from . import _capi
 from ._capi import call
 from ._core import BufferInfo, ExchangePlan, _flatten, _layout_of, context
 
-__all__ = ["DifferentiableExchange", "stencil7", "Stencil7", "diffusion_program"]
+__all__ = ["DifferentiableExchange", "stencil7", "Stencil7", "diffusion_program", "GraphedDiffusion"]
 
 
 class _PlanPool:
@@ -216,3 +216,74 @@ def interior_loss(xs: Sequence[torch.Tensor], halo: int = 1) -> torch.Tensor:
     """Sum of squares of the interiors."""
     h = halo
     return sum((x[h:-h, h:-h, h:-h] ** 2).sum() for x in xs)
+
+
+class GraphedDiffusion:
+    """The diffusion program (``steps`` x (halo exchange, 7-point update), loss = sum of squares of
+    the final interiors) and its gradient with respect to the input fields, replayed from one CUDA
+    graph: the kernels of ``diffusion_program`` and of its backward through torch.autograd, in the
+    same order, on buffers of fixed memory, so that the host launches one graph instead of the
+    program's kernels one by one.
+
+    The forward alternates two buffer sets; the backward seeds 2 x (final interior) and applies, for
+    every step in reverse, the stencil's transpose and then the exchange's adjoint, on two more
+    buffer sets. Four exchange plans of its own are bound to the four sets before the capture, so
+    the capture holds only kernel launches. ``run(xs)`` copies the inputs in, replays the graph, and returns the loss and
+    the gradient (tensors the next run overwrites)."""
+
+    def __init__(self, dx: DifferentiableExchange, templates: Sequence[torch.Tensor], steps: int = 10,
+                 alpha: float = 0.1, halo: int = 1):
+        templates = list(templates)
+        dx.check(templates)
+        self.dx, self.steps, self.alpha, self.halo = dx, steps, alpha, halo
+        dev = templates[0].device
+
+        def buffers():
+            return [torch.zeros_like(t) for t in templates]
+        self._inp, self._a, self._b, self._g1, self._g2 = buffers(), buffers(), buffers(), buffers(), buffers()
+        stream = torch.cuda.Stream(device=dev)
+        stream.wait_stream(torch.cuda.current_stream(dev))
+
+        def plan_for(bufs):
+            # a plan of its own, bound to these buffers for the graph's life (a plan of the
+            # differentiable exchange's pool may be rebound to other tensors later)
+            plan = ExchangePlan(dx.context, dx._bis)
+            plan.rebind(bufs, stream=stream)
+            return plan
+        with torch.cuda.stream(stream):
+            self._fwd = [plan_for(bufs) for bufs in (self._a, self._b)]
+            self._bwd = [plan_for(bufs) for bufs in (self._g1, self._g2)]
+            for plan in self._bwd:
+                if plan.info()["adjoint_launches"] != 1:
+                    raise ValueError("a graphed program needs an exchange whose adjoint is one kernel")
+        torch.cuda.synchronize(dev)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph, stream=stream):
+            self.loss, self.grad = self._body()
+
+    def _body(self):
+        s = torch.cuda.current_stream()
+        h = self.halo
+        for x, y in zip(self._a, self._inp):
+            x.copy_(y)
+        cur, nxt, plans = self._a, self._b, self._fwd
+        for k in range(self.steps):
+            plans[k % 2].launch(stream=s)
+            _launch_stencil(cur, nxt, self.alpha, h, adjoint=False)
+            cur, nxt = nxt, cur
+        loss = interior_loss(cur, h)
+        g, gn, bplans = self._g1, self._g2, self._bwd
+        for gt, x in zip(g, cur):
+            gt.zero_()
+            gt[h:-h, h:-h, h:-h] = 2 * x[h:-h, h:-h, h:-h]
+        for k in range(self.steps):
+            _launch_stencil(g, gn, self.alpha, h, adjoint=True)
+            bplans[(k + 1) % 2].adjoint(stream=s)
+            g, gn = gn, g
+        return loss, g
+
+    def run(self, xs: Sequence[torch.Tensor]):
+        for y, x in zip(self._inp, xs):
+            y.copy_(x)
+        self.graph.replay()
+        return self.loss, self.grad

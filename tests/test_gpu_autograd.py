@@ -161,3 +161,24 @@ def test_plan_pool_rebinds(cuda):
     torch.cuda.synchronize()
     for s in sets:
         assert sum(bits_equal(t.cpu().numpy(), r) for t, r in zip(s, ref)) == 0
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_graphed_program_same_bits(cuda, dtype):
+    """The program and its gradient replayed from one CUDA graph (GraphedDiffusion) give the
+    autograd program's loss and gradient bit for bit, and the oracle's gradient, on two different
+    inputs through the same graph."""
+    p = Program(W.config4(shape=(32, 24, 16), dtype=dtype), cuda)
+    graphed = AG.GraphedDiffusion(p.dx, p.x0, STEPS, ALPHA)
+    for scale in (1.0, -0.5):
+        xs = [x * scale for x in p.x0]
+        leaves = [x.clone().requires_grad_(True) for x in xs]
+        ys = AG.diffusion_program(p.dx, [x.clone() for x in leaves], STEPS, ALPHA)
+        loss = AG.interior_loss(ys)
+        loss.backward()
+        loss_g, grad_g = graphed.run(xs)
+        torch.cuda.synchronize()
+        assert bits_equal(loss_g.cpu().numpy(), loss.detach().cpu().numpy()) == 0
+        assert sum(bits_equal(g.cpu().numpy(), l.grad.cpu().numpy()) for g, l in zip(grad_g, leaves)) == 0
+    g_ref = p.oracle.gradient([h * -0.5 for h in p.host])
+    assert sum(bits_equal(g.cpu().numpy(), r) for g, r in zip(grad_g, g_ref)) == 0
