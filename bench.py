@@ -77,8 +77,9 @@ def parse():
     ap.add_argument("--calibrate-host", action="store_true",
                     help="the same row pattern in pinned host memory (the e2e form's access over the host "
                          "interconnect) and host<->device copies")
-    ap.add_argument("--profile", choices=["batched", "per_field", "adjoint"], default=None,
-                    help="only run `--steps` launches of one form after `--warmup` (for ncu captures)")
+    ap.add_argument("--profile", choices=["batched", "per_field", "adjoint", "program"], default=None,
+                    help="only run `--steps` launches of one form after `--warmup` (for ncu captures); "
+                         "`program` replays the graphed differentiable program of cfg4 or cfg4_f32")
     ap.add_argument("--tuning", default=None,
                     help="the tuning of the headline workload's plan, as printed in the bench line's "
                          "roofline.traffic_tuning (e.g. k8.b128.p0.s1.st8x16384.c4.g1; a trailing .a<-1..2> sets the adjoint's "
@@ -703,12 +704,9 @@ def measure_config(cfg, dev, timer, peak, steps, warmup, autotune=True, baseline
     return out
 
 
-def measure_program(dev, timer, dtype, steps, warmup, baseline=True) -> dict:
-    """The differentiable program of the 256x256x128 workload (2x2x2 domains, halo 1, periodic): 10
-    x (halo exchange, 7-point update x <- x + 0.1 L(x)), loss = sum of squares of the final
-    interiors, forward and backward through torch.autograd. One timed step = the whole program,
-    forward and backward (the backward runs the exchange's adjoint kernel and the stencil's
-    transpose); also timed: the forward alone."""
+def program_case(dev, dtype):
+    """The 256x256x128 workload (2x2x2 domains, halo 1, periodic) as a differentiable exchange:
+    (workload, DifferentiableExchange, host arrays, device fields)."""
     import torch
     from ghex_b200 import autograd as AG
     from ghex_b200 import workloads as W
@@ -722,7 +720,34 @@ def measure_program(dev, timer, dtype, steps, warmup, baseline=True) -> dict:
     host = [w.domain_array(d, spec) for d in w.domains]
     x0 = [torch.from_numpy(a).to(dev) for a in host]
     bis = [pat(R.make_field_descriptor(dm, t, w.offsets(spec), w.extents(d, spec))) for dm, d, t in zip(doms, w.domains, x0)]
-    dx = AG.DifferentiableExchange(ctx, bis)
+    return w, AG.DifferentiableExchange(ctx, bis), host, x0
+
+
+def profile_program(args, dev) -> None:
+    """`--profile program`: the graphed differentiable program (10 x (exchange, 7-point update),
+    forward and backward) of cfg4 (float64) or cfg4_f32, replayed `--warmup + --steps` times."""
+    import torch
+    from ghex_b200 import autograd as AG
+    dtype = np.float32 if args.config == "cfg4_f32" else np.float64
+    w, dx, _, x0 = program_case(dev, dtype)
+    graphed = AG.GraphedDiffusion(dx, x0, 10, 0.1)
+    for _ in range(args.warmup + args.steps):
+        graphed.run(x0)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": "program", "config": w.name, "dtype": np.dtype(dtype).name,
+                      "replays": args.warmup + args.steps}), flush=True)
+
+
+def measure_program(dev, timer, dtype, steps, warmup, baseline=True) -> dict:
+    """The differentiable program of the 256x256x128 workload (2x2x2 domains, halo 1, periodic): 10
+    x (halo exchange, 7-point update x <- x + 0.1 L(x)), loss = sum of squares of the final
+    interiors, forward and backward through torch.autograd. One timed step = the whole program,
+    forward and backward (the backward runs the exchange's adjoint kernel and the stencil's
+    transpose); also timed: the forward alone."""
+    import torch
+    from ghex_b200 import autograd as AG
+    w, dx, host, x0 = program_case(dev, dtype)
+    spec = w.fields[0]
     nsteps, alpha = 10, 0.1
     out = {}
 
@@ -1055,6 +1080,9 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
+    if args.profile == "program":
+        profile_program(args, dev)
+        return
     case = Case(args.config, dev, local)
     plan = case.plan
     if args.profile:
