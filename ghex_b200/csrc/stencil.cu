@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cstdint>
 
+#include "async_copy.hpp"
 #include "stencil.hpp"
 
 namespace ghexb
@@ -38,110 +39,172 @@ struct domain_args
     stencil_domain d[k_stencil_batch];
 };
 
-// A block of 32 x 8 threads covers a 32 x 8 patch of (i, j) columns of one domain (blockIdx.z)
-// and a slab of k_slab planes; each thread takes one column through the slab. The column's own
-// values of planes k0 - 1 .. k0 + k_slab are loaded once into registers (each serves three
-// planes), the four in-plane neighbours of every plane come from the caches, where the
-// neighbouring threads of the block load them as their own columns. All loads of the slab are
-// issued before the first result, so a thread keeps up to 5 * k_slab + 2 loads in flight.
-constexpr int k_tile_x = 32, k_tile_y = 8, k_slab = 4;
+// A block of 32 x 8 threads computes a patch of 32 x (8 x rows) (i, j) columns of one domain
+// (blockIdx.z) over a slab of planes, each thread the rows ty, ty + 8, ... of its column i. The
+// planes it reads (the patch and a ring of one column around it) pass through shared memory:
+// asynchronous element copies (cp.async, which zero-fill what the update treats as zero) keep
+// k_ahead planes in flight ahead of the plane being computed, in a ring of k_stages plane
+// buffers, and every neighbour is then a shared-memory read at a fixed offset. Element offsets
+// advance by the plane stride from plane to plane (I: 32-bit when every offset of the launch
+// fits, else 64-bit), so the work per element is a few copies, seven shared-memory reads, the
+// arithmetic and one store.
+constexpr int k_tx = 32, k_ty = 8, k_px = k_tx + 2;
+constexpr int k_stages = 8, k_ahead = k_stages - 1;
+constexpr int k_threads = k_tx * k_ty;
 
-template <typename T, bool ADJOINT>
-__global__ void __launch_bounds__(k_tile_x * k_tile_y) stencil7_kernel(const __grid_constant__ domain_args args, T alpha,
-    unsigned nslabs, unsigned nblocks_y)
+// Rows per thread: two for float (a 32 x 16 patch), one for double (32 x 8), whose larger
+// elements keep enough bytes in flight with the smaller patch (measured on the 130 x 130 x 66
+// domains of the 256x256x128 program: float 33 against 37 us, double 44 against 50 us).
+template <typename T> struct patch
 {
+    static constexpr int rows = sizeof(T) == 8 ? 1 : 2;
+    static constexpr int plane = k_px * (k_ty * rows + 2);          // the patch and its ring
+    static constexpr int slots = (plane + k_threads - 1) / k_threads; // copies per thread and plane
+};
+static_assert((k_stages & (k_stages - 1)) == 0, "a ring of a power of two");
+
+template <typename T>
+__device__ __forceinline__ void copy_element(uint32_t dst, const T* src, bool valid)
+{
+    // src-size 0 writes zeros and reads nothing
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"((int)sizeof(T)),
+                 "r"(valid ? (int)sizeof(T) : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void copy_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void copy_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Buffer element (a, b) of a plane holds (i0 - 1 + a, j0 - 1 + b). Forward: every element in the
+// array (an interior element reads only those); adjoint: G, the gradient on interior elements and
+// zero elsewhere.
+template <typename T, bool ADJOINT, typename I>
+__global__ void __launch_bounds__(k_threads) stencil7_kernel(const __grid_constant__ domain_args args, T alpha,
+    unsigned nslabs, unsigned nblocks_y, int slab)
+{
+    constexpr int k_rows = patch<T>::rows, k_plane = patch<T>::plane, k_slots = patch<T>::slots;
+    __shared__ __align__(16) T buf[k_stages][k_plane];
     const stencil_domain& d = args.d[blockIdx.z];
-    const int i = blockIdx.x * k_tile_x + threadIdx.x;
+    const T* __restrict__ in = static_cast<const T*>(d.in);
+    T* __restrict__ out = static_cast<T*>(d.out);
     const int h = d.halo, ex = d.ex, ey = d.ey, ez = d.ez;
-    const int64_t sx = d.sx, sy = d.sy, sz = d.sz;
+    const I sx = (I)d.sx, sy = (I)d.sy, sz = (I)d.sz;
     const auto within = [](int v, int lo, int hi) { return v >= lo && v < hi; };
+    const int tid = threadIdx.y * k_tx + threadIdx.x;
+    const int i0 = blockIdx.x * k_tx, i = i0 + threadIdx.x;
+    // copied planes: forward [0, ez), adjoint [h, ez - h)
+    const int klo = ADJOINT ? h : 0, khi = ADJOINT ? ez - h : ez;
+    const uint32_t base = smem_u32(&buf[0][0]);
     for (unsigned b = blockIdx.y; b < nblocks_y; b += gridDim.y)
     {
         const unsigned ytile = b / nslabs;
-        const int j = (int)(ytile * k_tile_y + threadIdx.y);
-        const int k0 = (int)(b - ytile * nslabs) * k_slab;
-        if (i >= ex || j >= ey || k0 >= ez) continue;
-        const int64_t base = i * sx + j * sy;
-        const T* __restrict__ c = static_cast<const T*>(d.in) + base;
-        T* __restrict__ o = static_cast<T*>(d.out) + base;
-        const bool iin = within(i, h, ex - h), jin = within(j, h, ey - h), col = iin && jin;
-        T v[k_slab + 2];     // the column at planes k0 - 1 + q
-        T nb[k_slab][4];     // -x, +x, -y, +y neighbours at plane k0 + q
-        if constexpr (!ADJOINT)
+        const int j0 = (int)ytile * (k_ty * k_rows);
+        const int k0 = (int)(b - ytile * nslabs) * slab;
+        if (i0 >= ex || j0 >= ey || k0 >= ez) continue; // uniform in the block
+        const int nout = min(slab, ez - k0), nplanes = nout + 2;
+        // this thread's elements of every plane buffer: offsets at plane k0 - 1 (advanced per plane)
+        I src[k_slots];
+        bool col[k_slots];
+        uint32_t dst[k_slots];
+#pragma unroll
+        for (int r = 0; r < k_slots; ++r)
         {
-            // interior planes [h, ez - h) read planes h - 1 .. ez - h of interior columns, all in the array
-#pragma unroll
-            for (int q = 0; q < k_slab + 2; ++q)
+            const int e = tid + r * k_threads;
+            const int gi = i0 - 1 + e % k_px, gj = j0 - 1 + e / k_px;
+            col[r] = e < k_plane && (ADJOINT ? within(gi, h, ex - h) && within(gj, h, ey - h) : within(gi, 0, ex) && within(gj, 0, ey));
+            src[r] = col[r] ? (I)gi * sx + (I)gj * sy + (I)(k0 - 1) * sz : I(0);
+            dst[r] = base + (uint32_t)(min(e, k_plane - 1) * sizeof(T));
+        }
+        int next = 0; // the next plane to copy
+        const auto issue = [&]() {
+            if (next < nplanes)
             {
-                const int k = k0 - 1 + q;
-                v[q] = col && k >= h - 1 && k <= ez - h ? c[k * sz] : T(0);
-            }
+                const int k = k0 - 1 + next;
+                const bool kin = k >= klo && k < khi;
+                const uint32_t so = (uint32_t)((next & (k_stages - 1)) * (k_plane * (int)sizeof(T)));
 #pragma unroll
-            for (int q = 0; q < k_slab; ++q)
-            {
-                const int k = k0 + q;
-                const bool on = col && within(k, h, ez - h);
-                const T* p = c + k * sz;
-                nb[q][0] = on ? p[-sx] : T(0);
-                nb[q][1] = on ? p[sx] : T(0);
-                nb[q][2] = on ? p[-sy] : T(0);
-                nb[q][3] = on ? p[sy] : T(0);
-            }
-#pragma unroll
-            for (int q = 0; q < k_slab; ++q)
-            {
-                const int k = k0 + q;
-                T y = T(0);
-                if (col && within(k, h, ez - h))
+                for (int r = 0; r < k_slots; ++r)
                 {
-                    const T x = v[q + 1];
-                    T s = add_rn(nb[q][0], nb[q][1]);
-                    s = add_rn(s, nb[q][2]);
-                    s = add_rn(s, nb[q][3]);
-                    s = add_rn(s, v[q]);
-                    s = add_rn(s, v[q + 2]);
-                    y = add_rn(x, mul_rn(alpha, sub_rn(s, mul_rn(T(6), x))));
+                    const bool ok = col[r] && kin;
+                    if ((r + 1) * k_threads <= k_plane || tid + r * k_threads < k_plane)
+                        copy_element(dst[r] + so, in + (ok ? src[r] : I(0)), ok);
+                    src[r] += sz;
                 }
-                if (k < ez) o[k * sz] = y;
             }
-        }
-        else
+            ++next;
+            copy_commit(); // an empty group past the last plane keeps the count of groups uniform
+        };
+#pragma unroll
+        for (int L = 0; L < k_ahead; ++L) issue();
+        int c[k_rows];
+        bool mine[k_rows], col_in[k_rows];
+        I o[k_rows];
+#pragma unroll
+        for (int q = 0; q < k_rows; ++q)
         {
-            // G(q) = gy[q] on interior elements, 0 elsewhere: a neighbour column is read only where
-            // it is interior, so every read is in the array
-            const bool mxm = within(i - 1, h, ex - h) && jin, mxp = within(i + 1, h, ex - h) && jin;
-            const bool mym = iin && within(j - 1, h, ey - h), myp = iin && within(j + 1, h, ey - h);
+            const int ty = threadIdx.y + q * k_ty, j = j0 + ty;
+            c[q] = (ty + 1) * k_px + threadIdx.x + 1;
+            mine[q] = i < ex && j < ey;
+            col_in[q] = within(i, h, ex - h) && within(j, h, ey - h);
+            o[q] = mine[q] ? (I)i * sx + (I)j * sy + (I)k0 * sz : I(0);
+        }
+        for (int m = 0; m < nout; ++m)
+        {
+            // planes m, m + 1 and m + 2 have landed (groups through m + k_ahead - 1 were committed)
+            copy_wait<k_ahead - 3>();
+            __syncthreads();
+            issue(); // plane m + k_ahead, into the buffer of plane m - 1, which every thread has read
+            const T* zm = buf[m & (k_stages - 1)];
+            const T* pk = buf[(m + 1) & (k_stages - 1)];
+            const T* zp = buf[(m + 2) & (k_stages - 1)];
+            const bool kin = within(k0 + m, h, ez - h);
 #pragma unroll
-            for (int q = 0; q < k_slab + 2; ++q)
+            for (int q = 0; q < k_rows; ++q)
             {
-                const int k = k0 - 1 + q;
-                v[q] = col && within(k, h, ez - h) ? c[k * sz] : T(0);
-            }
-#pragma unroll
-            for (int q = 0; q < k_slab; ++q)
-            {
-                const int k = k0 + q;
-                const bool kin = within(k, h, ez - h);
-                const T* p = c + k * sz;
-                nb[q][0] = mxm && kin ? p[-sx] : T(0);
-                nb[q][1] = mxp && kin ? p[sx] : T(0);
-                nb[q][2] = mym && kin ? p[-sy] : T(0);
-                nb[q][3] = myp && kin ? p[sy] : T(0);
-            }
-#pragma unroll
-            for (int q = 0; q < k_slab; ++q)
-            {
-                const int k = k0 + q;
-                const T g = v[q + 1];
-                T t = add_rn(nb[q][0], nb[q][1]);
-                t = add_rn(t, nb[q][2]);
-                t = add_rn(t, nb[q][3]);
-                t = add_rn(t, v[q]);
-                t = add_rn(t, v[q + 2]);
-                if (k < ez) o[k * sz] = add_rn(g, mul_rn(alpha, sub_rn(t, mul_rn(T(6), g))));
+                const int cq = c[q];
+                T y;
+                if constexpr (!ADJOINT)
+                {
+                    y = T(0);
+                    if (col_in[q] && kin)
+                    {
+                        const T x = pk[cq];
+                        T s = add_rn(pk[cq - 1], pk[cq + 1]);
+                        s = add_rn(s, pk[cq - k_px]);
+                        s = add_rn(s, pk[cq + k_px]);
+                        s = add_rn(s, zm[cq]);
+                        s = add_rn(s, zp[cq]);
+                        y = add_rn(x, mul_rn(alpha, sub_rn(s, mul_rn(T(6), x))));
+                    }
+                }
+                else
+                {
+                    const T g = pk[cq];
+                    T t = add_rn(pk[cq - 1], pk[cq + 1]);
+                    t = add_rn(t, pk[cq - k_px]);
+                    t = add_rn(t, pk[cq + k_px]);
+                    t = add_rn(t, zm[cq]);
+                    t = add_rn(t, zp[cq]);
+                    y = add_rn(g, mul_rn(alpha, sub_rn(t, mul_rn(T(6), g))));
+                }
+                if (mine[q]) out[o[q]] = y;
+                o[q] += sz;
             }
         }
+        // the next slab's copies reuse the buffers: all copies landed, all reads done
+        copy_wait<0>();
+        __syncthreads();
     }
+}
+
+template <typename T, typename I>
+void launch_kernel(bool adjoint, dim3 grid, const domain_args& args, T alpha, unsigned nslabs, unsigned ny, int slab,
+    cudaStream_t stream)
+{
+    const dim3 block(k_tx, k_ty);
+    if (adjoint)
+        stencil7_kernel<T, true, I><<<grid, block, 0, stream>>>(args, alpha, nslabs, ny, slab);
+    else
+        stencil7_kernel<T, false, I><<<grid, block, 0, stream>>>(args, alpha, nslabs, ny, slab);
 }
 
 template <typename T>
@@ -152,22 +215,28 @@ cudaError_t launch_t(const stencil_domain* doms, int n, double alpha, bool adjoi
         domain_args args{};
         const int m = n - b < k_stencil_batch ? n - b : k_stencil_batch;
         int mx = 0, my = 0, mz = 0;
+        bool narrow = true; // every element offset, and the offsets advanced two planes past the end, below 2^31
         for (int i = 0; i < m; ++i)
         {
-            args.d[i] = doms[b + i];
-            mx = std::max(mx, doms[b + i].ex), my = std::max(my, doms[b + i].ey), mz = std::max(mz, doms[b + i].ez);
+            const stencil_domain& d = doms[b + i];
+            args.d[i] = d;
+            mx = std::max(mx, d.ex), my = std::max(my, d.ey), mz = std::max(mz, d.ez);
+            const int64_t span = (int64_t)(d.ex - 1) * d.sx + (int64_t)(d.ey - 1) * d.sy + (int64_t)(d.ez + 2) * d.sz;
+            narrow = narrow && span < ((int64_t)1 << 31) - 1;
         }
         if (mx <= 0 || my <= 0 || mz <= 0) continue;
-        const unsigned xtiles = (unsigned)((mx + k_tile_x - 1) / k_tile_x);
-        const unsigned nslabs = (unsigned)((mz + k_slab - 1) / k_slab);
-        const uint64_t ny = (uint64_t)((my + k_tile_y - 1) / k_tile_y) * nslabs;
+        // slabs of about 16 planes, of equal depth
+        const int nsl = (mz + 15) / 16, slab = (mz + nsl - 1) / nsl;
+        const unsigned xtiles = (unsigned)((mx + k_tx - 1) / k_tx);
+        const unsigned nslabs = (unsigned)((mz + slab - 1) / slab);
+        constexpr int rows = k_ty * patch<T>::rows;
+        const uint64_t ny = (uint64_t)((my + rows - 1) / rows) * nslabs;
         if (ny > 0xffffffffull) return cudaErrorInvalidValue;
         const dim3 grid(xtiles, (unsigned)std::min<uint64_t>(ny, 65535), (unsigned)m);
-        const dim3 block(k_tile_x, k_tile_y);
-        if (adjoint)
-            stencil7_kernel<T, true><<<grid, block, 0, stream>>>(args, (T)alpha, nslabs, (unsigned)ny);
+        if (narrow)
+            launch_kernel<T, int32_t>(adjoint, grid, args, (T)alpha, nslabs, (unsigned)ny, slab, stream);
         else
-            stencil7_kernel<T, false><<<grid, block, 0, stream>>>(args, (T)alpha, nslabs, (unsigned)ny);
+            launch_kernel<T, int64_t>(adjoint, grid, args, (T)alpha, nslabs, (unsigned)ny, slab, stream);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }

@@ -68,6 +68,29 @@ def test_stencil_kernels_bit_exact(cuda, dtype, order):
         assert bits_equal(o.cpu().numpy(), S.adjoint(x, ALPHA)) == 0
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("halo", [1, 2])
+def test_stencil_kernels_edges_bit_exact(cuda, dtype, halo):
+    """Halo 2; 35 domains in one call (two launches of at most 32); extents that leave partial
+    32 x 8 patches and several slabs of planes (z extent 53 and 70); a strided view whose rows are
+    not contiguous: forward and transpose bit-exact against the oracle."""
+    rng = np.random.default_rng(11 + halo)
+    shapes = [(5 + (d % 7), 6 + (d % 5), 5 + (d % 3)) for d in range(33)] + [(40, 19, 53), (33, 9, 70)]
+    xs = [np.asarray(rng.standard_normal(s), dtype=dtype, order="F") for s in shapes]
+    dev = [to_device(x, cuda) for x in xs]
+    big = torch.zeros((2 * 38, 17, 25), dtype=dev[0].dtype, device=cuda)
+    view = big[::2, :, 1:-2]                     # strides (2, .., ..) over a C-ordered base
+    view.copy_(torch.from_numpy(np.asarray(rng.standard_normal(view.shape), dtype=dtype)).to(cuda))
+    xs.append(view.cpu().numpy())
+    dev.append(view)
+    for adjoint in (False, True):
+        outs = [torch.empty_strided(d.shape, d.stride(), dtype=d.dtype, device=cuda) for d in dev]
+        AG._launch_stencil(dev, outs, ALPHA, halo, adjoint=adjoint)
+        ref = S.adjoint if adjoint else S.apply
+        for x, o in zip(xs, outs):
+            assert bits_equal(o.cpu().numpy(), ref(x, ALPHA, halo)) == 0
+
+
 def test_stencil_rejects_bad_arguments(cuda):
     x = torch.zeros((2, 5, 5), dtype=torch.float64, device=cuda)
     with pytest.raises(Exception, match="twice the halo"):
