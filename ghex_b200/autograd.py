@@ -274,8 +274,13 @@ class GraphedDiffusion:
         loss = interior_loss(cur, h)
         g, gn, bplans = self._g1, self._g2, self._bwd
         for gt, x in zip(g, cur):
-            gt.zero_()
-            gt[h:-h, h:-h, h:-h] = 2 * x[h:-h, h:-h, h:-h]
+            if self.steps > 0:
+                # the last update wrote +0 on every halo cell, so doubling the whole array (exact)
+                # gives the seed, 2 x on the interior and +0 elsewhere, in one kernel
+                torch.mul(x, 2, out=gt)
+            else:
+                gt.zero_()
+                gt[h:-h, h:-h, h:-h] = 2 * x[h:-h, h:-h, h:-h]
         for k in range(self.steps):
             _launch_stencil(g, gn, self.alpha, h, adjoint=True)
             bplans[(k + 1) % 2].adjoint(stream=s)
