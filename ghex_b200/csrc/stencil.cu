@@ -52,9 +52,9 @@ constexpr int k_tx = 32, k_ty = 8, k_px = k_tx + 2;
 constexpr int k_stages = 8, k_ahead = k_stages - 1;
 constexpr int k_threads = k_tx * k_ty;
 
-// Rows per thread: two for float (a 32 x 16 patch), one for double (32 x 8), whose larger
-// elements keep enough bytes in flight with the smaller patch (measured on the 130 x 130 x 66
-// domains of the 256x256x128 program: float 33 against 37 us, double 44 against 50 us).
+// Rows per thread: two for float (a 32 x 16 patch), one for double (32 x 8), the faster choice
+// for each type on the 130 x 130 x 66 domains of the 256x256x128 program (forward, float: 33 us
+// with two rows against 37 us with one; double: 44 us with one row against 50 us with two).
 template <typename T> struct patch
 {
     static constexpr int rows = sizeof(T) == 8 ? 1 : 2;
