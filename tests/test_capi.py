@@ -133,3 +133,28 @@ def test_sharded_and_ipc_argument_checks():
 
 def test_adjoint_tuning_range():
     assert _capi.lib.ghexb_plan_set_adjoint_tuning(None, 0) == _capi.ERR_INVALID
+
+
+def test_stencil_argument_checks():
+    """ghexb_stencil7 refuses bad arguments before any device call (fake addresses, never read)."""
+    P = C.c_void_p * 1
+    I64 = C.c_int64 * 3
+
+    def call(dtype=_capi.F64, n=1, src=1 << 40, dst=(1 << 40) + (1 << 30), ext=(8, 8, 8), st=(1, 8, 64), halo=1):
+        return _capi.lib.ghexb_stencil7(dtype, n, P(src), P(dst), I64(*ext), I64(*st), halo, 0.1, 0, None)
+
+    assert call(n=0) == 0                                   # nothing to do, no device needed
+    cases = [
+        (dict(dtype=99), "float32 or float64"),
+        (dict(n=-1), "negative"),
+        (dict(halo=0), "halo"),
+        (dict(src=0), "null"),
+        (dict(src=(1 << 40) + 4), "aligned"),               # float64 data at a 4-byte boundary
+        (dict(ext=(2, 8, 8)), "twice the halo"),
+        (dict(ext=(8, 8, 4), halo=2), "twice the halo"),
+        (dict(st=(1, 0, 64)), "positive"),
+        (dict(dst=(1 << 40) + 8 * 100), "overlap"),         # inside the 512-element input
+    ]
+    for kw, msg in cases:
+        assert call(**kw) == _capi.ERR_INVALID, kw
+        assert msg in _capi.last_error(), (kw, _capi.last_error())
